@@ -1,0 +1,231 @@
+"""ctypes binding of the C ABI in include/gprat_cu.h (libgprat_cuda.so).
+
+This is the thinnest host path to the CUDA kernels: tests and the benchmark
+call the library through it exactly as a foreign-language caller would.  The
+library must have been built (``python -m gprat_b200.build``); importing this
+module fails loudly otherwise -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libgprat_cuda.so")
+HEADER = os.path.join(os.path.dirname(_PKG), "include", "gprat_cu.h")
+
+OK = 0
+ERR_INVALID_ARG = 1
+ERR_OOM = 2
+ERR_NOT_SPD = 3
+ERR_CUDA = 4
+ERR_TIMEOUT = 5
+ERR_NO_DEVICE = 6
+
+PREC_FP64 = 0
+PREC_MIXED_TF32 = 1
+PREC_MIXED_BF16 = 2
+
+
+class GpratCudaError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[gprat_cu error {code}] {message}")
+        self.code = code
+
+
+class NotPositiveDefiniteError(GpratCudaError):
+    pass
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_i64 = ctypes.c_int64
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libgprat_cuda.so is not built ({LIB_PATH}); run `python -m gprat_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.gprat_cu_last_error.restype = ctypes.c_char_p
+    lib.gprat_cu_version.restype = ctypes.c_char_p
+    lib.gprat_cu_device_count.argtypes = [_ip]
+    lib.gprat_cu_gp_create.argtypes = [ctypes.c_int, _dp, _i64, _dp, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_void_p)]
+    lib.gprat_cu_gp_destroy.argtypes = [ctypes.c_void_p]
+    lib.gprat_cu_gp_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.gprat_cu_cholesky.argtypes = [ctypes.c_void_p, _dp, _dp]
+    lib.gprat_cu_predict.argtypes = [ctypes.c_void_p, _dp, _dp, _i64, ctypes.c_int, ctypes.c_int, _dp]
+    for name in ("gprat_cu_predict_with_uncertainty", "gprat_cu_predict_with_full_cov"):
+        getattr(lib, name).argtypes = [ctypes.c_void_p, _dp, _dp, _i64, ctypes.c_int, ctypes.c_int, _dp, _dp]
+    lib.gprat_cu_predict_full_covariance.argtypes = [ctypes.c_void_p, _dp, _dp, _i64, ctypes.c_int, _dp, _dp]
+    lib.gprat_cu_compute_loss.argtypes = [ctypes.c_void_p, _dp, _dp]
+    lib.gprat_cu_loss_grad.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+    lib.gprat_cu_optimize_step.argtypes = [ctypes.c_void_p, _dp, _dp, _ip, ctypes.c_int, _dp]
+    lib.gprat_cu_optimize.argtypes = [ctypes.c_void_p, _dp, _dp, _ip, ctypes.c_int, _dp]
+    lib.gprat_cu_fit_predict_device.argtypes = [ctypes.c_void_p, _dp, ctypes.c_void_p, _i64, ctypes.c_int,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.gprat_cu_check_status.argtypes = [ctypes.c_void_p]
+    lib.gprat_cu_stats_enable_timing.argtypes = [ctypes.c_int]
+    lib.gprat_cu_stats_read.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _dp, _dp]
+    return lib
+
+
+lib = _load()
+
+
+def declared_symbols() -> List[str]:
+    """Every function name declared in include/gprat_cu.h."""
+    with open(HEADER) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"\b(gprat_cu_[a-z_0-9]+)\s*\(", text)))
+
+
+def check(rc: int) -> None:
+    if rc == OK:
+        return
+    msg = lib.gprat_cu_last_error().decode()
+    if rc == ERR_NOT_SPD:
+        raise NotPositiveDefiniteError(rc, msg)
+    raise GpratCudaError(rc, msg)
+
+
+def device_count() -> int:
+    c = ctypes.c_int(0)
+    check(lib.gprat_cu_device_count(ctypes.byref(c)))
+    return c.value
+
+
+def stats_reset() -> None:
+    check(lib.gprat_cu_stats_reset())
+
+
+def stats_enable_timing(enable: bool) -> None:
+    check(lib.gprat_cu_stats_enable_timing(int(bool(enable))))
+
+
+def stats_read() -> dict:
+    """{'launches', 'gemm_launches', 'gemm_ms', 'gemm_flops'} since the last reset."""
+    a, b = ctypes.c_int64(), ctypes.c_int64()
+    c, d = ctypes.c_double(), ctypes.c_double()
+    check(lib.gprat_cu_stats_read(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)))
+    return {"launches": a.value, "gemm_launches": b.value, "gemm_ms": c.value, "gemm_flops": d.value}
+
+
+def _arr(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _hyper(h) -> np.ndarray:
+    h = _arr(h)
+    if h.size != 3:
+        raise ValueError("hyper-parameters must be (lengthscale, vertical_lengthscale, noise_variance)")
+    return h
+
+
+class CudaGP:
+    """One device-resident GP (handle over gprat_cu_gp)."""
+
+    def __init__(self, x: Sequence[float], y: Sequence[float], n_tiles: int, n_tile_size: int, n_reg: int = 8,
+                 device: int = 0):
+        self.x, self.y = _arr(x), _arr(y)
+        self.n_tiles, self.n_tile_size, self.n_reg = int(n_tiles), int(n_tile_size), int(n_reg)
+        self.n = self.n_tiles * self.n_tile_size
+        h = ctypes.c_void_p()
+        check(lib.gprat_cu_gp_create(int(device), _p(self.x), self.x.size, _p(self.y), self.y.size, self.n_tiles,
+                                     self.n_tile_size, self.n_reg, ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.gprat_cu_gp_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def set_precision(self, precision: int) -> None:
+        check(lib.gprat_cu_gp_set_precision(self._h, int(precision)))
+
+    def cholesky(self, hyper) -> List[Optional[np.ndarray]]:
+        nt, t = self.n_tiles, self.n_tile_size
+        out = np.empty(nt * nt * t * t)
+        check(lib.gprat_cu_cholesky(self._h, _p(_hyper(hyper)), _p(out)))
+        tiles = out.reshape(nt * nt, t * t)
+        return [tiles[i * nt + j].copy() if j <= i else None for i in range(nt) for j in range(nt)]
+
+    def predict(self, hyper, xt, m_tiles: int, m_tile_size: int) -> np.ndarray:
+        xt = _arr(xt)
+        mean = np.empty(max(m_tiles * m_tile_size, 1))
+        check(lib.gprat_cu_predict(self._h, _p(_hyper(hyper)), _p(xt), xt.size, m_tiles, m_tile_size, _p(mean)))
+        return mean[: m_tiles * m_tile_size]
+
+    def predict_with_uncertainty(self, hyper, xt, m_tiles: int, m_tile_size: int) -> Tuple[np.ndarray, np.ndarray]:
+        xt = _arr(xt)
+        m = m_tiles * m_tile_size
+        mean, var = np.empty(max(m, 1)), np.empty(max(m, 1))
+        check(lib.gprat_cu_predict_with_uncertainty(self._h, _p(_hyper(hyper)), _p(xt), xt.size, m_tiles,
+                                                    m_tile_size, _p(mean), _p(var)))
+        return mean[:m], var[:m]
+
+    def predict_with_full_cov(self, hyper, xt, m_tiles: int, m_tile_size: int) -> Tuple[np.ndarray, np.ndarray]:
+        xt = _arr(xt)
+        m = m_tiles * m_tile_size
+        mean, var = np.empty(max(m, 1)), np.empty(max(m, 1))
+        check(lib.gprat_cu_predict_with_full_cov(self._h, _p(_hyper(hyper)), _p(xt), xt.size, m_tiles, m_tile_size,
+                                                 _p(mean), _p(var)))
+        return mean[:m], var[:m]
+
+    def predict_full_covariance(self, hyper, xt, m: int) -> Tuple[np.ndarray, np.ndarray]:
+        xt = _arr(xt)
+        mean, cov = np.empty(max(m, 1)), np.empty(max(m * m, 1))
+        check(lib.gprat_cu_predict_full_covariance(self._h, _p(_hyper(hyper)), _p(xt), xt.size, m, _p(mean),
+                                                   _p(cov)))
+        return mean[:m], cov[: m * m].reshape(m, m)
+
+    def compute_loss(self, hyper) -> float:
+        v = ctypes.c_double()
+        check(lib.gprat_cu_compute_loss(self._h, _p(_hyper(hyper)), ctypes.byref(v)))
+        return v.value
+
+    def loss_grad(self, hyper) -> Tuple[float, np.ndarray]:
+        v = ctypes.c_double()
+        g = np.empty(3)
+        check(lib.gprat_cu_loss_grad(self._h, _p(_hyper(hyper)), ctypes.byref(v), _p(g)))
+        return v.value, g
+
+    def optimize_step(self, params, adam, trainable, iter_: int) -> Tuple[float, np.ndarray]:
+        p = _arr(params).copy()
+        a = _arr(adam)
+        t = np.ascontiguousarray([int(bool(v)) for v in trainable], dtype=np.int32)
+        v = ctypes.c_double()
+        check(lib.gprat_cu_optimize_step(self._h, _p(p), _p(a), t.ctypes.data_as(_ip), int(iter_), ctypes.byref(v)))
+        return v.value, p
+
+    def optimize(self, params, adam, trainable, opt_iter: int) -> Tuple[np.ndarray, np.ndarray]:
+        p = _arr(params).copy()
+        a = _arr(adam)
+        t = np.ascontiguousarray([int(bool(v)) for v in trainable], dtype=np.int32)
+        losses = np.empty(max(int(opt_iter), 1))
+        check(lib.gprat_cu_optimize(self._h, _p(p), _p(a), t.ctypes.data_as(_ip), int(opt_iter), _p(losses)))
+        return losses[: int(opt_iter)], p
+
+    def fit_predict_device(self, hyper, d_xt: int, n_xt: int, m: int, d_mean: int, d_var: Optional[int],
+                           stream: int = 0) -> None:
+        check(lib.gprat_cu_fit_predict_device(self._h, _p(_hyper(hyper)), ctypes.c_void_p(d_xt), n_xt, m,
+                                              ctypes.c_void_p(d_mean), ctypes.c_void_p(d_var or 0),
+                                              ctypes.c_void_p(stream)))
+
+    def check_status(self) -> None:
+        check(lib.gprat_cu_check_status(self._h))

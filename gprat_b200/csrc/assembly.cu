@@ -1,0 +1,232 @@
+// Squared-exponential covariance assembly on sm_100a.
+//
+// k(z_i, z_j) = v * exp(-0.5 / l^2 * sum_k (z_{i+k} - z_{j+k})^2): feature
+// rows are sliding windows of one series (compute_covariance_function,
+// core/src/cpu/gp_algorithms.cpp:11-28; GPU twin core/src/gpu/gp_algorithms.cu:16-55).
+//
+// One CTA produces a 64-row x 128-column block.  The two windows of the
+// series it needs (64+d-1 and 128+d-1 values) are staged in shared memory
+// once; each thread owns one column and walks the rows four at a time, so
+// row values are shared-memory broadcasts and column values are
+// conflict-free.  Every row of the block is written by whole warps as
+// contiguous 256-byte segments (coalesced).  The distance sum keeps the
+// reference's order and rounding (separate multiply and add, k ascending),
+// so entries differ from the reference only by exp()'s last-place rounding.
+#include "common.cuh"
+
+namespace gprat_cu
+{
+namespace
+{
+
+constexpr int AR = 64;   // rows per CTA
+constexpr int AC = 128;  // columns per CTA (= threads)
+constexpr int RB = 4;    // rows per inner pass
+
+__device__ __forceinline__ double se_entry(double dist, double neg_half_inv_l2, double v)
+{
+    return v * exp(__dmul_rn(neg_half_inv_l2, dist));
+}
+
+// Computes RB distances for rows i..i+RB-1 (local) and column j (local).
+__device__ __forceinline__ void distances(const double *xr, const double *xc, int i, int j, int d, double (&acc)[RB])
+{
+#pragma unroll
+    for (int r = 0; r < RB; ++r)
+    {
+        acc[r] = 0.0;
+    }
+    for (int k = 0; k < d; ++k)
+    {
+        double c = xc[j + k];
+#pragma unroll
+        for (int r = 0; r < RB; ++r)
+        {
+            double z = __dsub_rn(xr[i + r + k], c);
+            acc[r] = __dadd_rn(acc[r], __dmul_rn(z, z));
+        }
+    }
+}
+
+// mode 0: K (lower tiles of size T incl. full diagonal tiles, + noise on the
+//         global diagonal); mode 1: cross / prior (all entries, no noise).
+template <int MODE>
+__global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
+                                               int rows,
+                                               const double *__restrict__ xcol,
+                                               int cols,
+                                               int d,
+                                               int T,
+                                               const DeviceParams *__restrict__ p,
+                                               double *__restrict__ out,
+                                               int64_t ldo,
+                                               const double *__restrict__ alpha,
+                                               double *__restrict__ mean_partial,
+                                               int mean_parts)
+{
+    extern __shared__ double sh[];
+    const int i0 = blockIdx.y * AR;
+    const int j0 = blockIdx.x * AC;
+    if (MODE == 0)
+    {
+        int last_row = min(i0 + AR, rows) - 1;
+        int max_col = (last_row / T + 1) * T - 1;
+        if (j0 > max_col)
+        {
+            return;
+        }
+    }
+    double *xr = sh;             // AR + d - 1
+    double *xc = sh + AR + d;    // AC + d - 1
+    double *red = xc + AC + d;   // AR x (AC/32) mean partials
+    for (int q = threadIdx.x; q < AR + d - 1; q += AC)
+    {
+        int g = i0 + q;
+        xr[q] = (g < rows + d - 1) ? xrow[g] : 0.0;
+    }
+    for (int q = threadIdx.x; q < AC + d - 1; q += AC)
+    {
+        int g = j0 + q;
+        xc[q] = (g < cols + d - 1) ? xcol[g] : 0.0;
+    }
+    __syncthreads();
+
+    const double l = p->hyper[0];
+    const double v = p->hyper[1];
+    const double noise = p->hyper[2];
+    const double nh = -0.5 / (l * l);
+    const int j = threadIdx.x;
+    const int gj = j0 + j;
+    const double aj = (alpha != nullptr && gj < cols) ? alpha[gj] : 0.0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+    for (int i = 0; i < AR; i += RB)
+    {
+        double acc[RB];
+        distances(xr, xc, i, j, d, acc);
+#pragma unroll
+        for (int r = 0; r < RB; ++r)
+        {
+            int gi = i0 + i + r;
+            double val = se_entry(acc[r], nh, v);
+            bool inside = gi < rows && gj < cols;
+            if (MODE == 0)
+            {
+                inside = inside && (gj / T <= gi / T);
+                if (gi == gj)
+                {
+                    val += noise;
+                }
+            }
+            if (inside && out != nullptr)
+            {
+                out[static_cast<int64_t>(gi) * ldo + gj] = val;
+            }
+            if (mean_partial != nullptr)
+            {
+                double prod = inside ? val * aj : 0.0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+                {
+                    prod += __shfl_xor_sync(0xffffffffu, prod, o);
+                }
+                if (lane == 0)
+                {
+                    red[(i + r) * (AC / 32) + warp] = prod;
+                }
+            }
+        }
+    }
+    if (mean_partial != nullptr)
+    {
+        __syncthreads();
+        for (int r = threadIdx.x; r < AR; r += AC)
+        {
+            int gi = i0 + r;
+            if (gi < rows)
+            {
+                double s = 0.0;
+#pragma unroll
+                for (int w = 0; w < AC / 32; ++w)
+                {
+                    s += red[r * (AC / 32) + w];
+                }
+                mean_partial[static_cast<int64_t>(gi) * mean_parts + blockIdx.x] = s;
+            }
+        }
+    }
+}
+
+__global__ void reduce_rows_kernel(const double *__restrict__ part, int m, int parts, double *__restrict__ out)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < m)
+    {
+        double s = 0.0;
+        for (int q = 0; q < parts; ++q)
+        {
+            s += part[static_cast<int64_t>(r) * parts + q];
+        }
+        out[r] = s;
+    }
+}
+
+size_t se_smem(int d) { return static_cast<size_t>(AR + d + AC + d + AR * (AC / 32)) * sizeof(double); }
+
+template <int MODE>
+void launch_se(const double *xrow, int rows, const double *xcol, int cols, int d, int T, const DeviceParams *p,
+               double *out, int64_t ldo, const double *alpha, double *mean_partial, int parts, cudaStream_t s)
+{
+    if (rows <= 0 || cols <= 0)
+    {
+        return;
+    }
+    size_t smem = se_smem(d);
+    if (smem > 227 * 1024)
+    {
+        throw Error(1, "too many regressors for the assembly kernel");
+    }
+    if (smem > 48 * 1024)
+    {
+        ensure_smem_attr(reinterpret_cast<const void *>(se_kernel<MODE>), static_cast<int>(smem));
+    }
+    dim3 grid(ceil_div(cols, AC), ceil_div(rows, AR));
+    se_kernel<MODE><<<grid, AC, smem, s>>>(xrow, rows, xcol, cols, d, T, p, out, ldo, alpha, mean_partial, parts);
+    GPRAT_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void assemble_covariance(const double *x, int n, int n_reg, int tile, const DeviceParams *p, double *K, int64_t ldk,
+                         cudaStream_t s)
+{
+    launch_se<0>(x, n, x, n, n_reg, tile, p, K, ldk, nullptr, nullptr, 0, s);
+}
+
+void assemble_cross(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, double *Kx,
+                    int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s)
+{
+    if (mean_partial != nullptr && mean_parts != ceil_div(n, AC))
+    {
+        throw Error(1, "assemble_cross: mean_parts must be ceil(n/128)");
+    }
+    launch_se<1>(xt, m, x, n, n_reg, 1, p, Kx, ldx, alpha, mean_partial, mean_parts, s);
+}
+
+void reduce_mean(const double *mean_partial, int m, int parts, double *mean, cudaStream_t s)
+{
+    if (m <= 0)
+    {
+        return;
+    }
+    reduce_rows_kernel<<<ceil_div(m, 256), 256, 0, s>>>(mean_partial, m, parts, mean);
+    GPRAT_LAUNCH_CHECK();
+}
+
+void assemble_prior(const double *xt, int m, int n_reg, const DeviceParams *p, double *Kss, int64_t lds,
+                    cudaStream_t s)
+{
+    launch_se<1>(xt, m, xt, m, n_reg, 1, p, Kss, lds, nullptr, nullptr, 0, s);
+}
+
+}  // namespace gprat_cu

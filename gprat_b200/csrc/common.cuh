@@ -1,0 +1,176 @@
+// Shared device/host definitions of libgprat_cuda.so (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+namespace gprat_cu
+{
+
+// Device-resident hyper-parameter and optimiser state.  Every kernel that
+// needs theta reads it from here, so an optimisation loop never returns to
+// the host between steps.
+struct DeviceParams
+{
+    double hyper[3];   // lengthscale, vertical_lengthscale, noise_variance
+    double m_T[3];     // Adam first moments (SEKParams::m_T, core/include/gp_kernels.hpp:37)
+    double w_T[3];     // Adam second moments (SEKParams::w_T, :39)
+    double adam[4];    // learning_rate, beta1, beta2, epsilon
+    int trainable[3];
+    int iter;          // Adam iteration index (bias correction)
+    double loss;       // last loss
+    double grad[3];    // last gradient (unconstrained, reference scaling)
+    double loss_hist_dummy;
+};
+
+// Device status word: first failing Cholesky pivot (1-based global row),
+// and a timeout flag for bounded waits.
+struct DeviceStatus
+{
+    int not_spd_row;  // 0 = ok
+    int timeout;      // 0 = ok
+};
+
+// Error carrying a gprat_cu status code.
+struct Error : std::runtime_error
+{
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) { }
+};
+
+#define GPRAT_CUDA_CHECK(expr)                                                                              \
+    do                                                                                                      \
+    {                                                                                                       \
+        cudaError_t _e = (expr);                                                                            \
+        if (_e != cudaSuccess)                                                                              \
+        {                                                                                                   \
+            throw ::gprat_cu::Error(_e == cudaErrorMemoryAllocation ? 2 : 4,                                \
+                                    std::string(#expr) + ": " + cudaGetErrorString(_e) + " (" __FILE__ ")"); \
+        }                                                                                                   \
+    } while (0)
+
+// Counts one kernel launch of this library (stats.cu).
+void note_launch();
+
+#define GPRAT_LAUNCH_CHECK()                    \
+    do                                          \
+    {                                           \
+        ::gprat_cu::note_launch();              \
+        GPRAT_CUDA_CHECK(cudaGetLastError());   \
+    } while (0)
+
+// GEMM timing hooks (stats.cu): returns true when timing is on, in which
+// case the caller brackets the launch with gemm_timing_begin/end.
+bool gemm_timing_enabled();
+void gemm_timing_begin(cudaStream_t s);
+void gemm_timing_end(cudaStream_t s, double flops);
+
+// Raises the dynamic shared-memory limit of `func` once per device.
+inline void ensure_smem_attr(const void *func, int bytes)
+{
+    static std::mutex mtx;
+    static std::set<std::pair<const void *, int>> done;
+    int dev = 0;
+    GPRAT_CUDA_CHECK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mtx);
+    if (done.count({ func, dev }) != 0)
+    {
+        return;
+    }
+    GPRAT_CUDA_CHECK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    done.insert({ func, dev });
+}
+
+// Writes the whole parameter block from a kernel argument (no host staging
+// buffer, so back-to-back asynchronous calls cannot race on it).
+void set_params(DeviceParams *p, const DeviceParams &value, cudaStream_t s);
+
+inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// Kernel launchers (defined in the .cu files).  All matrices are row-major
+// FP64 with an even leading dimension and 16-byte aligned bases.
+
+// C[MxN] = beta*C + alpha*op(A)*op(B) on FP64 DMMA tensor cores.
+//   transA=false: A is M x K (A[m*lda+k]); true: A stored K x M (A[k*lda+m]).
+//   transB=false: B stored K x N (B[k*ldb+n]); true: B stored N x K (B[n*ldb+k]).
+//   lower: M == N and only C[i][j] with i >= j is written (tiles above the
+//          diagonal are skipped).
+//   rowsq (optional, requires N <= 128): rowsq[i] += sum_j C_new[i][j]^2.
+struct GemmArgs
+{
+    int M, N, K;
+    const double *A;
+    int64_t lda;
+    bool transA;
+    const double *B;
+    int64_t ldb;
+    bool transB;
+    double *C;
+    int64_t ldc;
+    double alpha, beta;
+    bool lower;
+    double *rowsq;
+    int k_tri;  // if >0: for C row-tile starting at row r0, the K loop starts at r0 rounded down to k_tri (A upper-triangular-by-blocks)
+};
+void dgemm(const GemmArgs &a, cudaStream_t s);
+
+// SE covariance assembly (gen_tile_covariance, core/src/cpu/gp_algorithms.cpp:30-62):
+// K[i][j] = v*exp(-0.5/l^2 * sum_k (x[i+k]-x[j+k])^2) (+ noise if i == j), for all
+// (i,j) with floor(j/T) <= floor(i/T) (lower tiles incl. full diagonal tiles).
+void assemble_covariance(const double *x, int n, int n_reg, int tile, const DeviceParams *p, double *K, int64_t ldk,
+                         cudaStream_t s);
+
+// Cross covariance Kx[r][c] = k(xt_r, x_c), r < m, c < n
+// (gen_tile_cross_covariance, core/src/cpu/gp_algorithms.cpp:113-140).  If
+// alpha != nullptr, also mean[r] = sum_c Kx[r][c]*alpha[c]; if Kx == nullptr
+// the matrix is not stored.
+void assemble_cross(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, double *Kx,
+                    int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s);
+void reduce_mean(const double *mean_partial, int m, int parts, double *mean, cudaStream_t s);
+
+// Prior covariance matrix K**[r][c] = k(xt_r, xt_c) (gen_tile_full_prior_covariance,
+// core/src/cpu/gp_algorithms.cpp:64-88), full m x m.
+void assemble_prior(const double *xt, int m, int n_reg, const DeviceParams *p, double *Kss, int64_t lds,
+                    cudaStream_t s);
+
+// Diagonal block Cholesky + inverse: A (bs x bs at A, lda) -> L (lower
+// written back, strict upper untouched), Linv (bs x bs, ld = ldi, zero above
+// the diagonal).  Records the first failing pivot in status.
+void potrf_diag(double *A, int64_t lda, int bs, int row0, double *Linv, int64_t ldi, DeviceStatus *status,
+                cudaStream_t s);
+
+// Triangular solves with the blocked factor (L in Lmat, diagonal-block
+// inverses in Linv, block size nb).
+void trsv_forward(const double *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, double *tmp,
+                  cudaStream_t s);
+void trsv_backward(const double *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, double *tmp,
+                   cudaStream_t s);
+
+// Loss 0.5*(y.a + sum log(L_ii^2) + n log 2pi)/n -> p->loss.
+void loss_kernel(const double *y, const double *alpha, const double *L, int64_t ldl, int n, DeviceParams *p,
+                 cudaStream_t s);
+
+// var[r] = v - acc[r]
+void finalize_variance(const double *acc, int m, const DeviceParams *p, double *var, cudaStream_t s);
+
+// Fill helpers
+void set_identity(double *A, int64_t lda, int n, cudaStream_t s);
+void copy_rows(const double *src, int64_t lds, double *dst, int64_t ldd, int rows, int cols, cudaStream_t s);
+
+// Adjoint: per lower tile partial sums of (Kinv - a a^T) .* dK for l and v, and
+// the noise term; then reduction + Adam (see optimizer.cu).
+void adjoint_trace(const double *U, int64_t ldu, const double *alpha, const double *x, int n, int n_reg,
+                   const DeviceParams *p, double *partials, int *n_partials, cudaStream_t s);
+void adjoint_finish(const double *partials, int n_partials, int n, DeviceParams *p, bool adam_step,
+                    cudaStream_t s);
+
+}  // namespace gprat_cu

@@ -1,0 +1,800 @@
+// C-ABI entry points of libgprat_cuda.so and the device-side pipelines.
+//
+// A gprat_cu_gp owns, on one device: the training series and outputs, the
+// covariance / Cholesky factor K (n x ld, row-major, lower triangle used),
+// the inverses of its 128 x 128 diagonal blocks, alpha, the device-resident
+// parameters, a status word, and grow-only workspaces (test series, the
+// n_test x n solve matrix, the inverse factor for the optimiser).
+//
+// Pipelines (reference files in parentheses, relative to the project root):
+//   factor   = SE assembly of the lower tiles + blocked right-looking
+//              Cholesky: potrf+inverse of the diagonal block, panel solve as
+//              a DMMA GEMM with the inverse, lower-only DMMA trailing update
+//              (right_looking_cholesky_tiled, core/src/cpu/tiled_algorithms.cpp:14-57)
+//   alpha    = blocked forward/backward solves (:61-115)
+//   mean     = cross covariance fused with the mat-vec (:187-210)
+//   variance = right-looking solve W L^T = K*  with the row sums of W^2
+//              fused into the diagonal-block step (:117-149, :212-263)
+//   loss     = (core/src/cpu/gp_optimizer.cpp:187-218)
+//   gradient = U = L^-T, fused K^-1 = U U^T tile GEMM + derivative-tile
+//              regeneration + trace reduction, then Adam (optimizer.cu)
+#include "common.cuh"
+#include "gprat_cu.h"
+
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using namespace gprat_cu;
+
+namespace
+{
+
+thread_local std::string g_last_error;
+
+constexpr int NB = 128;  // factorisation block size
+
+struct DeviceGuard
+{
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        GPRAT_CUDA_CHECK(cudaGetDevice(&prev));
+        if (prev != dev)
+        {
+            GPRAT_CUDA_CHECK(cudaSetDevice(dev));
+        }
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0)
+        {
+            cudaSetDevice(prev);
+        }
+    }
+};
+
+template <typename T>
+struct DevBuf
+{
+    T *ptr = nullptr;
+    int64_t cap = 0;  // elements
+    void ensure(int64_t n)
+    {
+        if (n <= cap)
+        {
+            return;
+        }
+        release();
+        GPRAT_CUDA_CHECK(cudaMalloc(&ptr, static_cast<size_t>(n) * sizeof(T)));
+        cap = n;
+    }
+    void release()
+    {
+        if (ptr != nullptr)
+        {
+            cudaFree(ptr);
+        }
+        ptr = nullptr;
+        cap = 0;
+    }
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+};
+
+}  // namespace
+
+struct gprat_cu_gp
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int n = 0, n_tiles = 0, T = 0, d = 0;
+    int64_t n_in = 0;
+    int64_t ld = 0;
+    int nblk = 0;
+    int precision = GPRAT_CU_PREC_FP64;
+
+    DevBuf<double> x, y, K, Linv, alpha, U, partials;
+    DevBuf<double> xt, W, vacc, mean_part, mean, var, losses;
+    DevBuf<DeviceParams> params;
+    DevBuf<DeviceStatus> status;
+    DeviceParams *h_params = nullptr;
+    DeviceStatus *h_status = nullptr;
+
+    ~gprat_cu_gp()
+    {
+        int prev = -1;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        if (stream != nullptr)
+        {
+            cudaStreamSynchronize(stream);
+        }
+        for (DevBuf<double> *b : { &x, &y, &K, &Linv, &alpha, &U, &partials, &xt, &W, &vacc, &mean_part, &mean, &var,
+                                   &losses })
+        {
+            b->release();
+        }
+        params.release();
+        status.release();
+        if (h_params != nullptr)
+        {
+            cudaFreeHost(h_params);
+        }
+        if (h_status != nullptr)
+        {
+            cudaFreeHost(h_status);
+        }
+        if (stream != nullptr)
+        {
+            cudaStreamDestroy(stream);
+        }
+        if (prev >= 0)
+        {
+            cudaSetDevice(prev);
+        }
+    }
+};
+
+namespace
+{
+
+template <typename F>
+int guarded(F &&f)
+{
+    try
+    {
+        f();
+        g_last_error.clear();
+        return GPRAT_CU_OK;
+    }
+    catch (const Error &e)
+    {
+        g_last_error = e.what();
+        return e.code;
+    }
+    catch (const std::bad_alloc &)
+    {
+        g_last_error = "host out of memory";
+        return GPRAT_CU_ERR_OOM;
+    }
+    catch (const std::exception &e)
+    {
+        g_last_error = e.what();
+        return GPRAT_CU_ERR_INVALID_ARG;
+    }
+}
+
+void require(bool cond, const std::string &msg)
+{
+    if (!cond)
+    {
+        throw Error(GPRAT_CU_ERR_INVALID_ARG, msg);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// device pipelines (enqueue only)
+
+void upload_hyper(gprat_cu_gp *gp, const double hyper[3], cudaStream_t s)
+{
+    require(hyper != nullptr, "hyper-parameters must not be NULL");
+    DeviceParams v;
+    std::memset(&v, 0, sizeof(v));
+    for (int q = 0; q < 3; ++q)
+    {
+        v.hyper[q] = hyper[q];
+    }
+    set_params(gp->params.ptr, v, s);
+    GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->status.ptr, 0, sizeof(DeviceStatus), s));
+}
+
+double *kblock(gprat_cu_gp *gp, int r, int c) { return gp->K.ptr + static_cast<int64_t>(r) * gp->ld + c; }
+
+double *linv_block(gprat_cu_gp *gp, int k) { return gp->Linv.ptr + static_cast<int64_t>(k) * NB * NB; }
+
+void cholesky_blocked(gprat_cu_gp *gp, cudaStream_t s)
+{
+    const int n = gp->n;
+    for (int k = 0; k < gp->nblk; ++k)
+    {
+        const int r0 = k * NB;
+        const int bs = std::min(NB, n - r0);
+        potrf_diag(kblock(gp, r0, r0), gp->ld, bs, r0, linv_block(gp, k), NB, gp->status.ptr, s);
+        const int rows = n - r0 - bs;
+        if (rows <= 0)
+        {
+            continue;
+        }
+        // panel: P = P * Linv_kk^T (in place; one CTA column since bs <= 128)
+        GemmArgs pa{};
+        pa.M = rows;
+        pa.N = bs;
+        pa.K = bs;
+        pa.A = kblock(gp, r0 + bs, r0);
+        pa.lda = gp->ld;
+        pa.transA = false;
+        pa.B = linv_block(gp, k);
+        pa.ldb = NB;
+        pa.transB = true;
+        pa.C = kblock(gp, r0 + bs, r0);
+        pa.ldc = gp->ld;
+        pa.alpha = 1.0;
+        pa.beta = 0.0;
+        dgemm(pa, s);
+        // trailing: C -= P P^T, lower triangle only
+        GemmArgs ta{};
+        ta.M = rows;
+        ta.N = rows;
+        ta.K = bs;
+        ta.A = kblock(gp, r0 + bs, r0);
+        ta.lda = gp->ld;
+        ta.transA = false;
+        ta.B = kblock(gp, r0 + bs, r0);
+        ta.ldb = gp->ld;
+        ta.transB = true;
+        ta.C = kblock(gp, r0 + bs, r0 + bs);
+        ta.ldc = gp->ld;
+        ta.alpha = -1.0;
+        ta.beta = 1.0;
+        ta.lower = true;
+        dgemm(ta, s);
+    }
+}
+
+void factor(gprat_cu_gp *gp, cudaStream_t s)
+{
+    assemble_covariance(gp->x.ptr, gp->n, gp->d, gp->T, gp->params.ptr, gp->K.ptr, gp->ld, s);
+    cholesky_blocked(gp, s);
+}
+
+void solve_alpha(gprat_cu_gp *gp, cudaStream_t s)
+{
+    GPRAT_CUDA_CHECK(
+        cudaMemcpyAsync(gp->alpha.ptr, gp->y.ptr, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    trsv_forward(gp->K.ptr, gp->ld, gp->Linv.ptr, NB, gp->n, gp->alpha.ptr, nullptr, s);
+    trsv_backward(gp->K.ptr, gp->ld, gp->Linv.ptr, NB, gp->n, gp->alpha.ptr, nullptr, s);
+}
+
+// Right-looking blocked solve W L^T = W (in place) over the first `rows`
+// rows of W (m x ld); if rowsq != nullptr accumulates sum_j W_ij^2.
+// row_limit(k) bounds the rows touched at block step k (triangular RHS).
+template <typename RowLimit>
+void solve_right_lt(gprat_cu_gp *gp, double *W, int64_t ldw, int rows, double *rowsq, RowLimit row_limit,
+                    cudaStream_t s)
+{
+    const int n = gp->n;
+    for (int k = 0; k < gp->nblk; ++k)
+    {
+        const int c0 = k * NB;
+        const int bs = std::min(NB, n - c0);
+        const int mrows = std::min(rows, row_limit(k));
+        GemmArgs da{};
+        da.M = mrows;
+        da.N = bs;
+        da.K = bs;
+        da.A = W + c0;
+        da.lda = ldw;
+        da.transA = false;
+        da.B = linv_block(gp, k);
+        da.ldb = NB;
+        da.transB = true;
+        da.C = W + c0;
+        da.ldc = ldw;
+        da.alpha = 1.0;
+        da.beta = 0.0;
+        da.rowsq = rowsq;
+        dgemm(da, s);
+        const int rest = n - c0 - bs;
+        if (rest <= 0)
+        {
+            continue;
+        }
+        GemmArgs ua{};
+        ua.M = mrows;
+        ua.N = rest;
+        ua.K = bs;
+        ua.A = W + c0;
+        ua.lda = ldw;
+        ua.transA = false;
+        ua.B = kblock(gp, c0 + bs, c0);
+        ua.ldb = gp->ld;
+        ua.transB = true;
+        ua.C = W + c0 + bs;
+        ua.ldc = ldw;
+        ua.alpha = -1.0;
+        ua.beta = 1.0;
+        dgemm(ua, s);
+    }
+}
+
+// Mean (and variance if var != nullptr) for m test points at d_xt.
+void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
+{
+    if (m <= 0)
+    {
+        return;
+    }
+    const int parts = ceil_div(gp->n, 128);
+    gp->mean_part.ensure(static_cast<int64_t>(m) * parts);
+    if (d_var == nullptr)
+    {
+        assemble_cross(d_xt, m, gp->x.ptr, gp->n, gp->d, gp->params.ptr, nullptr, 0, gp->alpha.ptr,
+                       gp->mean_part.ptr, parts, s);
+        reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
+        return;
+    }
+    gp->W.ensure(static_cast<int64_t>(m) * gp->ld);
+    gp->vacc.ensure(m);
+    assemble_cross(d_xt, m, gp->x.ptr, gp->n, gp->d, gp->params.ptr, gp->W.ptr, gp->ld, gp->alpha.ptr,
+                   gp->mean_part.ptr, parts, s);
+    reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
+    GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->vacc.ptr, 0, m * sizeof(double), s));
+    solve_right_lt(gp, gp->W.ptr, gp->ld, m, gp->vacc.ptr, [m](int) { return m; }, s);
+    finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, s);
+}
+
+void finish_and_check(gprat_cu_gp *gp)
+{
+    GPRAT_CUDA_CHECK(
+        cudaMemcpyAsync(gp->h_status, gp->status.ptr, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, gp->stream));
+    GPRAT_CUDA_CHECK(cudaStreamSynchronize(gp->stream));
+    if (gp->h_status->not_spd_row != 0)
+    {
+        throw Error(GPRAT_CU_ERR_NOT_SPD, "Cholesky factorisation failed: covariance matrix is not positive definite "
+                                          "(non-positive pivot at row " +
+                                              std::to_string(gp->h_status->not_spd_row - 1) + ")");
+    }
+    if (gp->h_status->timeout != 0)
+    {
+        throw Error(GPRAT_CU_ERR_TIMEOUT, "a bounded device wait timed out");
+    }
+}
+
+void upload_test(gprat_cu_gp *gp, const double *test_in, int64_t n_test_in, int m)
+{
+    require(test_in != nullptr, "test input must not be NULL");
+    require(m >= 0, "number of test points must be >= 0");
+    require(n_test_in >= static_cast<int64_t>(m) + gp->d - 1 || m == 0,
+            "test input holds " + std::to_string(n_test_in) + " values; " + std::to_string(m) + " points with " +
+                std::to_string(gp->d) + " regressors need " + std::to_string(static_cast<int64_t>(m) + gp->d - 1));
+    const int64_t need = std::max<int64_t>(static_cast<int64_t>(m) + gp->d - 1, 1);
+    gp->xt.ensure(need);
+    GPRAT_CUDA_CHECK(cudaMemcpyAsync(gp->xt.ptr, test_in, (m > 0 ? need : 0) * sizeof(double), cudaMemcpyHostToDevice,
+                                     gp->stream));
+}
+
+void download(gprat_cu_gp *gp, double *host, const double *dev, int64_t count)
+{
+    if (count > 0)
+    {
+        GPRAT_CUDA_CHECK(cudaMemcpyAsync(host, dev, count * sizeof(double), cudaMemcpyDeviceToHost, gp->stream));
+    }
+}
+
+void gradient_device(gprat_cu_gp *gp, bool adam, cudaStream_t s)
+{
+    factor(gp, s);
+    solve_alpha(gp, s);
+    loss_kernel(gp->y.ptr, gp->alpha.ptr, gp->K.ptr, gp->ld, gp->n, gp->params.ptr, s);
+    // U = L^-T: solve U L^T = I; column block k of U has nonzeros in rows < (k+1)*NB
+    gp->U.ensure(static_cast<int64_t>(gp->n) * gp->ld);
+    set_identity(gp->U.ptr, gp->ld, gp->n, s);
+    solve_right_lt(gp, gp->U.ptr, gp->ld, gp->n, nullptr, [](int k) { return (k + 1) * NB; }, s);
+    const int t = ceil_div(gp->n, 128);
+    gp->partials.ensure(static_cast<int64_t>(t) * (t + 1) / 2 * 3);
+    int np = 0;
+    adjoint_trace(gp->U.ptr, gp->ld, gp->alpha.ptr, gp->x.ptr, gp->n, gp->d, gp->params.ptr, gp->partials.ptr, &np,
+                  s);
+    adjoint_finish(gp->partials.ptr, np, gp->n, gp->params.ptr, adam, s);
+}
+
+void check_gp(gprat_cu_gp *gp) { require(gp != nullptr, "GP handle is NULL"); }
+
+}  // namespace
+
+extern "C" {
+
+const char *gprat_cu_last_error(void) { return g_last_error.c_str(); }
+
+const char *gprat_cu_version(void) { return "gprat_cu 0.1 sm_100a fp64-dmma"; }
+
+int gprat_cu_device_count(int *count)
+{
+    return guarded(
+        [&]
+        {
+            require(count != nullptr, "count must not be NULL");
+            int c = 0;
+            cudaError_t e = cudaGetDeviceCount(&c);
+            if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+            {
+                cudaGetLastError();
+                c = 0;
+            }
+            else
+            {
+                GPRAT_CUDA_CHECK(e);
+            }
+            *count = c;
+        });
+}
+
+int gprat_cu_gp_create(int device, const double *train_in, int64_t n_in, const double *train_out, int64_t n_out,
+                       int n_tiles, int n_tile_size, int n_regressors, gprat_cu_gp **out)
+{
+    return guarded(
+        [&]
+        {
+            require(out != nullptr, "output handle pointer must not be NULL");
+            *out = nullptr;
+            require(train_in != nullptr && train_out != nullptr, "training data must not be NULL");
+            require(n_tiles > 0 && n_tile_size > 0, "n_tiles and n_tile_size must be positive");
+            require(n_regressors > 0, "n_regressors must be positive");
+            const int64_t n = static_cast<int64_t>(n_tiles) * n_tile_size;
+            require(n <= (1LL << 30), "training set too large");
+            require(n_in >= n + n_regressors - 1, "training input holds " + std::to_string(n_in) +
+                                                      " values; the sliding window needs " +
+                                                      std::to_string(n + n_regressors - 1));
+            require(n_out >= n, "training output holds " + std::to_string(n_out) + " values; need " +
+                                    std::to_string(n));
+            int count = 0;
+            cudaError_t ce = cudaGetDeviceCount(&count);
+            if (ce != cudaSuccess || count == 0)
+            {
+                cudaGetLastError();
+                throw Error(GPRAT_CU_ERR_NO_DEVICE, "no CUDA device available");
+            }
+            if (device < 0 || device >= count)
+            {
+                throw Error(GPRAT_CU_ERR_NO_DEVICE, "Requested GPU device is not available.");
+            }
+            DeviceGuard guard(device);
+            auto *gp = new gprat_cu_gp();
+            try
+            {
+                gp->device = device;
+                gp->n = static_cast<int>(n);
+                gp->n_tiles = n_tiles;
+                gp->T = n_tile_size;
+                gp->d = n_regressors;
+                gp->n_in = n + n_regressors - 1;
+                gp->ld = round_up(n, 8);
+                gp->nblk = ceil_div(n, NB);
+                GPRAT_CUDA_CHECK(cudaStreamCreateWithFlags(&gp->stream, cudaStreamNonBlocking));
+                GPRAT_CUDA_CHECK(cudaMallocHost(&gp->h_params, sizeof(DeviceParams)));
+                GPRAT_CUDA_CHECK(cudaMallocHost(&gp->h_status, sizeof(DeviceStatus)));
+                gp->params.ensure(1);
+                gp->status.ensure(1);
+                gp->x.ensure(gp->n_in);
+                gp->y.ensure(n);
+                gp->K.ensure(n * gp->ld);
+                gp->Linv.ensure(static_cast<int64_t>(gp->nblk) * NB * NB);
+                gp->alpha.ensure(n);
+                GPRAT_CUDA_CHECK(cudaMemcpyAsync(gp->x.ptr, train_in, gp->n_in * sizeof(double),
+                                                 cudaMemcpyHostToDevice, gp->stream));
+                GPRAT_CUDA_CHECK(
+                    cudaMemcpyAsync(gp->y.ptr, train_out, n * sizeof(double), cudaMemcpyHostToDevice, gp->stream));
+                GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->K.ptr, 0, n * gp->ld * sizeof(double), gp->stream));
+                GPRAT_CUDA_CHECK(cudaStreamSynchronize(gp->stream));
+            }
+            catch (...)
+            {
+                delete gp;
+                throw;
+            }
+            *out = gp;
+        });
+}
+
+int gprat_cu_gp_destroy(gprat_cu_gp *gp)
+{
+    return guarded([&] { delete gp; });
+}
+
+int gprat_cu_gp_set_precision(gprat_cu_gp *gp, int precision)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(precision == GPRAT_CU_PREC_FP64, "only GPRAT_CU_PREC_FP64 is available in this build");
+            gp->precision = precision;
+        });
+}
+
+int gprat_cu_cholesky(gprat_cu_gp *gp, const double hyper[3], double *tiles_out)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(tiles_out != nullptr, "output must not be NULL");
+            DeviceGuard guard(gp->device);
+            upload_hyper(gp, hyper, gp->stream);
+            factor(gp, gp->stream);
+            std::vector<double> full(static_cast<size_t>(gp->n) * gp->ld);
+            download(gp, full.data(), gp->K.ptr, static_cast<int64_t>(gp->n) * gp->ld);
+            finish_and_check(gp);
+            const int T = gp->T, nt = gp->n_tiles;
+            const size_t tt = static_cast<size_t>(T) * T;
+            for (int i = 0; i < nt; ++i)
+            {
+                for (int j = 0; j < nt; ++j)
+                {
+                    double *dst = tiles_out + (static_cast<size_t>(i) * nt + j) * tt;
+                    if (j > i)
+                    {
+                        std::memset(dst, 0, tt * sizeof(double));
+                        continue;
+                    }
+                    for (int r = 0; r < T; ++r)
+                    {
+                        std::memcpy(dst + static_cast<size_t>(r) * T,
+                                    full.data() + static_cast<size_t>(i * T + r) * gp->ld + static_cast<size_t>(j) * T,
+                                    T * sizeof(double));
+                    }
+                }
+            }
+        });
+}
+
+int gprat_cu_predict(gprat_cu_gp *gp, const double hyper[3], const double *test_in, int64_t n_test_in, int m_tiles,
+                     int m_tile_size, double *mean)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(m_tiles >= 0 && m_tile_size >= 0, "m_tiles and m_tile_size must be >= 0");
+            const int m = m_tiles * m_tile_size;
+            require(mean != nullptr || m == 0, "mean output must not be NULL");
+            DeviceGuard guard(gp->device);
+            upload_hyper(gp, hyper, gp->stream);
+            upload_test(gp, test_in, n_test_in, m);
+            gp->mean.ensure(std::max(m, 1));
+            factor(gp, gp->stream);
+            solve_alpha(gp, gp->stream);
+            predict_device(gp, gp->xt.ptr, m, gp->mean.ptr, nullptr, gp->stream);
+            download(gp, mean, gp->mean.ptr, m);
+            finish_and_check(gp);
+        });
+}
+
+static int predict_var_common(gprat_cu_gp *gp, const double hyper[3], const double *test_in, int64_t n_test_in,
+                              int m_tiles, int m_tile_size, double *mean, double *var)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(m_tiles >= 0 && m_tile_size >= 0, "m_tiles and m_tile_size must be >= 0");
+            const int m = m_tiles * m_tile_size;
+            require((mean != nullptr && var != nullptr) || m == 0, "outputs must not be NULL");
+            DeviceGuard guard(gp->device);
+            upload_hyper(gp, hyper, gp->stream);
+            upload_test(gp, test_in, n_test_in, m);
+            gp->mean.ensure(std::max(m, 1));
+            gp->var.ensure(std::max(m, 1));
+            factor(gp, gp->stream);
+            solve_alpha(gp, gp->stream);
+            predict_device(gp, gp->xt.ptr, m, gp->mean.ptr, gp->var.ptr, gp->stream);
+            download(gp, mean, gp->mean.ptr, m);
+            download(gp, var, gp->var.ptr, m);
+            finish_and_check(gp);
+        });
+}
+
+int gprat_cu_predict_with_uncertainty(gprat_cu_gp *gp, const double hyper[3], const double *test_in,
+                                      int64_t n_test_in, int m_tiles, int m_tile_size, double *mean, double *var)
+{
+    return predict_var_common(gp, hyper, test_in, n_test_in, m_tiles, m_tile_size, mean, var);
+}
+
+int gprat_cu_predict_with_full_cov(gprat_cu_gp *gp, const double hyper[3], const double *test_in, int64_t n_test_in,
+                                   int m_tiles, int m_tile_size, double *mean, double *var)
+{
+    return predict_var_common(gp, hyper, test_in, n_test_in, m_tiles, m_tile_size, mean, var);
+}
+
+int gprat_cu_predict_full_covariance(gprat_cu_gp *gp, const double hyper[3], const double *test_in,
+                                     int64_t n_test_in, int m, double *mean, double *cov)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(m >= 0, "m must be >= 0");
+            require((mean != nullptr && cov != nullptr) || m == 0, "outputs must not be NULL");
+            DeviceGuard guard(gp->device);
+            upload_hyper(gp, hyper, gp->stream);
+            upload_test(gp, test_in, n_test_in, m);
+            if (m == 0)
+            {
+                finish_and_check(gp);
+                return;
+            }
+            gp->mean.ensure(m);
+            gp->var.ensure(m);
+            factor(gp, gp->stream);
+            solve_alpha(gp, gp->stream);
+            predict_device(gp, gp->xt.ptr, m, gp->mean.ptr, gp->var.ptr, gp->stream);
+            // Sigma = K** - W W^T  (W = K* L^-T, m x n, left in gp->W)
+            const int64_t lds = round_up(m, 8);
+            DevBuf<double> S;
+            S.ensure(static_cast<int64_t>(m) * lds);
+            assemble_prior(gp->xt.ptr, m, gp->d, gp->params.ptr, S.ptr, lds, gp->stream);
+            GemmArgs a{};
+            a.M = m;
+            a.N = m;
+            a.K = gp->n;
+            a.A = gp->W.ptr;
+            a.lda = gp->ld;
+            a.transA = false;
+            a.B = gp->W.ptr;
+            a.ldb = gp->ld;
+            a.transB = true;
+            a.C = S.ptr;
+            a.ldc = lds;
+            a.alpha = -1.0;
+            a.beta = 1.0;
+            dgemm(a, gp->stream);
+            download(gp, mean, gp->mean.ptr, m);
+            GPRAT_CUDA_CHECK(cudaMemcpy2DAsync(cov, m * sizeof(double), S.ptr, lds * sizeof(double),
+                                               m * sizeof(double), m, cudaMemcpyDeviceToHost, gp->stream));
+            finish_and_check(gp);
+            S.release();
+        });
+}
+
+int gprat_cu_compute_loss(gprat_cu_gp *gp, const double hyper[3], double *loss)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(loss != nullptr, "loss must not be NULL");
+            DeviceGuard guard(gp->device);
+            upload_hyper(gp, hyper, gp->stream);
+            factor(gp, gp->stream);
+            solve_alpha(gp, gp->stream);
+            loss_kernel(gp->y.ptr, gp->alpha.ptr, gp->K.ptr, gp->ld, gp->n, gp->params.ptr, gp->stream);
+            GPRAT_CUDA_CHECK(cudaMemcpyAsync(gp->h_params, gp->params.ptr, sizeof(DeviceParams),
+                                             cudaMemcpyDeviceToHost, gp->stream));
+            finish_and_check(gp);
+            *loss = gp->h_params->loss;
+        });
+}
+
+int gprat_cu_loss_grad(gprat_cu_gp *gp, const double hyper[3], double *loss, double grad[3])
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(loss != nullptr && grad != nullptr, "outputs must not be NULL");
+            DeviceGuard guard(gp->device);
+            upload_hyper(gp, hyper, gp->stream);
+            gradient_device(gp, false, gp->stream);
+            GPRAT_CUDA_CHECK(cudaMemcpyAsync(gp->h_params, gp->params.ptr, sizeof(DeviceParams),
+                                             cudaMemcpyDeviceToHost, gp->stream));
+            finish_and_check(gp);
+            *loss = gp->h_params->loss;
+            for (int q = 0; q < 3; ++q)
+            {
+                grad[q] = gp->h_params->grad[q];
+            }
+        });
+}
+
+static void upload_opt_state(gprat_cu_gp *gp, const double params[9], const double adam[4], const int trainable[3],
+                             int iter)
+{
+    require(params != nullptr && adam != nullptr && trainable != nullptr, "optimiser arguments must not be NULL");
+    require(iter >= 0, "iter must be >= 0");
+    DeviceParams v;
+    std::memset(&v, 0, sizeof(v));
+    for (int q = 0; q < 3; ++q)
+    {
+        v.hyper[q] = params[q];
+        v.m_T[q] = params[3 + q];
+        v.w_T[q] = params[6 + q];
+        v.trainable[q] = trainable[q] != 0;
+    }
+    for (int q = 0; q < 4; ++q)
+    {
+        v.adam[q] = adam[q];
+    }
+    v.iter = iter;
+    set_params(gp->params.ptr, v, gp->stream);
+    GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->status.ptr, 0, sizeof(DeviceStatus), gp->stream));
+}
+
+static void download_opt_state(gprat_cu_gp *gp, double params[9])
+{
+    GPRAT_CUDA_CHECK(
+        cudaMemcpyAsync(gp->h_params, gp->params.ptr, sizeof(DeviceParams), cudaMemcpyDeviceToHost, gp->stream));
+    finish_and_check(gp);
+    for (int q = 0; q < 3; ++q)
+    {
+        params[q] = gp->h_params->hyper[q];
+        params[3 + q] = gp->h_params->m_T[q];
+        params[6 + q] = gp->h_params->w_T[q];
+    }
+}
+
+int gprat_cu_optimize_step(gprat_cu_gp *gp, double params[9], const double adam[4], const int trainable[3], int iter,
+                           double *loss)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(loss != nullptr, "loss must not be NULL");
+            DeviceGuard guard(gp->device);
+            upload_opt_state(gp, params, adam, trainable, iter);
+            gradient_device(gp, true, gp->stream);
+            download_opt_state(gp, params);
+            *loss = gp->h_params->loss;
+        });
+}
+
+int gprat_cu_optimize(gprat_cu_gp *gp, double params[9], const double adam[4], const int trainable[3], int opt_iter,
+                      double *losses)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(opt_iter >= 0, "opt_iter must be >= 0");
+            require(losses != nullptr || opt_iter == 0, "losses must not be NULL");
+            DeviceGuard guard(gp->device);
+            upload_opt_state(gp, params, adam, trainable, 0);
+            gp->losses.ensure(std::max(opt_iter, 1));
+            for (int it = 0; it < opt_iter; ++it)
+            {
+                gradient_device(gp, true, gp->stream);
+                GPRAT_CUDA_CHECK(cudaMemcpyAsync(gp->losses.ptr + it, &gp->params.ptr->loss, sizeof(double),
+                                                 cudaMemcpyDeviceToDevice, gp->stream));
+            }
+            download(gp, losses, gp->losses.ptr, opt_iter);
+            download_opt_state(gp, params);
+        });
+}
+
+int gprat_cu_fit_predict_device(gprat_cu_gp *gp, const double hyper[3], const double *d_test_in, int64_t n_test_in,
+                                int m, double *d_mean, double *d_var, void *stream)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(m >= 0, "m must be >= 0");
+            require(d_test_in != nullptr && d_mean != nullptr, "device buffers must not be NULL");
+            require(n_test_in >= static_cast<int64_t>(m) + gp->d - 1, "test series too short for the sliding window");
+            DeviceGuard guard(gp->device);
+            cudaStream_t s = stream != nullptr ? static_cast<cudaStream_t>(stream) : gp->stream;
+            upload_hyper(gp, hyper, s);
+            factor(gp, s);
+            solve_alpha(gp, s);
+            predict_device(gp, d_test_in, m, d_mean, d_var, s);
+        });
+}
+
+int gprat_cu_check_status(gprat_cu_gp *gp)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            DeviceGuard guard(gp->device);
+            GPRAT_CUDA_CHECK(cudaDeviceSynchronize());
+            finish_and_check(gp);
+        });
+}
+
+}  // extern "C"

@@ -1,0 +1,210 @@
+/*
+ * gprat_cu.h — C ABI of the B200 (sm_100a) GP-regression library
+ * libgprat_cuda.so.  Plain pointers and sizes; no C++ or torch types.
+ *
+ * One opaque handle (gprat_cu_gp) owns a device-resident copy of the
+ * training series and outputs plus the device workspace for one GP.  Every
+ * reference-facing call below takes HOST buffers, runs the whole pipeline on
+ * the GPU (one CUDA stream per handle) and returns after the results are back
+ * in the caller's buffers.  Calls on one handle are serialised by the
+ * caller; different handles may be used from different threads.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   gpu::predict / predict_with_uncertainty / predict_with_full_cov /
+ *   compute_loss / optimize / optimize_step / cholesky
+ *   (core/include/gpu/gp_functions.cuh:27-199, core/src/gpu/gp_functions.cu:17-467)
+ *   and their CPU twins cpu::* (core/src/cpu/gp_functions.cpp:18-1269), which
+ *   gprat::GP dispatches to (core/src/gprat_c.cpp:106-361).
+ *
+ * Conventions (identical to the reference):
+ *   - training input is a 1-D series; feature row i is in[i .. i+n_reg-1]
+ *     (core/src/cpu/gp_algorithms.cpp:22-26), so n_in >= n_tiles*n_tile_size
+ *     + n_reg - 1;
+ *   - hyper = {lengthscale, vertical_lengthscale, noise_variance}
+ *     (core/include/gp_kernels.hpp:14-39);
+ *   - test size m = m_tiles * m_tile_size (utils::compute_test_tiles,
+ *     core/src/utils_c.cpp:34-52, is the caller's business).
+ *
+ * Status codes: every function returns GPRAT_CU_OK (0) or one of the codes
+ * below; gprat_cu_last_error() returns a thread-local message for the last
+ * failure on the calling thread.
+ */
+#ifndef GPRAT_CU_H
+#define GPRAT_CU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPRAT_CU_OK 0
+#define GPRAT_CU_ERR_INVALID_ARG 1
+#define GPRAT_CU_ERR_OOM 2
+#define GPRAT_CU_ERR_NOT_SPD 3 /* Cholesky met a non-positive pivot */
+#define GPRAT_CU_ERR_CUDA 4
+#define GPRAT_CU_ERR_TIMEOUT 5 /* a bounded device wait gave up */
+#define GPRAT_CU_ERR_NO_DEVICE 6
+
+/* Precision of the factorisation and of the variance solve. */
+#define GPRAT_CU_PREC_FP64 0       /* all FP64 (DMMA tensor cores) */
+#define GPRAT_CU_PREC_MIXED_TF32 1 /* FP32 storage, TF32 tcgen05 trailing updates, FP64 diagonal */
+#define GPRAT_CU_PREC_MIXED_BF16 2 /* FP32 storage, BF16 tcgen05 trailing updates, FP64 diagonal */
+
+typedef struct gprat_cu_gp gprat_cu_gp;
+
+/* Thread-local text of the last error on this thread ("" if none). */
+const char *gprat_cu_last_error(void);
+
+/* Number of CUDA devices (gprat::gpu_count, core/src/target.cpp:143-155). */
+int gprat_cu_device_count(int *count);
+
+/* Library build identification, e.g. "gprat_cu sm_100a". */
+const char *gprat_cu_version(void);
+
+/*
+ * Creates a GP on `device`: copies the training series (n_in doubles) and
+ * outputs (n_out >= n_tiles*n_tile_size doubles) to HBM.  Replaces the
+ * per-call host->device copies of gpu::predict* (core/src/gpu/gp_functions.cu:114-116)
+ * and the state kept by gprat::GP (core/include/gprat_c.hpp:56-87).
+ */
+int gprat_cu_gp_create(int device,
+                       const double *train_in,
+                       int64_t n_in,
+                       const double *train_out,
+                       int64_t n_out,
+                       int n_tiles,
+                       int n_tile_size,
+                       int n_regressors,
+                       gprat_cu_gp **out);
+
+int gprat_cu_gp_destroy(gprat_cu_gp *gp);
+
+/* Selects GPRAT_CU_PREC_* for subsequent calls (default FP64). */
+int gprat_cu_gp_set_precision(gprat_cu_gp *gp, int precision);
+
+/*
+ * Tiled Cholesky factor (gprat::GP::cholesky, core/src/gprat_c.cpp:336-361;
+ * cpu::cholesky core/src/cpu/gp_functions.cpp:18-78).  Writes n_tiles^2
+ * row-major tiles of n_tile_size^2 doubles, tile (i,j) at offset
+ * (i*n_tiles+j)*n_tile_size^2.  Lower tiles hold L; diagonal tiles keep K's
+ * strict upper triangle (as LAPACKE dpotrf2('L') does); upper tiles are zero
+ * (the reference returns them empty).
+ */
+int gprat_cu_cholesky(gprat_cu_gp *gp, const double hyper[3], double *tiles_out);
+
+/* Predictive mean (gprat::GP::predict, core/src/gprat_c.cpp:106-154). */
+int gprat_cu_predict(gprat_cu_gp *gp,
+                     const double hyper[3],
+                     const double *test_in,
+                     int64_t n_test_in,
+                     int m_tiles,
+                     int m_tile_size,
+                     double *mean);
+
+/* Mean and per-point posterior variance
+ * (gprat::GP::predict_with_uncertainty, core/src/gprat_c.cpp:156-203). */
+int gprat_cu_predict_with_uncertainty(gprat_cu_gp *gp,
+                                      const double hyper[3],
+                                      const double *test_in,
+                                      int64_t n_test_in,
+                                      int m_tiles,
+                                      int m_tile_size,
+                                      double *mean,
+                                      double *var);
+
+/* gprat::GP::predict_with_full_cov (core/src/gprat_c.cpp:206-253): the
+ * reference forms K** - V^T V and returns its diagonal; same outputs. */
+int gprat_cu_predict_with_full_cov(gprat_cu_gp *gp,
+                                   const double hyper[3],
+                                   const double *test_in,
+                                   int64_t n_test_in,
+                                   int m_tiles,
+                                   int m_tile_size,
+                                   double *mean,
+                                   double *var);
+
+/* Full m x m posterior covariance K** - K*^T K^-1 K* (row-major, both
+ * triangles).  No counterpart in the reference, which discards all but the
+ * diagonal (core/src/cpu/gp_functions.cpp:663-676). */
+int gprat_cu_predict_full_covariance(gprat_cu_gp *gp,
+                                     const double hyper[3],
+                                     const double *test_in,
+                                     int64_t n_test_in,
+                                     int m,
+                                     double *mean,
+                                     double *cov);
+
+/* Mean negative log marginal likelihood 0.5*(y^T a + sum log L_ii^2 + N log 2pi)/N
+ * (gprat::GP::calculate_loss, core/src/gprat_c.cpp:306-334). */
+int gprat_cu_compute_loss(gprat_cu_gp *gp, const double hyper[3], double *loss);
+
+/* Loss and its gradient w.r.t. the softplus-unconstrained hyper-parameters,
+ * scaled like the reference's update_hyperparameter_tiled
+ * (core/src/cpu/tiled_algorithms.cpp:296-426):
+ *   g = sigmoid(u) * 0.5/N * (tr(K^-1 dK/dtheta) - a^T dK/dtheta a). */
+int gprat_cu_loss_grad(gprat_cu_gp *gp, const double hyper[3], double *loss, double grad[3]);
+
+/*
+ * One Adam step (gprat::GP::optimize_step, core/src/gprat_c.cpp:280-301;
+ * cpu::optimize_step core/src/cpu/gp_functions.cpp:1032-1269).
+ * params[9] = {lengthscale, vertical_lengthscale, noise_variance, m_T[3], w_T[3]}
+ * is read and updated in place; adam[4] = {learning_rate, beta1, beta2, epsilon};
+ * trainable[3] flags; returns the loss at the pre-step parameters.
+ */
+int gprat_cu_optimize_step(gprat_cu_gp *gp,
+                           double params[9],
+                           const double adam[4],
+                           const int trainable[3],
+                           int iter,
+                           double *loss);
+
+/* opt_iter Adam steps with iter = 0..opt_iter-1 (gprat::GP::optimize,
+ * core/src/gprat_c.cpp:255-278); losses[opt_iter] receives each step's loss. */
+int gprat_cu_optimize(gprat_cu_gp *gp,
+                      double params[9],
+                      const double adam[4],
+                      const int trainable[3],
+                      int opt_iter,
+                      double *losses);
+
+/*
+ * Device-resident fit + predict: assembly, Cholesky, alpha, mean and
+ * variance with the test series, mean and var already in HBM on the same
+ * device (d_var may be NULL for mean only).  Enqueued on `stream`
+ * (a cudaStream_t; NULL = the handle's own stream); returns without
+ * synchronising.  No counterpart in the reference (whose calls always copy
+ * from and to the host).
+ */
+int gprat_cu_fit_predict_device(gprat_cu_gp *gp,
+                                const double hyper[3],
+                                const double *d_test_in,
+                                int64_t n_test_in,
+                                int m,
+                                double *d_mean,
+                                double *d_var,
+                                void *stream);
+
+/* Checks the device status word after a device-resident call (non-SPD
+ * pivot, timeouts); synchronises the handle's stream. */
+int gprat_cu_check_status(gprat_cu_gp *gp);
+
+/*
+ * Instrumentation (no counterpart in the reference; the reference times
+ * phases with APEX, core/include/apex_utils.hpp:24-54).  Process-wide
+ * counters: every kernel launch of this library increments `launches`.
+ * With timing enabled, each FP64 tensor-core GEMM launch is bracketed by
+ * CUDA events on its own stream; gprat_cu_stats_read synchronises those
+ * events and returns the launch count, their summed device time (ms) and
+ * their algorithmic FLOPs (2*M*N*K, lower-triangular updates counted as
+ * the lower triangle only).
+ */
+int gprat_cu_stats_reset(void);
+int gprat_cu_stats_enable_timing(int enable);
+int gprat_cu_stats_read(int64_t *launches, int64_t *gemm_launches, double *gemm_ms, double *gemm_flops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPRAT_CU_H */

@@ -1,0 +1,101 @@
+"""Generates the golden fixtures under tests/golden/ (run in a container that
+has the reference tree and the compiled reference, oracle/_ref):
+
+    make -C oracle REF=/root/reference && python tests/golden/make_golden.py
+
+1. data_1024_n128.json: the reference's own known-answer test
+   (test/src/output_correctness.cpp:60-247): the first 128 values of
+   data/data_1024/{training_input,training_output,test_input}.txt and the
+   expected results of data/data_1024/output.json.
+2. ref_cases.npz: outputs of the reference's CPU code (compiled from source,
+   oracle/_ref) on seeded synthetic inputs: a 1024-point case with 64-wide
+   tiles, a ragged test set, a 64-regressor case, and 5 Adam steps with the
+   gradient at every step.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import gprat_oracle as O  # noqa: E402
+from oracle import ref  # noqa: E402
+
+REF = os.environ.get("GPRAT_REFERENCE", "/root/reference")
+
+
+def known_answer():
+    d = os.path.join(REF, "data", "data_1024")
+    raw = {}
+    for name in ("training_input", "training_output", "test_input"):
+        raw[name] = np.loadtxt(os.path.join(d, name + ".txt"), max_rows=128).tolist()
+    with open(os.path.join(d, "output.json")) as f:
+        expected = json.load(f)
+    out = {
+        "source": "reference data/data_1024 + output.json; config of test/src/output_correctness.cpp:60-71",
+        "n_train": 128, "n_test": 128, "n_tiles": 4, "n_reg": 8, "kernel_params": [1.0, 1.0, 0.1],
+        "adam": [0.1, 0.9, 0.999, 1e-8, 3],
+        "raw": raw,
+        "expected": expected,
+    }
+    with open(os.path.join(HERE, "data_1024_n128.json"), "w") as f:
+        json.dump(out, f)
+
+
+def case_predict(tag, n, m, d, T, hyper, store):
+    x, y, xt = O.synthetic(n, m, d)
+    nt = n // T
+    mt, mts = ref.compute_test_tiles(m, nt, T)
+    gp = ref.RefGP(x, y, nt, T, d, hyper)
+    mean, var = gp.predict_with_uncertainty(xt, mt, mts)
+    fmean, fvar = gp.predict_with_full_cov(xt, mt, mts)
+    pmean = gp.predict(xt, mt, mts)
+    loss = gp.calculate_loss()
+    tiles = gp.cholesky()
+    chk = np.array([t.sum() if t is not None else np.nan for t in tiles])
+    store.update({
+        f"{tag}_cfg": np.array([n, m, d, T, mt, mts], dtype=np.int64),
+        f"{tag}_hyper": np.array(hyper),
+        f"{tag}_mean": mean, f"{tag}_var": var, f"{tag}_full_mean": fmean, f"{tag}_full_var": fvar,
+        f"{tag}_pred": pmean, f"{tag}_loss": np.array([loss]),
+        f"{tag}_tile_sums": chk,
+        f"{tag}_tile_last": tiles[nt * nt - 1],
+        f"{tag}_tile_0": tiles[0],
+        f"{tag}_tile_10": tiles[nt],
+    })
+
+
+def case_optimize(store):
+    n, d, T = 256, 8, 64
+    x, y, _ = O.synthetic(n, 16, d)
+    gp = ref.RefGP(x, y, n // T, T, d, (0.5, 2.0, 0.5))
+    losses, params, grads = [], [], []
+    for it in range(5):
+        grads.append(gp.gradient(0.1, 0.9, 0.999, 1e-8))
+        losses.append(gp.optimize_step(it, 0.1, 0.9, 0.999, 1e-8))
+        params.append(gp.get_params())
+    store.update({
+        "opt_cfg": np.array([n, d, T], dtype=np.int64),
+        "opt_losses": np.array(losses), "opt_params": np.array(params), "opt_grads": np.array(grads),
+    })
+
+
+def main():
+    ref.start()
+    known_answer()
+    store = {}
+    case_predict("c0", 1024, 1024, 8, 64, (1.0, 1.0, 0.1), store)
+    case_predict("ragged", 256, 200, 8, 64, (1.0, 1.0, 0.1), store)
+    case_predict("d64", 512, 256, 64, 128, (4.0, 1.0, 0.01), store)
+    case_optimize(store)
+    np.savez_compressed(os.path.join(HERE, "ref_cases.npz"), **store)
+
+
+if __name__ == "__main__":
+    main()
