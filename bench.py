@@ -254,6 +254,10 @@ def run_ours(args, wl):
 
     mean_h, var_h = dmean.cpu().numpy(), dvar.cpu().numpy()
     sane = bool(np.all(np.isfinite(mean_h)) and np.all(var_h > 0) and np.all(var_h <= hyper[1] + 1e-12))
+    if args.profile:
+        print(json.dumps({"profile_run": True, "ms_per_step": ms_per_step, "gpu_launches": int(stats["launches"]),
+                          "sanity": sane}), flush=True)
+        return
 
     # end-to-end through the C ABI with host buffers (H2D of the test series,
     # D2H of mean and variance inside every call)
@@ -332,6 +336,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
     ap.add_argument("--precision", choices=["fp64", "mixed-tf32", "mixed-bf16"], default="fp64")
+    ap.add_argument("--profile", action="store_true",
+                    help="device steps only (no CPU sample, e2e loop or peak measurement): for ncu captures")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
