@@ -397,6 +397,12 @@ void check_gp(gprat_cu_gp *gp) { require(gp != nullptr, "GP handle is NULL"); }
 
 }  // namespace
 
+namespace gprat_cu
+{
+// Lets other entry points of the library report through gprat_cu_last_error().
+void set_last_error(const std::string &message) { g_last_error = message; }
+}  // namespace gprat_cu
+
 extern "C" {
 
 const char *gprat_cu_last_error(void) { return g_last_error.c_str(); }

@@ -190,6 +190,35 @@ int gprat_cu_fit_predict_device(gprat_cu_gp *gp,
 int gprat_cu_check_status(gprat_cu_gp *gp);
 
 /*
+ * Loss without any memory allocation.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc -- code running under an allocator
+ * or memory pool it does not own, or a latency-critical loop that must not
+ * enter the driver's allocator (which can synchronise the device) -- this
+ * computes the same value as gprat_cu_compute_loss from caller-owned DEVICE
+ * buffers: the training series (n_in doubles), the outputs (n_out doubles)
+ * and the result (one double at d_loss), on `stream` (a cudaStream_t; NULL =
+ * the default stream); it returns after synchronising that stream.
+ * hyper[3] is a host array.  All scratch lives in one fixed device array of
+ * the library (about 9.4 MB per GPU that loads the library, held until the
+ * process exits), so n_tiles * n_tile_size is limited to 1024; larger
+ * problems return GPRAT_CU_ERR_INVALID_ARG.  The array is shared by every
+ * call and keeps the last call's contents: calls that overlap on the GPU
+ * race.  The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress, once per device); make it before any stream capture.
+ */
+int gprat_cu_compute_loss_noalloc(int device,
+                                  const double *d_train_in,
+                                  int64_t n_in,
+                                  const double *d_train_out,
+                                  int64_t n_out,
+                                  int n_tiles,
+                                  int n_tile_size,
+                                  int n_regressors,
+                                  const double hyper[3],
+                                  double *d_loss,
+                                  void *stream);
+
+/*
  * Instrumentation (no counterpart in the reference; the reference times
  * phases with APEX, core/include/apex_utils.hpp:24-54).  Process-wide
  * counters: every kernel launch of this library increments `launches`.
