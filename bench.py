@@ -280,7 +280,7 @@ def run_ours(args, wl):
     fp64_peak = measure_fp64_gemm_peak(torch, device)
     gemm_tflops = stats["gemm_flops"] / (stats["gemm_ms"] / 1e3) / 1e12 if stats["gemm_ms"] > 0 else None
     step_flops = algorithmic_flops(n, m)
-    if world == 1:
+    if world == 1 and not args.skip_cpu_baseline:
         sample_s, scale, desc, threads = cpu_reference_sample(wl, 3)
         cpu = {"value": sample_s * scale, "unit": "s", "cores": threads, "kind": "reference", "sample": desc}
     else:
@@ -336,6 +336,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
     ap.add_argument("--precision", choices=["fp64", "mixed-tf32", "mixed-bf16"], default="fp64")
+    ap.add_argument("--skip-cpu-baseline", action="store_true",
+                    help="omit the CPU reference sample (cpu_baseline becomes null)")
     ap.add_argument("--profile", action="store_true",
                     help="device steps only (no CPU sample, e2e loop or peak measurement): for ncu captures")
     args = ap.parse_args()

@@ -85,12 +85,12 @@ def build_host(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(LIB, exist_ok=True)
     sources = sorted(glob.glob(os.path.join(CPP, "*.cpp")))
     sources = [s for s in sources if not os.path.basename(s).startswith("py_")]
-    headers = sorted(glob.glob(os.path.join(CPP, "*.hpp")) + glob.glob(os.path.join(INCLUDE, "*.h")))
+    headers = sorted(glob.glob(os.path.join(INCLUDE, "gprat", "*.hpp")) + glob.glob(os.path.join(INCLUDE, "*.h")))
     if not sources:
         return HOST_LIB
     if not force and not _stale(HOST_LIB, sources + headers + [CUDA_LIB, __file__]):
         return HOST_LIB
-    cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-I", INCLUDE, "-I", CPP, "-I",
+    cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-I", INCLUDE, "-I", os.path.join(INCLUDE, "gprat"), "-I", CPP, "-I",
            os.path.join(CUDA_HOME, "include"), *sources, "-o", HOST_LIB, "-L", LIB, "-lgprat_cuda",
            "-Wl,-rpath,$ORIGIN", "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart", "-pthread"]
     _run(cmd, verbose)
@@ -102,13 +102,13 @@ def build_python(verbose: bool = False, force: bool = False) -> str:
     import pybind11
 
     sources = sorted(glob.glob(os.path.join(CPP, "py_*.cpp")))
-    headers = sorted(glob.glob(os.path.join(CPP, "*.hpp")))
+    headers = sorted(glob.glob(os.path.join(INCLUDE, "gprat", "*.hpp")))
     if not sources:
         return PY_MODULE
     if not force and not _stale(PY_MODULE, sources + headers + [HOST_LIB, __file__]):
         return PY_MODULE
     py_inc = sysconfig.get_paths()["include"]
-    cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-I", INCLUDE, "-I", CPP, "-I", pybind11.get_include(),
+    cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-I", INCLUDE, "-I", os.path.join(INCLUDE, "gprat"), "-I", CPP, "-I", pybind11.get_include(),
            "-I", py_inc, *sources, "-o", PY_MODULE, "-L", LIB, "-lgprat", "-lgprat_cuda", "-Wl,-rpath,$ORIGIN/lib",
            "-pthread"]
     _run(cmd, verbose)

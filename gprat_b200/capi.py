@@ -71,6 +71,9 @@ def _load() -> ctypes.CDLL:
     lib.gprat_cu_check_status.argtypes = [ctypes.c_void_p]
     lib.gprat_cu_stats_enable_timing.argtypes = [ctypes.c_int]
     lib.gprat_cu_stats_read.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _dp, _dp]
+    _fp = ctypes.POINTER(ctypes.c_float)
+    lib.gprat_cu_test_tc_gemm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _fp, _i64, _fp,
+                                          _i64, _fp, _i64, ctypes.c_float, ctypes.c_float, ctypes.c_int, _dp]
     return lib
 
 
@@ -113,6 +116,22 @@ def stats_read() -> dict:
     c, d = ctypes.c_double(), ctypes.c_double()
     check(lib.gprat_cu_stats_read(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)))
     return {"launches": a.value, "gemm_launches": b.value, "gemm_ms": c.value, "gemm_flops": d.value}
+
+
+def test_tc_gemm(kind: int, A: np.ndarray, B: np.ndarray, C: np.ndarray, alpha: float, beta: float,
+                 lower: bool = False, rowsq: Optional[np.ndarray] = None) -> None:
+    """Runs the tcgen05 GEMM C = beta*C + alpha*A B^T in place on float32 arrays
+    (kind 0 = TF32, 1 = BF16)."""
+    _fp = ctypes.POINTER(ctypes.c_float)
+    for a in (A, B, C):
+        if a.dtype != np.float32 or not a.flags.c_contiguous:
+            raise ValueError("A, B and C must be C-contiguous float32 arrays")
+    M, K = A.shape
+    N = B.shape[0]
+    rp = rowsq.ctypes.data_as(_dp) if rowsq is not None else None
+    check(lib.gprat_cu_test_tc_gemm(int(kind), M, N, K, A.ctypes.data_as(_fp), K, B.ctypes.data_as(_fp), K,
+                                    C.ctypes.data_as(_fp), C.shape[1], float(alpha), float(beta), int(bool(lower)),
+                                    rp))
 
 
 def _arr(a) -> np.ndarray:

@@ -50,7 +50,7 @@ __device__ __forceinline__ void distances(const double *xr, const double *xc, in
 
 // mode 0: K (lower tiles of size T incl. full diagonal tiles, + noise on the
 //         global diagonal); mode 1: cross / prior (all entries, no noise).
-template <int MODE>
+template <int MODE, typename OutT>
 __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
                                                int rows,
                                                const double *__restrict__ xcol,
@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
                                                int d,
                                                int T,
                                                const DeviceParams *__restrict__ p,
-                                               double *__restrict__ out,
+                                               OutT *__restrict__ out,
                                                int64_t ldo,
                                                const double *__restrict__ alpha,
                                                double *__restrict__ mean_partial,
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
             }
             if (inside && out != nullptr)
             {
-                out[static_cast<int64_t>(gi) * ldo + gj] = val;
+                out[static_cast<int64_t>(gi) * ldo + gj] = static_cast<OutT>(val);
             }
             if (mean_partial != nullptr)
             {
@@ -173,9 +173,9 @@ __global__ void reduce_rows_kernel(const double *__restrict__ part, int m, int p
 
 size_t se_smem(int d) { return static_cast<size_t>(AR + d + AC + d + AR * (AC / 32)) * sizeof(double); }
 
-template <int MODE>
+template <int MODE, typename OutT>
 void launch_se(const double *xrow, int rows, const double *xcol, int cols, int d, int T, const DeviceParams *p,
-               double *out, int64_t ldo, const double *alpha, double *mean_partial, int parts, cudaStream_t s)
+               OutT *out, int64_t ldo, const double *alpha, double *mean_partial, int parts, cudaStream_t s)
 {
     if (rows <= 0 || cols <= 0)
     {
@@ -188,10 +188,11 @@ void launch_se(const double *xrow, int rows, const double *xcol, int cols, int d
     }
     if (smem > 48 * 1024)
     {
-        ensure_smem_attr(reinterpret_cast<const void *>(se_kernel<MODE>), static_cast<int>(smem));
+        ensure_smem_attr(reinterpret_cast<const void *>(se_kernel<MODE, OutT>), static_cast<int>(smem));
     }
     dim3 grid(ceil_div(cols, AC), ceil_div(rows, AR));
-    se_kernel<MODE><<<grid, AC, smem, s>>>(xrow, rows, xcol, cols, d, T, p, out, ldo, alpha, mean_partial, parts);
+    se_kernel<MODE, OutT><<<grid, AC, smem, s>>>(xrow, rows, xcol, cols, d, T, p, out, ldo, alpha, mean_partial,
+                                                 parts);
     GPRAT_LAUNCH_CHECK();
 }
 
@@ -205,6 +206,16 @@ void assemble_covariance(const double *x, int n, int n_reg, int tile, const Devi
 
 void assemble_cross(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, double *Kx,
                     int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s)
+{
+    if (mean_partial != nullptr && mean_parts != ceil_div(n, AC))
+    {
+        throw Error(1, "assemble_cross: mean_parts must be ceil(n/128)");
+    }
+    launch_se<1>(xt, m, x, n, n_reg, 1, p, Kx, ldx, alpha, mean_partial, mean_parts, s);
+}
+
+void assemble_cross_f32(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, float *Kx,
+                        int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s)
 {
     if (mean_partial != nullptr && mean_parts != ceil_div(n, AC))
     {

@@ -135,6 +135,9 @@ void assemble_covariance(const double *x, int n, int n_reg, int tile, const Devi
 // the matrix is not stored.
 void assemble_cross(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, double *Kx,
                     int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s);
+// Same with the matrix stored in FP32 (the mean partials stay FP64).
+void assemble_cross_f32(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, float *Kx,
+                        int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s);
 void reduce_mean(const double *mean_partial, int m, int parts, double *mean, cudaStream_t s);
 
 // Prior covariance matrix K**[r][c] = k(xt_r, xt_c) (gen_tile_full_prior_covariance,
@@ -154,6 +157,9 @@ void trsv_forward(const double *L, int64_t ldl, const double *Linv, int nb, int 
                   cudaStream_t s);
 void trsv_backward(const double *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, double *tmp,
                    cudaStream_t s);
+// Same with an FP32 factor (mixed precision); FP64 right-hand side and arithmetic.
+void trsv_forward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s);
+void trsv_backward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s);
 
 // Loss 0.5*(y.a + sum log(L_ii^2) + n log 2pi)/n -> p->loss.
 void loss_kernel(const double *y, const double *alpha, const double *L, int64_t ldl, int n, DeviceParams *p,

@@ -17,16 +17,24 @@ namespace
 
 using namespace gemm;
 
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(THREADS, 1) dgemm_kernel(GemmArgs a)
+template <int WN, bool TA, bool TB>
+__global__ void __launch_bounds__(Cfg<WN>::THREADS, Cfg<WN>::MIN_BLOCKS) dgemm_kernel(GemmArgs a)
 {
+    using C = Cfg<WN>;
     extern __shared__ __align__(16) double smem[];
-    TileCoord tc = tile_coord(a.lower);
+    const TileCoord tc = tile_coord<C::BM, C::BN>(a.lower);
     const int m0 = tc.m0, n0 = tc.n0;
-    Frag f = frag_coords();
+    if (n0 >= a.N || m0 >= a.M)
+    {
+        return;
+    }
+    const Frag f = frag_coords<WN>();
 
-    // Fused form: acc starts at C and A is negated when alpha == -1.
+    // Fused form (beta == 1, alpha == +-1): acc starts at alpha*C, the main
+    // loop accumulates +A*B, and the store multiplies by alpha again, so
+    // C_new = C + alpha*A*B without any per-fragment sign flips.
     const bool fused = (a.beta == 1.0) && (a.alpha == 1.0 || a.alpha == -1.0);
+    const double osign = (fused && a.alpha == -1.0) ? -1.0 : 1.0;
     double acc[4][4][4];
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
@@ -54,8 +62,8 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_kernel(GemmArgs a)
                         v0 = cp[0];
                     }
                 }
-                acc[mi][ni][2 * h] = v0;
-                acc[mi][ni][2 * h + 1] = v1;
+                acc[mi][ni][2 * h] = osign * v0;
+                acc[mi][ni][2 * h + 1] = osign * v1;
             }
         }
     }
@@ -65,7 +73,7 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_kernel(GemmArgs a)
     {
         k_begin = (max(m0, n0) / BK) * BK;
     }
-    mainloop<TA, TB>(a, m0, n0, smem, acc, fused && a.alpha == -1.0, k_begin, f);
+    mainloop<WN, TA, TB>(a, m0, n0, smem, acc, k_begin, f);
 
     // Epilogue: store (lower-only respected) and optional row sums of squares.
     double rs[4][2];
@@ -91,7 +99,7 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_kernel(GemmArgs a)
                     continue;
                 }
                 double *cp = a.C + static_cast<int64_t>(r) * a.ldc + c;
-                double v0 = acc[mi][ni][2 * h], v1 = acc[mi][ni][2 * h + 1];
+                double v0 = osign * acc[mi][ni][2 * h], v1 = osign * acc[mi][ni][2 * h + 1];
                 if (!fused)
                 {
                     double o0 = 0.0, o1 = 0.0;
@@ -133,8 +141,8 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_kernel(GemmArgs a)
 
     if (a.rowsq != nullptr)
     {
-        // rows of this CTA: reduce over the quad (t), then over the 4 N-warps.
-        double *red = smem;  // [BM][4], pipeline smem is free after mainloop
+        // rows of this CTA: reduce over the quad (t), then over the N-warps.
+        double *red = smem;  // [BM][WN], pipeline smem is free after mainloop
 #pragma unroll
         for (int mi = 0; mi < 4; ++mi)
         {
@@ -146,48 +154,67 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_kernel(GemmArgs a)
                 v += __shfl_xor_sync(0xffffffffu, v, 2);
                 if (f.t == 0)
                 {
-                    red[(f.wm * 64 + mi * 16 + f.g + h * 8) * 4 + f.wn] = v;
+                    red[(f.wm * 64 + mi * 16 + f.g + h * 8) * WN + f.wn] = v;
                 }
             }
         }
         __syncthreads();
-        for (int r = threadIdx.x; r < BM; r += THREADS)
+        for (int r = threadIdx.x; r < C::BM; r += C::THREADS)
         {
             int gr = m0 + r;
             if (gr < a.M)
             {
-                a.rowsq[gr] += ((red[r * 4 + 0] + red[r * 4 + 1]) + red[r * 4 + 2]) + red[r * 4 + 3];
+                double s = 0.0;
+#pragma unroll
+                for (int w = 0; w < WN; ++w)
+                {
+                    s += red[r * WN + w];
+                }
+                a.rowsq[gr] += s;
             }
         }
     }
 }
 
-template <bool TA, bool TB>
+template <int WN, bool TA, bool TB>
 void launch(const GemmArgs &a, cudaStream_t s)
 {
-    constexpr int smem = smem_bytes<TA, TB>();
-    ensure_smem_attr(reinterpret_cast<const void *>(dgemm_kernel<TA, TB>), smem);
+    using C = Cfg<WN>;
+    constexpr int smem = smem_bytes<WN, TA, TB>();
+    ensure_smem_attr(reinterpret_cast<const void *>(dgemm_kernel<WN, TA, TB>), smem);
     dim3 grid;
     if (a.lower)
     {
-        int t = ceil_div(a.M, BM);
-        grid = dim3(t * (t + 1) / 2, 1, 1);
+        grid = dim3(lower_grid<C::BM, C::BN>(a.M), 1, 1);
     }
     else
     {
-        grid = dim3(ceil_div(a.N, BN), ceil_div(a.M, BM), 1);
+        grid = dim3(ceil_div(a.N, C::BN), ceil_div(a.M, C::BM), 1);
     }
     const bool timed = gemm_timing_enabled();
     if (timed)
     {
         gemm_timing_begin(s);
     }
-    dgemm_kernel<TA, TB><<<grid, THREADS, smem, s>>>(a);
+    dgemm_kernel<WN, TA, TB><<<grid, C::THREADS, smem, s>>>(a);
     GPRAT_LAUNCH_CHECK();
     if (timed)
     {
         const double mn = a.lower ? 0.5 * static_cast<double>(a.M) * (a.M + 1) : static_cast<double>(a.M) * a.N;
         gemm_timing_end(s, 2.0 * mn * a.K);
+    }
+}
+
+template <int WN>
+void dispatch(const GemmArgs &a, cudaStream_t s)
+{
+    if (a.transA)
+    {
+        a.transB ? launch<WN, true, true>(a, s) : launch<WN, true, false>(a, s);
+    }
+    else
+    {
+        a.transB ? launch<WN, false, true>(a, s) : launch<WN, false, false>(a, s);
     }
 }
 
@@ -208,17 +235,20 @@ void dgemm(const GemmArgs &a, cudaStream_t s)
     {
         throw Error(1, "dgemm: lower mode needs M == N");
     }
-    if (a.rowsq != nullptr && (a.N > BN || a.lower))
+    if (a.rowsq != nullptr && (a.N > 128 || a.lower))
     {
         throw Error(1, "dgemm: rowsq needs N <= 128 and full tiles");
     }
-    if (a.transA)
+    // N <= 128: one CTA column covers every output column, which the in-place
+    // panel solves and the fused row sums rely on.  Wider problems use the
+    // 2-CTA/SM shape.
+    if (a.N <= 128)
     {
-        a.transB ? launch<true, true>(a, s) : launch<true, false>(a, s);
+        dispatch<4>(a, s);
     }
     else
     {
-        a.transB ? launch<false, true>(a, s) : launch<false, false>(a, s);
+        dispatch<2>(a, s);
     }
 }
 

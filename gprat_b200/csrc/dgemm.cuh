@@ -1,56 +1,70 @@
 // FP64 tensor-core (DMMA, mma.sync m16n8k8 .f64) GEMM mainloop for sm_100a.
 //
-// CTA tile 128x128, K step 16, 4-stage cp.async pipeline, 8 warps laid out
-// 2 (M) x 4 (N), warp tile 64x32 = 4x4 m16n8k8 fragments.  Shared-memory
-// rows are padded so that every fragment load is conflict-free (row stride
-// = 4 mod 16 doubles when K is the contiguous index, 8 mod 16 when M/N is).
-// The epilogue is a template parameter: plain C update (dgemm.cu) or the
-// fused adjoint trace (optimizer.cu).
+// Two CTA shapes share one mainloop (template parameter WN = warps along N):
+//   WN = 4: CTA tile 128x128, 8 warps, 4-stage pipeline, 1 CTA/SM.  Used
+//           when N <= 128 (panel solves, in-place diagonal-block steps).
+//   WN = 2: CTA tile 128x64, 4 warps, 3-stage pipeline, 2 CTAs/SM, so one
+//           CTA's C load/store overlaps the other CTA's DMMA main loop.
+//           Used for the large trailing updates.
+// Warp tile 64x32 = 4x4 m16n8k8 fragments (64 FP64 accumulators/thread).
+// K step 16 via cp.async.  Shared-memory rows are padded so every fragment
+// load is conflict-free (row stride = 4 mod 16 doubles when K is the
+// contiguous index, 8 mod 16 when M/N is).  The epilogue is supplied by the
+// kernel that instantiates the mainloop.
 #pragma once
 
 #include "common.cuh"
+
+#include <type_traits>
 
 namespace gprat_cu
 {
 namespace gemm
 {
 
-constexpr int BM = 128;
-constexpr int BN = 128;
 constexpr int BK = 16;
-constexpr int STAGES = 4;
-constexpr int THREADS = 256;
 constexpr int PAD_K = 4;  // stride BK+4 = 20 doubles
-constexpr int PAD_T = 8;  // stride BM+8 = 136 doubles
+constexpr int PAD_T = 8;  // stride ROWS+8 doubles
 
-template <bool T>
-struct OpLayout;  // operand whose rows run along K (T=false for A, true for B)
+template <int WN>
+struct Cfg
+{
+    static constexpr int WM = 2;
+    static constexpr int THREADS = 32 * WM * WN;
+    static constexpr int BM = 64 * WM;  // 128
+    static constexpr int BN = 32 * WN;  // 128 or 64
+    static constexpr int STAGES = (WN == 4) ? 4 : 3;
+    static constexpr int MIN_BLOCKS = (WN == 4) ? 1 : 2;
+};
 
-// "K-contiguous" operand tile: [rows][BK+PAD_K]
+// Operand tile whose rows run along K: [ROWS][BK+PAD_K]
+template <int ROWS>
 struct KMajor
 {
-    static constexpr int SIZE = BM * (BK + PAD_K);
+    static constexpr int SIZE = ROWS * (BK + PAD_K);
     __device__ __forceinline__ static int idx(int row, int k) { return row * (BK + PAD_K) + k; }
 };
 
-// "row-contiguous" operand tile: [BK][rows+PAD_T]
+// Operand tile whose rows run along M or N: [BK][ROWS+PAD_T]
+template <int ROWS>
 struct RMajor
 {
-    static constexpr int SIZE = BK * (BM + PAD_T);
-    __device__ __forceinline__ static int idx(int row, int k) { return k * (BM + PAD_T) + row; }
+    static constexpr int SIZE = BK * (ROWS + PAD_T);
+    __device__ __forceinline__ static int idx(int row, int k) { return k * (ROWS + PAD_T) + row; }
 };
 
 // A: transA=false -> A[m][k] rows along K -> KMajor; true -> RMajor.
 // B: transB=true  -> B[n][k] rows along K -> KMajor; false -> RMajor.
-template <bool TA>
-using ALayout = typename std::conditional<TA, RMajor, KMajor>::type;
-template <bool TB>
-using BLayout = typename std::conditional<TB, KMajor, RMajor>::type;
+template <bool TA, int ROWS>
+using ALayout = typename std::conditional<TA, RMajor<ROWS>, KMajor<ROWS>>::type;
+template <bool TB, int ROWS>
+using BLayout = typename std::conditional<TB, KMajor<ROWS>, RMajor<ROWS>>::type;
 
-template <bool TA, bool TB>
+template <int WN, bool TA, bool TB>
 constexpr int smem_bytes()
 {
-    return STAGES * (ALayout<TA>::SIZE + BLayout<TB>::SIZE) * 8;
+    using C = Cfg<WN>;
+    return C::STAGES * (ALayout<TA, C::BM>::SIZE + BLayout<TB, C::BN>::SIZE) * 8;
 }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes)
@@ -76,18 +90,18 @@ __device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4]
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-// Copies one operand tile (rows [r0, r0+128) of the operand, K range
-// [k0, k0+16)) into shared memory.  `trans` selects the global layout:
-// false -> element (row, k) at P[row*ld + k]; true -> at P[k*ld + row].
-template <bool KMAJOR>
+// Copies one operand tile (ROWS rows of the operand starting at r0, K range
+// [k0, k0+16)) into shared memory with zero fill outside [rows) x [K).
+// KMAJOR: element (row, k) at P[row*ld + k]; otherwise at P[k*ld + row].
+template <bool KMAJOR, int ROWS, int THREADS>
 __device__ __forceinline__ void load_tile(double *s, const double *P, int64_t ld, int rows, int K, int r0, int k0,
                                           int tid)
 {
     if (KMAJOR)
     {
-        // 128 rows x 8 chunks of 2 doubles
+        constexpr int CHUNKS = ROWS * (BK / 2);
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < CHUNKS / THREADS; ++i)
         {
             int c = tid + i * THREADS;
             int row = c >> 3;
@@ -95,22 +109,23 @@ __device__ __forceinline__ void load_tile(double *s, const double *P, int64_t ld
             int gr = r0 + row, gk = k0 + kc;
             int nv = (gr < rows) ? min(max(K - gk, 0), 2) : 0;
             const double *src = nv ? P + static_cast<int64_t>(gr) * ld + gk : P;
-            cp_async16(s + KMajor::idx(row, kc), src, nv * 8);
+            cp_async16(s + KMajor<ROWS>::idx(row, kc), src, nv * 8);
         }
     }
     else
     {
-        // 16 k-rows x 64 chunks of 2 doubles
+        constexpr int PER_ROW = ROWS / 2;
+        constexpr int CHUNKS = BK * PER_ROW;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < CHUNKS / THREADS; ++i)
         {
             int c = tid + i * THREADS;
-            int krow = c >> 6;
-            int rc = (c & 63) * 2;
+            int krow = c / PER_ROW;
+            int rc = (c % PER_ROW) * 2;
             int gk = k0 + krow, gr = r0 + rc;
             int nv = (gk < K) ? min(max(rows - gr, 0), 2) : 0;
             const double *src = nv ? P + static_cast<int64_t>(gk) * ld + gr : P;
-            cp_async16(s + RMajor::idx(rc, krow), src, nv * 8);
+            cp_async16(s + RMajor<ROWS>::idx(rc, krow), src, nv * 8);
         }
     }
 }
@@ -118,30 +133,30 @@ __device__ __forceinline__ void load_tile(double *s, const double *P, int64_t ld
 struct TileCoord
 {
     int m0, n0;
-    bool skip;
 };
 
-// Maps blockIdx to the C tile; in `lower` mode the grid is 1-D over the
-// lower-triangular tiles (j <= i).
+// Maps blockIdx to the C tile.  In `lower` mode the grid is 1-D over the
+// tiles that touch the lower triangle: row tile i (BM high) has (i+1)*BM/BN
+// column tiles.
+template <int BM, int BN>
 __device__ __forceinline__ TileCoord tile_coord(bool lower)
 {
     TileCoord t;
-    t.skip = false;
     if (lower)
     {
-        int q = blockIdx.x;
-        int i = static_cast<int>((sqrt(8.0 * q + 1.0) - 1.0) * 0.5);
-        while ((i + 1) * (i + 2) / 2 <= q)
+        constexpr int R = BM / BN;
+        const int q = blockIdx.x;
+        int i = static_cast<int>((sqrt(8.0 * q / R + 1.0) - 1.0) * 0.5);
+        while (R * (i + 1) * (i + 2) / 2 <= q)
         {
             ++i;
         }
-        while (i * (i + 1) / 2 > q)
+        while (i > 0 && R * i * (i + 1) / 2 > q)
         {
             --i;
         }
-        int j = q - i * (i + 1) / 2;
         t.m0 = i * BM;
-        t.n0 = j * BN;
+        t.n0 = (q - R * i * (i + 1) / 2) * BN;
     }
     else
     {
@@ -151,18 +166,40 @@ __device__ __forceinline__ TileCoord tile_coord(bool lower)
     return t;
 }
 
+template <int BM, int BN>
+inline int lower_grid(int M)
+{
+    const int t = (M + BM - 1) / BM;
+    return (BM / BN) * t * (t + 1) / 2;
+}
+
 // acc[mi][ni][0..3]: rows wm*64+mi*16+g (+8 for [2],[3]), cols wn*32+ni*8+2t (+1)
 struct Frag
 {
     int g, t, wm, wn;
 };
 
-template <bool TA, bool TB>
-__device__ __forceinline__ void mainloop(const GemmArgs &a, int m0, int n0, double *smem, double (&acc)[4][4][4],
-                                         bool negate, int k_begin, const Frag &f)
+template <int WN>
+__device__ __forceinline__ Frag frag_coords()
 {
-    using LA = ALayout<TA>;
-    using LB = BLayout<TB>;
+    Frag f;
+    int lane = threadIdx.x & 31;
+    int warp = threadIdx.x >> 5;
+    f.g = lane >> 2;
+    f.t = lane & 3;
+    f.wm = warp / WN;  // 0..1
+    f.wn = warp % WN;
+    return f;
+}
+
+template <int WN, bool TA, bool TB>
+__device__ __forceinline__ void mainloop(const GemmArgs &a, int m0, int n0, double *smem, double (&acc)[4][4][4],
+                                         int k_begin, const Frag &f)
+{
+    using C = Cfg<WN>;
+    using LA = ALayout<TA, C::BM>;
+    using LB = BLayout<TB, C::BN>;
+    constexpr int STAGES = C::STAGES;
     double *sA = smem;
     double *sB = smem + STAGES * LA::SIZE;
     const int tid = threadIdx.x;
@@ -172,10 +209,8 @@ __device__ __forceinline__ void mainloop(const GemmArgs &a, int m0, int n0, doub
     auto load_stage = [&](int kt, int stage)
     {
         int k0 = k_begin + kt * BK;
-        // A tile: rows = M dimension
-        load_tile<!TA>(sA + stage * LA::SIZE, a.A, a.lda, a.M, a.K, m0, k0, tid);
-        // B tile: rows = N dimension
-        load_tile<TB>(sB + stage * LB::SIZE, a.B, a.ldb, a.N, a.K, n0, k0, tid);
+        load_tile<!TA, C::BM, C::THREADS>(sA + stage * LA::SIZE, a.A, a.lda, a.M, a.K, m0, k0, tid);
+        load_tile<TB, C::BN, C::THREADS>(sB + stage * LB::SIZE, a.B, a.ldb, a.N, a.K, n0, k0, tid);
     };
 
 #pragma unroll
@@ -188,7 +223,6 @@ __device__ __forceinline__ void mainloop(const GemmArgs &a, int m0, int n0, doub
         cp_async_commit();
     }
 
-    const double sgn = negate ? -1.0 : 1.0;
     for (int kt = 0; kt < KT; ++kt)
     {
         cp_async_wait<STAGES - 2>();
@@ -212,10 +246,10 @@ __device__ __forceinline__ void mainloop(const GemmArgs &a, int m0, int n0, doub
             {
                 int r = f.wm * 64 + mi * 16 + f.g;
                 int c = ks * 8 + f.t;
-                af[mi][0] = sgn * cA[LA::idx(r, c)];
-                af[mi][1] = sgn * cA[LA::idx(r + 8, c)];
-                af[mi][2] = sgn * cA[LA::idx(r, c + 4)];
-                af[mi][3] = sgn * cA[LA::idx(r + 8, c + 4)];
+                af[mi][0] = cA[LA::idx(r, c)];
+                af[mi][1] = cA[LA::idx(r + 8, c)];
+                af[mi][2] = cA[LA::idx(r, c + 4)];
+                af[mi][3] = cA[LA::idx(r + 8, c + 4)];
             }
 #pragma unroll
             for (int ni = 0; ni < 4; ++ni)
@@ -238,18 +272,6 @@ __device__ __forceinline__ void mainloop(const GemmArgs &a, int m0, int n0, doub
     }
     cp_async_wait<0>();
     __syncthreads();
-}
-
-__device__ __forceinline__ Frag frag_coords()
-{
-    Frag f;
-    int lane = threadIdx.x & 31;
-    int warp = threadIdx.x >> 5;
-    f.g = lane >> 2;
-    f.t = lane & 3;
-    f.wm = warp >> 2;  // 0..1
-    f.wn = warp & 3;   // 0..3
-    return f;
 }
 
 }  // namespace gemm

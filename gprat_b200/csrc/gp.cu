@@ -19,6 +19,7 @@
 //   gradient = U = L^-T, fused K^-1 = U U^T tile GEMM + derivative-tile
 //              regeneration + trace reduction, then Adam (optimizer.cu)
 #include "common.cuh"
+#include "gp_state.cuh"
 #include "gprat_cu.h"
 
 #include <cstring>
@@ -32,8 +33,6 @@ namespace
 {
 
 thread_local std::string g_last_error;
-
-constexpr int NB = 128;  // factorisation block size
 
 struct DeviceGuard
 {
@@ -56,89 +55,7 @@ struct DeviceGuard
     }
 };
 
-template <typename T>
-struct DevBuf
-{
-    T *ptr = nullptr;
-    int64_t cap = 0;  // elements
-    void ensure(int64_t n)
-    {
-        if (n <= cap)
-        {
-            return;
-        }
-        release();
-        GPRAT_CUDA_CHECK(cudaMalloc(&ptr, static_cast<size_t>(n) * sizeof(T)));
-        cap = n;
-    }
-    void release()
-    {
-        if (ptr != nullptr)
-        {
-            cudaFree(ptr);
-        }
-        ptr = nullptr;
-        cap = 0;
-    }
-    DevBuf() = default;
-    DevBuf(const DevBuf &) = delete;
-    DevBuf &operator=(const DevBuf &) = delete;
-    ~DevBuf() { release(); }
-};
-
 }  // namespace
-
-struct gprat_cu_gp
-{
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int n = 0, n_tiles = 0, T = 0, d = 0;
-    int64_t n_in = 0;
-    int64_t ld = 0;
-    int nblk = 0;
-    int precision = GPRAT_CU_PREC_FP64;
-
-    DevBuf<double> x, y, K, Linv, alpha, U, partials;
-    DevBuf<double> xt, W, vacc, mean_part, mean, var, losses;
-    DevBuf<DeviceParams> params;
-    DevBuf<DeviceStatus> status;
-    DeviceParams *h_params = nullptr;
-    DeviceStatus *h_status = nullptr;
-
-    ~gprat_cu_gp()
-    {
-        int prev = -1;
-        cudaGetDevice(&prev);
-        cudaSetDevice(device);
-        if (stream != nullptr)
-        {
-            cudaStreamSynchronize(stream);
-        }
-        for (DevBuf<double> *b : { &x, &y, &K, &Linv, &alpha, &U, &partials, &xt, &W, &vacc, &mean_part, &mean, &var,
-                                   &losses })
-        {
-            b->release();
-        }
-        params.release();
-        status.release();
-        if (h_params != nullptr)
-        {
-            cudaFreeHost(h_params);
-        }
-        if (h_status != nullptr)
-        {
-            cudaFreeHost(h_status);
-        }
-        if (stream != nullptr)
-        {
-            cudaStreamDestroy(stream);
-        }
-        if (prev >= 0)
-        {
-            cudaSetDevice(prev);
-        }
-    }
-};
 
 namespace
 {
@@ -197,67 +114,123 @@ double *kblock(gprat_cu_gp *gp, int r, int c) { return gp->K.ptr + static_cast<i
 
 double *linv_block(gprat_cu_gp *gp, int k) { return gp->Linv.ptr + static_cast<int64_t>(k) * NB * NB; }
 
+// C[MxN] = beta*C + alpha * A B^T (A: M x K, B: N x K, row-major)
+void gemm_nt(int M, int N, int K, const double *A, int64_t lda, const double *B, int64_t ldb, double *C,
+             int64_t ldc, double alpha, double beta, bool lower, double *rowsq, cudaStream_t s)
+{
+    GemmArgs g{};
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.A = A;
+    g.lda = lda;
+    g.transA = false;
+    g.B = B;
+    g.ldb = ldb;
+    g.transB = true;
+    g.C = C;
+    g.ldc = ldc;
+    g.alpha = alpha;
+    g.beta = beta;
+    g.lower = lower;
+    g.rowsq = rowsq;
+    dgemm(g, s);
+}
+
+// Two-level right-looking blocked Cholesky.  Inner steps (NB = 128): FP64
+// potrf + inverse of the diagonal block, panel solve P = P Linv^T (in place),
+// and the update of the rest of the current outer panel.  Outer steps
+// (NBO = 512): one lower-triangular DMMA update of the trailing matrix with
+// K = 512.
 void cholesky_blocked(gprat_cu_gp *gp, cudaStream_t s)
 {
     const int n = gp->n;
-    for (int k = 0; k < gp->nblk; ++k)
+    const int64_t ld = gp->ld;
+    for (int K0 = 0; K0 < n; K0 += NBO)
     {
-        const int r0 = k * NB;
-        const int bs = std::min(NB, n - r0);
-        potrf_diag(kblock(gp, r0, r0), gp->ld, bs, r0, linv_block(gp, k), NB, gp->status.ptr, s);
-        const int rows = n - r0 - bs;
-        if (rows <= 0)
+        const int bo = std::min(NBO, n - K0);
+        const int pend = K0 + bo;  // end of this outer panel
+        for (int r0 = K0; r0 < pend; r0 += NB)
         {
-            continue;
+            const int bs = std::min(NB, pend - r0);
+            const int k = r0 / NB;
+            potrf_diag(kblock(gp, r0, r0), ld, bs, r0, linv_block(gp, k), NB, gp->status.ptr, s);
+            const int rows = n - r0 - bs;
+            if (rows <= 0)
+            {
+                continue;
+            }
+            // panel solve: P = P * Linv_kk^T (in place; one CTA column since bs <= 128)
+            gemm_nt(rows, bs, bs, kblock(gp, r0 + bs, r0), ld, linv_block(gp, k), NB, kblock(gp, r0 + bs, r0), ld,
+                    1.0, 0.0, false, nullptr, s);
+            // update the rest of the outer panel: columns [r0+bs, pend)
+            const int ncols = pend - (r0 + bs);
+            if (ncols > 0)
+            {
+                // square part (rows [r0+bs, pend)): lower triangle only
+                gemm_nt(ncols, ncols, bs, kblock(gp, r0 + bs, r0), ld, kblock(gp, r0 + bs, r0), ld,
+                        kblock(gp, r0 + bs, r0 + bs), ld, -1.0, 1.0, true, nullptr, s);
+                // rows below the outer panel
+                const int below = n - pend;
+                if (below > 0)
+                {
+                    gemm_nt(below, ncols, bs, kblock(gp, pend, r0), ld, kblock(gp, r0 + bs, r0), ld,
+                            kblock(gp, pend, r0 + bs), ld, -1.0, 1.0, false, nullptr, s);
+                }
+            }
         }
-        // panel: P = P * Linv_kk^T (in place; one CTA column since bs <= 128)
-        GemmArgs pa{};
-        pa.M = rows;
-        pa.N = bs;
-        pa.K = bs;
-        pa.A = kblock(gp, r0 + bs, r0);
-        pa.lda = gp->ld;
-        pa.transA = false;
-        pa.B = linv_block(gp, k);
-        pa.ldb = NB;
-        pa.transB = true;
-        pa.C = kblock(gp, r0 + bs, r0);
-        pa.ldc = gp->ld;
-        pa.alpha = 1.0;
-        pa.beta = 0.0;
-        dgemm(pa, s);
-        // trailing: C -= P P^T, lower triangle only
-        GemmArgs ta{};
-        ta.M = rows;
-        ta.N = rows;
-        ta.K = bs;
-        ta.A = kblock(gp, r0 + bs, r0);
-        ta.lda = gp->ld;
-        ta.transA = false;
-        ta.B = kblock(gp, r0 + bs, r0);
-        ta.ldb = gp->ld;
-        ta.transB = true;
-        ta.C = kblock(gp, r0 + bs, r0 + bs);
-        ta.ldc = gp->ld;
-        ta.alpha = -1.0;
-        ta.beta = 1.0;
-        ta.lower = true;
-        dgemm(ta, s);
+        const int rest = n - pend;
+        if (rest > 0)
+        {
+            // outer trailing update: C -= P_o P_o^T, K = bo, lower triangle only
+            gemm_nt(rest, rest, bo, kblock(gp, pend, K0), ld, kblock(gp, pend, K0), ld, kblock(gp, pend, pend), ld,
+                    -1.0, 1.0, true, nullptr, s);
+        }
     }
 }
 
-void factor(gprat_cu_gp *gp, cudaStream_t s)
+// FP64 factorisation (always used by cholesky() and the optimiser).
+void factor_fp64(gprat_cu_gp *gp, cudaStream_t s)
 {
     assemble_covariance(gp->x.ptr, gp->n, gp->d, gp->T, gp->params.ptr, gp->K.ptr, gp->ld, s);
     cholesky_blocked(gp, s);
 }
 
-void solve_alpha(gprat_cu_gp *gp, cudaStream_t s)
+void solve_alpha_fp64(gprat_cu_gp *gp, cudaStream_t s)
 {
     GPRAT_CUDA_CHECK(
         cudaMemcpyAsync(gp->alpha.ptr, gp->y.ptr, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     trsv_forward(gp->K.ptr, gp->ld, gp->Linv.ptr, NB, gp->n, gp->alpha.ptr, nullptr, s);
     trsv_backward(gp->K.ptr, gp->ld, gp->Linv.ptr, NB, gp->n, gp->alpha.ptr, nullptr, s);
+}
+
+bool mixed(const gprat_cu_gp *gp) { return gp->precision != GPRAT_CU_PREC_FP64; }
+
+// Factorisation + alpha in the handle's precision mode.
+void fit(gprat_cu_gp *gp, cudaStream_t s)
+{
+    if (mixed(gp))
+    {
+        factor_mixed(gp, s);
+        alpha_mixed(gp, s);
+    }
+    else
+    {
+        factor_fp64(gp, s);
+        solve_alpha_fp64(gp, s);
+    }
+}
+
+void loss_after_fit(gprat_cu_gp *gp, cudaStream_t s)
+{
+    if (mixed(gp))
+    {
+        loss_mixed(gp, s);
+    }
+    else
+    {
+        loss_kernel(gp->y.ptr, gp->alpha.ptr, gp->K.ptr, gp->ld, gp->n, gp->params.ptr, s);
+    }
 }
 
 // Right-looking blocked solve W L^T = W (in place) over the first `rows`
@@ -267,48 +240,34 @@ template <typename RowLimit>
 void solve_right_lt(gprat_cu_gp *gp, double *W, int64_t ldw, int rows, double *rowsq, RowLimit row_limit,
                     cudaStream_t s)
 {
+    // Two-level blocking like the factorisation: inner 128-column steps
+    // inside a 512-column outer panel, then one K = 512 update of the rest.
     const int n = gp->n;
-    for (int k = 0; k < gp->nblk; ++k)
+    const int64_t ld = gp->ld;
+    for (int K0 = 0; K0 < n; K0 += NBO)
     {
-        const int c0 = k * NB;
-        const int bs = std::min(NB, n - c0);
-        const int mrows = std::min(rows, row_limit(k));
-        GemmArgs da{};
-        da.M = mrows;
-        da.N = bs;
-        da.K = bs;
-        da.A = W + c0;
-        da.lda = ldw;
-        da.transA = false;
-        da.B = linv_block(gp, k);
-        da.ldb = NB;
-        da.transB = true;
-        da.C = W + c0;
-        da.ldc = ldw;
-        da.alpha = 1.0;
-        da.beta = 0.0;
-        da.rowsq = rowsq;
-        dgemm(da, s);
-        const int rest = n - c0 - bs;
-        if (rest <= 0)
+        const int bo = std::min(NBO, n - K0);
+        const int pend = K0 + bo;
+        for (int c0 = K0; c0 < pend; c0 += NB)
         {
-            continue;
+            const int bs = std::min(NB, pend - c0);
+            const int k = c0 / NB;
+            const int mrows = std::min(rows, row_limit(k));
+            gemm_nt(mrows, bs, bs, W + c0, ldw, linv_block(gp, k), NB, W + c0, ldw, 1.0, 0.0, false, rowsq, s);
+            const int ncols = pend - (c0 + bs);
+            if (ncols > 0)
+            {
+                gemm_nt(mrows, ncols, bs, W + c0, ldw, kblock(gp, c0 + bs, c0), ld, W + c0 + bs, ldw, -1.0, 1.0,
+                        false, nullptr, s);
+            }
         }
-        GemmArgs ua{};
-        ua.M = mrows;
-        ua.N = rest;
-        ua.K = bs;
-        ua.A = W + c0;
-        ua.lda = ldw;
-        ua.transA = false;
-        ua.B = kblock(gp, c0 + bs, c0);
-        ua.ldb = gp->ld;
-        ua.transB = true;
-        ua.C = W + c0 + bs;
-        ua.ldc = ldw;
-        ua.alpha = -1.0;
-        ua.beta = 1.0;
-        dgemm(ua, s);
+        const int rest = n - pend;
+        if (rest > 0)
+        {
+            const int mrows = std::min(rows, row_limit((pend - 1) / NB));
+            gemm_nt(mrows, rest, bo, W + K0, ldw, kblock(gp, pend, K0), ld, W + pend, ldw, -1.0, 1.0, false, nullptr,
+                    s);
+        }
     }
 }
 
@@ -320,6 +279,11 @@ void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
         return;
     }
     const int parts = ceil_div(gp->n, 128);
+    if (mixed(gp) && d_var != nullptr)
+    {
+        variance_mixed(gp, d_xt, m, d_mean, d_var, s);
+        return;
+    }
     gp->mean_part.ensure(static_cast<int64_t>(m) * parts);
     if (d_var == nullptr)
     {
@@ -378,8 +342,9 @@ void download(gprat_cu_gp *gp, double *host, const double *dev, int64_t count)
 
 void gradient_device(gprat_cu_gp *gp, bool adam, cudaStream_t s)
 {
-    factor(gp, s);
-    solve_alpha(gp, s);
+    // the adjoint gradient and Adam always run in FP64
+    factor_fp64(gp, s);
+    solve_alpha_fp64(gp, s);
     loss_kernel(gp->y.ptr, gp->alpha.ptr, gp->K.ptr, gp->ld, gp->n, gp->params.ptr, s);
     // U = L^-T: solve U L^T = I; column block k of U has nonzeros in rows < (k+1)*NB
     gp->U.ensure(static_cast<int64_t>(gp->n) * gp->ld);
@@ -470,6 +435,7 @@ int gprat_cu_gp_create(int device, const double *train_in, int64_t n_in, const d
                 gp->d = n_regressors;
                 gp->n_in = n + n_regressors - 1;
                 gp->ld = round_up(n, 8);
+                gp->ld32 = round_up(n, 64);
                 gp->nblk = ceil_div(n, NB);
                 GPRAT_CUDA_CHECK(cudaStreamCreateWithFlags(&gp->stream, cudaStreamNonBlocking));
                 GPRAT_CUDA_CHECK(cudaMallocHost(&gp->h_params, sizeof(DeviceParams)));
@@ -508,7 +474,12 @@ int gprat_cu_gp_set_precision(gprat_cu_gp *gp, int precision)
         [&]
         {
             check_gp(gp);
-            require(precision == GPRAT_CU_PREC_FP64, "only GPRAT_CU_PREC_FP64 is available in this build");
+            require(precision == GPRAT_CU_PREC_FP64 || precision == GPRAT_CU_PREC_MIXED_TF32 ||
+                        precision == GPRAT_CU_PREC_MIXED_BF16,
+                    "unknown precision mode " + std::to_string(precision));
+            require(precision == GPRAT_CU_PREC_FP64 || gp->n % NB == 0,
+                    "mixed precision needs n_tiles * n_tile_size to be a multiple of 128 (got " +
+                        std::to_string(gp->n) + ")");
             gp->precision = precision;
         });
 }
@@ -522,7 +493,7 @@ int gprat_cu_cholesky(gprat_cu_gp *gp, const double hyper[3], double *tiles_out)
             require(tiles_out != nullptr, "output must not be NULL");
             DeviceGuard guard(gp->device);
             upload_hyper(gp, hyper, gp->stream);
-            factor(gp, gp->stream);
+            factor_fp64(gp, gp->stream);
             std::vector<double> full(static_cast<size_t>(gp->n) * gp->ld);
             download(gp, full.data(), gp->K.ptr, static_cast<int64_t>(gp->n) * gp->ld);
             finish_and_check(gp);
@@ -563,8 +534,7 @@ int gprat_cu_predict(gprat_cu_gp *gp, const double hyper[3], const double *test_
             upload_hyper(gp, hyper, gp->stream);
             upload_test(gp, test_in, n_test_in, m);
             gp->mean.ensure(std::max(m, 1));
-            factor(gp, gp->stream);
-            solve_alpha(gp, gp->stream);
+            fit(gp, gp->stream);
             predict_device(gp, gp->xt.ptr, m, gp->mean.ptr, nullptr, gp->stream);
             download(gp, mean, gp->mean.ptr, m);
             finish_and_check(gp);
@@ -586,8 +556,7 @@ static int predict_var_common(gprat_cu_gp *gp, const double hyper[3], const doub
             upload_test(gp, test_in, n_test_in, m);
             gp->mean.ensure(std::max(m, 1));
             gp->var.ensure(std::max(m, 1));
-            factor(gp, gp->stream);
-            solve_alpha(gp, gp->stream);
+            fit(gp, gp->stream);
             predict_device(gp, gp->xt.ptr, m, gp->mean.ptr, gp->var.ptr, gp->stream);
             download(gp, mean, gp->mean.ptr, m);
             download(gp, var, gp->var.ptr, m);
@@ -626,8 +595,16 @@ int gprat_cu_predict_full_covariance(gprat_cu_gp *gp, const double hyper[3], con
             }
             gp->mean.ensure(m);
             gp->var.ensure(m);
-            factor(gp, gp->stream);
-            solve_alpha(gp, gp->stream);
+            // the full posterior covariance is always computed in FP64
+            const int saved_precision = gp->precision;
+            gp->precision = GPRAT_CU_PREC_FP64;
+            struct Restore
+            {
+                gprat_cu_gp *g;
+                int p;
+                ~Restore() { g->precision = p; }
+            } restore{ gp, saved_precision };
+            fit(gp, gp->stream);
             predict_device(gp, gp->xt.ptr, m, gp->mean.ptr, gp->var.ptr, gp->stream);
             // Sigma = K** - W W^T  (W = K* L^-T, m x n, left in gp->W)
             const int64_t lds = round_up(m, 8);
@@ -666,9 +643,8 @@ int gprat_cu_compute_loss(gprat_cu_gp *gp, const double hyper[3], double *loss)
             require(loss != nullptr, "loss must not be NULL");
             DeviceGuard guard(gp->device);
             upload_hyper(gp, hyper, gp->stream);
-            factor(gp, gp->stream);
-            solve_alpha(gp, gp->stream);
-            loss_kernel(gp->y.ptr, gp->alpha.ptr, gp->K.ptr, gp->ld, gp->n, gp->params.ptr, gp->stream);
+            fit(gp, gp->stream);
+            loss_after_fit(gp, gp->stream);
             GPRAT_CUDA_CHECK(cudaMemcpyAsync(gp->h_params, gp->params.ptr, sizeof(DeviceParams),
                                              cudaMemcpyDeviceToHost, gp->stream));
             finish_and_check(gp);
@@ -785,8 +761,7 @@ int gprat_cu_fit_predict_device(gprat_cu_gp *gp, const double hyper[3], const do
             DeviceGuard guard(gp->device);
             cudaStream_t s = stream != nullptr ? static_cast<cudaStream_t>(stream) : gp->stream;
             upload_hyper(gp, hyper, s);
-            factor(gp, s);
-            solve_alpha(gp, s);
+            fit(gp, s);
             predict_device(gp, d_test_in, m, d_mean, d_var, s);
         });
 }

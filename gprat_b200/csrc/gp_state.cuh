@@ -1,0 +1,138 @@
+// Device state of one GP handle (struct gprat_cu_gp of the C ABI), shared by
+// the FP64 pipeline (gp.cu) and the mixed-precision pipeline (mixed.cu).
+#pragma once
+
+#include "common.cuh"
+#include "gprat_cu.h"
+#include "tc_gemm.cuh"
+
+#include <initializer_list>
+
+namespace gprat_cu
+{
+
+constexpr int NB = 128;   // diagonal block size (potrf + inverse)
+constexpr int NBO = 512;  // outer block of the two-level factorisation and solves
+
+template <typename T>
+struct DevBuf
+{
+    T *ptr = nullptr;
+    int64_t cap = 0;  // elements
+    void ensure(int64_t n)
+    {
+        if (n <= cap)
+        {
+            return;
+        }
+        release();
+        GPRAT_CUDA_CHECK(cudaMalloc(&ptr, static_cast<size_t>(n) * sizeof(T)));
+        cap = n;
+    }
+    void release()
+    {
+        if (ptr != nullptr)
+        {
+            cudaFree(ptr);
+        }
+        ptr = nullptr;
+        cap = 0;
+    }
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+};
+
+// Scalars of the preconditioned CG solve on the device.
+struct PcgScalars
+{
+    double rz;      // r . z
+    double pq;      // p . q
+    double rr;      // r . r
+    double yy;      // y . y
+    double a, b;    // step lengths
+    int converged;  // 1 once |r| <= tol |y|
+    int iters;      // iterations taken
+};
+
+}  // namespace gprat_cu
+
+struct gprat_cu_gp
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int n = 0, n_tiles = 0, T = 0, d = 0;
+    int64_t n_in = 0;
+    int64_t ld = 0;    // FP64 leading dimension
+    int64_t ld32 = 0;  // FP32 / BF16 leading dimension (multiple of 64)
+    int nblk = 0;
+    int precision = GPRAT_CU_PREC_FP64;
+
+    // FP64 path
+    gprat_cu::DevBuf<double> x, y, K, Linv, alpha, U, partials;
+    gprat_cu::DevBuf<double> xt, W, vacc, mean_part, mean, var, losses;
+    gprat_cu::DevBuf<gprat_cu::DeviceParams> params;
+    gprat_cu::DevBuf<gprat_cu::DeviceStatus> status;
+    gprat_cu::DeviceParams *h_params = nullptr;
+    gprat_cu::DeviceStatus *h_status = nullptr;
+
+    // mixed path
+    gprat_cu::DevBuf<float> K32, Linv32, W32;
+    gprat_cu::DevBuf<uint16_t> Lb, Wb;  // BF16 copies (mixed-bf16)
+    gprat_cu::DevBuf<double> D64;       // one diagonal block in FP64
+    gprat_cu::DevBuf<double> pcg_r, pcg_z, pcg_p, pcg_q, symv_part;
+    gprat_cu::DevBuf<gprat_cu::PcgScalars> pcg_s;
+    int pcg_last_iters = 0;
+
+    ~gprat_cu_gp()
+    {
+        int prev = -1;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        if (stream != nullptr)
+        {
+            cudaStreamSynchronize(stream);
+        }
+        for (gprat_cu::DevBuf<double> *b : { &x, &y, &K, &Linv, &alpha, &U, &partials, &xt, &W, &vacc, &mean_part,
+                                             &mean, &var, &losses, &D64, &pcg_r, &pcg_z, &pcg_p, &pcg_q, &symv_part })
+        {
+            b->release();
+        }
+        K32.release();
+        Linv32.release();
+        W32.release();
+        Lb.release();
+        Wb.release();
+        pcg_s.release();
+        params.release();
+        status.release();
+        if (h_params != nullptr)
+        {
+            cudaFreeHost(h_params);
+        }
+        if (h_status != nullptr)
+        {
+            cudaFreeHost(h_status);
+        }
+        if (stream != nullptr)
+        {
+            cudaStreamDestroy(stream);
+        }
+        if (prev >= 0)
+        {
+            cudaSetDevice(prev);
+        }
+    }
+};
+
+namespace gprat_cu
+{
+
+// mixed.cu
+void factor_mixed(gprat_cu_gp *gp, cudaStream_t s);
+void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s);
+void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s);
+void loss_mixed(gprat_cu_gp *gp, cudaStream_t s);
+
+}  // namespace gprat_cu

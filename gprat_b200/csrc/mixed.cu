@@ -1,0 +1,524 @@
+// Mixed-precision pipeline (GPRAT_CU_PREC_MIXED_TF32 / _BF16).
+//
+// Factorisation: K is assembled in FP64 and copied to an FP32 working matrix
+// K32.  Two-level right-looking blocked Cholesky as in the FP64 path, but
+//   - each 128 x 128 diagonal block is factored and inverted in FP64
+//     (potrf_diag on an FP64 copy), its FP64 diagonal kept for the
+//     log-determinant;
+//   - the panel solves P = P Linv^T run on the tcgen05 tensor cores (TF32
+//     operands, FP32 accumulation in TMEM), in place;
+//   - the inner (K = 128) and outer (K = 512) trailing updates run on the
+//     tcgen05 tensor cores with TF32 operands (MIXED_TF32) or BF16 operands
+//     (MIXED_BF16, from a BF16 copy of the factor), FP32 accumulation.
+// alpha: preconditioned conjugate gradients in FP64 on the exact FP64 K
+// (a lower-storage symmetric mat-vec), preconditioned by the low-precision
+// factor, to a relative residual of 1e-12.  The loss uses that alpha and
+// the FP64 diagonal of the factor.
+// Mean: FP64 cross covariance fused with the refined alpha.
+// Variance: the cross covariance stored in FP32 and the solve W L^T = K*
+// on the tensor cores with the same two-level blocking, row sums of W^2
+// accumulated in FP64.  Its error is that of the low-precision factor.
+#include "gp_state.cuh"
+
+#include <cmath>
+#include <string>
+
+namespace gprat_cu
+{
+namespace
+{
+
+constexpr int PCG_MAX_ITERS = 60;
+constexpr double PCG_TOL = 1e-12;
+constexpr int DOT_BLOCKS = 296;
+constexpr int DOT_THREADS = 256;
+
+struct MixedOps
+{
+    TcOperand L;     // K32 (TF32 view)
+    TcOperand Lb;    // BF16 factor copy
+    TcOperand Linv;  // Linv32 (TF32 view)
+    bool bf16;
+    const TcOperand &trail() const { return bf16 ? Lb : L; }
+};
+
+MixedOps make_ops(gprat_cu_gp *gp)
+{
+    MixedOps o;
+    o.bf16 = gp->precision == GPRAT_CU_PREC_MIXED_BF16;
+    tc_make_operand(o.L, gp->K32.ptr, gp->n, static_cast<int>(gp->ld32), gp->ld32, TcKind::TF32);
+    tc_make_operand(o.Linv, gp->Linv32.ptr, gp->nblk * NB, NB, NB, TcKind::TF32);
+    if (o.bf16)
+    {
+        tc_make_operand(o.Lb, gp->Lb.ptr, gp->n, static_cast<int>(gp->ld32), gp->ld32, TcKind::BF16);
+    }
+    return o;
+}
+
+TcGemmArgs tc_args(int M, int N, int K, int ar, int ac, int br, int bc, float *C, int64_t ldc, float alpha,
+                   float beta, bool lower, double *rowsq, DeviceStatus *st)
+{
+    TcGemmArgs g{};
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.a_row0 = ar;
+    g.a_col0 = ac;
+    g.b_row0 = br;
+    g.b_col0 = bc;
+    g.C = C;
+    g.ldc = ldc;
+    g.alpha = alpha;
+    g.beta = beta;
+    g.lower = lower;
+    g.rowsq = rowsq;
+    g.status = st;
+    return g;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 symmetric mat-vec q = K p from the lower triangle (row-major, ld).
+// One CTA per lower 128x128 tile (I, J <= I): it adds K_IJ p_J to the rows of
+// block I and K_IJ^T p_I to the rows of block J.  Each (block, rows) pair of
+// the partial buffer part[B][i] has exactly one writer, and q_i sums
+// part[0..nblk)[i] in a fixed order, so the result is deterministic.
+constexpr int SV_THREADS = 256;
+
+__global__ void __launch_bounds__(SV_THREADS) symv_tile_kernel(const double *__restrict__ K, int64_t ld, int n,
+                                                               const double *__restrict__ p, double *__restrict__ part)
+{
+    __shared__ double pI[128], pJ[128];
+    __shared__ double colsum[8][128];
+    __shared__ double rowsum[128];
+    const int q = blockIdx.x;
+    int I = static_cast<int>((sqrt(8.0 * q + 1.0) - 1.0) * 0.5);
+    while ((I + 1) * (I + 2) / 2 <= q)
+    {
+        ++I;
+    }
+    while (I > 0 && I * (I + 1) / 2 > q)
+    {
+        --I;
+    }
+    const int J = q - I * (I + 1) / 2;
+    const int i0 = I * 128, j0 = J * 128;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int t = threadIdx.x; t < 128; t += SV_THREADS)
+    {
+        pI[t] = (i0 + t < n) ? p[i0 + t] : 0.0;
+        pJ[t] = (j0 + t < n) ? p[j0 + t] : 0.0;
+    }
+    __syncthreads();
+    double cs[4] = { 0.0, 0.0, 0.0, 0.0 };
+    for (int r = warp; r < 128; r += SV_THREADS / 32)
+    {
+        const int gi = i0 + r;
+        double rs = 0.0;
+        if (gi < n)
+        {
+            const double *kr = K + static_cast<int64_t>(gi) * ld + j0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                const int lj = lane + 32 * c;
+                const int gj = j0 + lj;
+                if (gj < n && (I != J || lj <= r))
+                {
+                    const double v = kr[lj];
+                    rs += v * pJ[lj];
+                    if (I != J || lj < r)
+                    {
+                        cs[c] += v * pI[r];
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            rs += __shfl_xor_sync(0xffffffffu, rs, o);
+        }
+        if (lane == 0)
+        {
+            rowsum[r] = rs;
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+    {
+        colsum[warp][lane + 32 * c] = cs[c];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 128; t += SV_THREADS)
+    {
+        double c = 0.0;
+#pragma unroll
+        for (int w = 0; w < SV_THREADS / 32; ++w)
+        {
+            c += colsum[w][t];
+        }
+        if (I == J)
+        {
+            if (i0 + t < n)
+            {
+                part[static_cast<int64_t>(I) * n + i0 + t] = rowsum[t] + c;
+            }
+        }
+        else
+        {
+            if (i0 + t < n)
+            {
+                part[static_cast<int64_t>(J) * n + i0 + t] = rowsum[t];
+            }
+            if (j0 + t < n)
+            {
+                part[static_cast<int64_t>(I) * n + j0 + t] = c;
+            }
+        }
+    }
+}
+
+__global__ void symv_reduce_kernel(const double *__restrict__ part, int nblk, int n, double *__restrict__ q)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        double s = 0.0;
+        for (int b = 0; b < nblk; ++b)
+        {
+            s += part[static_cast<int64_t>(b) * n + i];
+        }
+        q[i] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// PCG helpers (all scalars live in PcgScalars on the device)
+
+__global__ void __launch_bounds__(DOT_THREADS) dot_partial_kernel(const double *__restrict__ a,
+                                                                  const double *__restrict__ b, int n,
+                                                                  double *__restrict__ part)
+{
+    __shared__ double red[DOT_THREADS];
+    double s = 0.0;
+    for (int i = blockIdx.x * DOT_THREADS + threadIdx.x; i < n; i += DOT_BLOCKS * DOT_THREADS)
+    {
+        s += a[i] * b[i];
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = DOT_THREADS / 2; w > 0; w >>= 1)
+    {
+        if (threadIdx.x < w)
+        {
+            red[threadIdx.x] += red[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        part[blockIdx.x] = red[0];
+    }
+}
+
+__device__ double sum_parts(const double *part)
+{
+    double s = 0.0;
+    for (int b = 0; b < DOT_BLOCKS; ++b)
+    {
+        s += part[b];
+    }
+    return s;
+}
+
+// which: 0 = yy (init), 1 = rz (init), 2 = pq -> a, 3 = rr -> converged, 4 = rz -> b
+__global__ void pcg_scalar_kernel(PcgScalars *s, const double *part, int which, double tol)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+    {
+        return;
+    }
+    const double v = sum_parts(part);
+    switch (which)
+    {
+        case 0:
+            s->yy = v;
+            s->converged = (v == 0.0) ? 1 : 0;
+            s->iters = 0;
+            break;
+        case 1: s->rz = v; break;
+        case 2:
+            s->pq = v;
+            s->a = (v != 0.0) ? s->rz / v : 0.0;
+            break;
+        case 3:
+            s->rr = v;
+            s->iters += 1;
+            s->converged = (v <= tol * tol * s->yy) ? 1 : 0;
+            break;
+        case 4:
+            s->b = (s->rz != 0.0) ? v / s->rz : 0.0;
+            s->rz = v;
+            break;
+    }
+}
+
+// x += a p; r -= a q
+__global__ void pcg_update_kernel(const PcgScalars *__restrict__ s, double *__restrict__ x,
+                                  double *__restrict__ r, const double *__restrict__ p,
+                                  const double *__restrict__ q, int n)
+{
+    const double a = s->a;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        x[i] += a * p[i];
+        r[i] -= a * q[i];
+    }
+}
+
+// p = z + b p
+__global__ void pcg_direction_kernel(const PcgScalars *__restrict__ s, double *__restrict__ p,
+                                     const double *__restrict__ z, int n)
+{
+    const double b = s->b;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        p[i] = z[i] + b * p[i];
+    }
+}
+
+void dot(const double *a, const double *b, int n, double *part, cudaStream_t s)
+{
+    dot_partial_kernel<<<DOT_BLOCKS, DOT_THREADS, 0, s>>>(a, b, n, part);
+    GPRAT_LAUNCH_CHECK();
+}
+
+void scalar(PcgScalars *ps, const double *part, int which, cudaStream_t s)
+{
+    pcg_scalar_kernel<<<1, 32, 0, s>>>(ps, part, which, PCG_TOL);
+    GPRAT_LAUNCH_CHECK();
+}
+
+int blocks_for(int n) { return std::min(ceil_div(n, 256), 148 * 8); }
+
+void symv(gprat_cu_gp *gp, const double *p, double *q, cudaStream_t s)
+{
+    const int tiles = gp->nblk * (gp->nblk + 1) / 2;
+    symv_tile_kernel<<<tiles, SV_THREADS, 0, s>>>(gp->K.ptr, gp->ld, gp->n, p, gp->symv_part.ptr);
+    GPRAT_LAUNCH_CHECK();
+    symv_reduce_kernel<<<ceil_div(gp->n, 256), 256, 0, s>>>(gp->symv_part.ptr, gp->nblk, gp->n, q);
+    GPRAT_LAUNCH_CHECK();
+}
+
+void precondition(gprat_cu_gp *gp, const double *r, double *z, cudaStream_t s)
+{
+    GPRAT_CUDA_CHECK(cudaMemcpyAsync(z, r, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    trsv_forward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, NB, gp->n, z, s);
+    trsv_backward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, NB, gp->n, z, s);
+}
+
+}  // namespace
+
+void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
+{
+    const int n = gp->n;
+    if (n % NB != 0)
+    {
+        throw Error(GPRAT_CU_ERR_INVALID_ARG,
+                    "mixed precision needs n_tiles * n_tile_size to be a multiple of 128 (got " + std::to_string(n) +
+                        ")");
+    }
+    const int64_t ld32 = gp->ld32;
+    gp->K32.ensure(static_cast<int64_t>(n) * ld32);
+    gp->Linv32.ensure(static_cast<int64_t>(gp->nblk) * NB * NB);
+    gp->D64.ensure(static_cast<int64_t>(NB) * NB + n);  // one block + the FP64 diagonal of L
+    if (gp->precision == GPRAT_CU_PREC_MIXED_BF16)
+    {
+        gp->Lb.ensure(static_cast<int64_t>(n) * ld32);
+    }
+    double *D = gp->D64.ptr;
+    double *ldiag = gp->D64.ptr + NB * NB;
+
+    assemble_covariance(gp->x.ptr, n, gp->d, gp->T, gp->params.ptr, gp->K.ptr, gp->ld, s);
+    convert_f64_to_f32(gp->K.ptr, gp->ld, gp->K32.ptr, ld32, n, n, s);
+    const MixedOps ops = make_ops(gp);
+    float *K32 = gp->K32.ptr;
+    auto at = [&](int r, int c) { return K32 + static_cast<int64_t>(r) * ld32 + c; };
+
+    for (int K0 = 0; K0 < n; K0 += NBO)
+    {
+        const int bo = std::min(NBO, n - K0);
+        const int pend = K0 + bo;
+        for (int r0 = K0; r0 < pend; r0 += NB)
+        {
+            const int k = r0 / NB;
+            double *Lk = gp->Linv.ptr + static_cast<int64_t>(k) * NB * NB;
+            convert_f32_to_f64(at(r0, r0), ld32, D, NB, NB, NB, s);
+            potrf_diag(D, NB, NB, r0, Lk, NB, gp->status.ptr, s);
+            GPRAT_CUDA_CHECK(cudaMemcpy2DAsync(ldiag + r0, sizeof(double), D, (NB + 1) * sizeof(double),
+                                               sizeof(double), NB, cudaMemcpyDeviceToDevice, s));
+            convert_f64_to_f32(D, NB, at(r0, r0), ld32, NB, NB, s);
+            convert_f64_to_f32(Lk, NB, gp->Linv32.ptr + static_cast<int64_t>(k) * NB * NB, NB, NB, NB, s);
+            const int rows = n - r0 - NB;
+            if (rows > 0)
+            {
+                // panel solve P = P Linv^T on the tensor cores (TF32), in place
+                tc_gemm(ops.L, ops.Linv,
+                        tc_args(rows, NB, NB, r0 + NB, r0, k * NB, 0, at(r0 + NB, r0), ld32, 1.0f, 0.0f, false,
+                                nullptr, gp->status.ptr),
+                        s);
+            }
+            if (ops.bf16)
+            {
+                convert_f32_to_bf16(at(r0, r0), ld32, gp->Lb.ptr + static_cast<int64_t>(r0) * ld32 + r0, ld32,
+                                    n - r0, NB, s);
+            }
+            const int ncols = pend - (r0 + NB);
+            if (ncols > 0)
+            {
+                tc_gemm(ops.trail(), ops.trail(),
+                        tc_args(ncols, ncols, NB, r0 + NB, r0, r0 + NB, r0, at(r0 + NB, r0 + NB), ld32, -1.0f, 1.0f,
+                                true, nullptr, gp->status.ptr),
+                        s);
+                const int below = n - pend;
+                if (below > 0)
+                {
+                    tc_gemm(ops.trail(), ops.trail(),
+                            tc_args(below, ncols, NB, pend, r0, r0 + NB, r0, at(pend, r0 + NB), ld32, -1.0f, 1.0f,
+                                    false, nullptr, gp->status.ptr),
+                            s);
+                }
+            }
+        }
+        const int rest = n - pend;
+        if (rest > 0)
+        {
+            tc_gemm(ops.trail(), ops.trail(),
+                    tc_args(rest, rest, bo, pend, K0, pend, K0, at(pend, pend), ld32, -1.0f, 1.0f, true, nullptr,
+                            gp->status.ptr),
+                    s);
+        }
+    }
+}
+
+void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s)
+{
+    const int n = gp->n;
+    for (DevBuf<double> *b : { &gp->pcg_r, &gp->pcg_z, &gp->pcg_p, &gp->pcg_q })
+    {
+        b->ensure(n);
+    }
+    gp->symv_part.ensure(static_cast<int64_t>(gp->nblk) * n + 3 * DOT_BLOCKS);
+    gp->pcg_s.ensure(1);
+    double *part = gp->symv_part.ptr + static_cast<int64_t>(gp->nblk) * n;  // dot partials
+    PcgScalars *ps = gp->pcg_s.ptr;
+    double *x = gp->alpha.ptr, *r = gp->pcg_r.ptr, *z = gp->pcg_z.ptr, *p = gp->pcg_p.ptr, *q = gp->pcg_q.ptr;
+    const int nb = blocks_for(n);
+
+    GPRAT_CUDA_CHECK(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+    GPRAT_CUDA_CHECK(cudaMemcpyAsync(r, gp->y.ptr, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    dot(r, r, n, part, s);
+    scalar(ps, part, 0, s);
+    precondition(gp, r, z, s);
+    dot(r, z, n, part, s);
+    scalar(ps, part, 1, s);
+    GPRAT_CUDA_CHECK(cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    PcgScalars h{};
+    int it = 0;
+    for (; it < PCG_MAX_ITERS; ++it)
+    {
+        symv(gp, p, q, s);
+        dot(p, q, n, part, s);
+        scalar(ps, part, 2, s);
+        pcg_update_kernel<<<nb, 256, 0, s>>>(ps, x, r, p, q, n);
+        GPRAT_LAUNCH_CHECK();
+        dot(r, r, n, part, s);
+        scalar(ps, part, 3, s);
+        GPRAT_CUDA_CHECK(cudaMemcpyAsync(&h, ps, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
+        GPRAT_CUDA_CHECK(cudaStreamSynchronize(s));
+        if (h.converged)
+        {
+            break;
+        }
+        precondition(gp, r, z, s);
+        dot(r, z, n, part, s);
+        scalar(ps, part, 4, s);
+        pcg_direction_kernel<<<nb, 256, 0, s>>>(ps, p, z, n);
+        GPRAT_LAUNCH_CHECK();
+    }
+    gp->pcg_last_iters = h.iters;
+}
+
+void loss_mixed(gprat_cu_gp *gp, cudaStream_t s)
+{
+    // y . alpha with the refined alpha, log-determinant from the FP64 diagonal
+    loss_kernel(gp->y.ptr, gp->alpha.ptr, gp->D64.ptr + NB * NB, 0, gp->n, gp->params.ptr, s);
+}
+
+void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
+{
+    const int n = gp->n;
+    const int64_t ld32 = gp->ld32;
+    const int parts = ceil_div(n, 128);
+    gp->mean_part.ensure(static_cast<int64_t>(m) * parts);
+    gp->W32.ensure(static_cast<int64_t>(m) * ld32);
+    gp->vacc.ensure(m);
+    const bool bf16 = gp->precision == GPRAT_CU_PREC_MIXED_BF16;
+    if (bf16)
+    {
+        gp->Wb.ensure(static_cast<int64_t>(m) * ld32);
+    }
+    float *W = gp->W32.ptr;
+    assemble_cross_f32(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, W, ld32, gp->alpha.ptr, gp->mean_part.ptr,
+                       parts, s);
+    reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
+    if (d_var == nullptr)
+    {
+        return;
+    }
+    GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->vacc.ptr, 0, m * sizeof(double), s));
+    const MixedOps ops = make_ops(gp);
+    TcOperand opW, opWb;
+    tc_make_operand(opW, W, m, static_cast<int>(ld32), ld32, TcKind::TF32);
+    if (bf16)
+    {
+        tc_make_operand(opWb, gp->Wb.ptr, m, static_cast<int>(ld32), ld32, TcKind::BF16);
+    }
+    const TcOperand &opWt = bf16 ? opWb : opW;
+    for (int K0 = 0; K0 < n; K0 += NBO)
+    {
+        const int bo = std::min(NBO, n - K0);
+        const int pend = K0 + bo;
+        for (int c0 = K0; c0 < pend; c0 += NB)
+        {
+            const int k = c0 / NB;
+            tc_gemm(opW, ops.Linv,
+                    tc_args(m, NB, NB, 0, c0, k * NB, 0, W + c0, ld32, 1.0f, 0.0f, false, gp->vacc.ptr,
+                            gp->status.ptr),
+                    s);
+            if (bf16)
+            {
+                convert_f32_to_bf16(W + c0, ld32, gp->Wb.ptr + c0, ld32, m, NB, s);
+            }
+            const int ncols = pend - (c0 + NB);
+            if (ncols > 0)
+            {
+                tc_gemm(opWt, ops.trail(),
+                        tc_args(m, ncols, NB, 0, c0, c0 + NB, c0, W + c0 + NB, ld32, -1.0f, 1.0f, false, nullptr,
+                                gp->status.ptr),
+                        s);
+            }
+        }
+        const int rest = n - pend;
+        if (rest > 0)
+        {
+            tc_gemm(opWt, ops.trail(),
+                    tc_args(m, rest, bo, 0, K0, pend, K0, W + pend, ld32, -1.0f, 1.0f, false, nullptr,
+                            gp->status.ptr),
+                    s);
+        }
+    }
+    finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, s);
+}
+
+}  // namespace gprat_cu

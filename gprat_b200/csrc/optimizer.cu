@@ -26,6 +26,10 @@ namespace
 {
 
 using namespace gemm;
+using AC = Cfg<4>;  // 128x128 tiles, 8 warps
+constexpr int THREADS = AC::THREADS;
+constexpr int BM = AC::BM;
+constexpr int BN = AC::BN;
 
 __global__ void __launch_bounds__(THREADS, 1) adjoint_kernel(GemmArgs a, const double *__restrict__ alpha,
                                                              const double *__restrict__ x, int d,
@@ -33,9 +37,9 @@ __global__ void __launch_bounds__(THREADS, 1) adjoint_kernel(GemmArgs a, const d
                                                              double *__restrict__ partials)
 {
     extern __shared__ __align__(16) double smem[];
-    TileCoord tc = tile_coord(true);
+    TileCoord tc = tile_coord<BM, BN>(true);
     const int m0 = tc.m0, n0 = tc.n0;
-    Frag f = frag_coords();
+    Frag f = frag_coords<4>();
     double acc[4][4][4];
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
@@ -46,7 +50,7 @@ __global__ void __launch_bounds__(THREADS, 1) adjoint_kernel(GemmArgs a, const d
                 acc[mi][ni][q] = 0.0;
 
     // U is upper triangular: rows >= m0 vanish for p < m0.
-    mainloop<false, true>(a, m0, n0, smem, acc, false, (m0 / BK) * BK, f);
+    mainloop<4, false, true>(a, m0, n0, smem, acc, (m0 / BK) * BK, f);
 
     // stage series windows and alpha for the tile's rows and columns
     double *xr = smem;
@@ -226,7 +230,7 @@ void adjoint_trace(const double *U, int64_t ldu, const double *alpha, const doub
     {
         throw Error(1, "adjoint_trace: U must be 16-byte aligned with an even leading dimension");
     }
-    constexpr int smem_main = smem_bytes<false, true>();
+    constexpr int smem_main = smem_bytes<4, false, true>();
     const int smem_epi = static_cast<int>((BM + BN + 2 * n_reg + BM + BN + 3 * THREADS / 32) * sizeof(double));
     const int smem = smem_main > smem_epi ? smem_main : smem_epi;
     if (smem > 227 * 1024)

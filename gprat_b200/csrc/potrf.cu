@@ -2,16 +2,22 @@
 //
 // Replaces the per-tile potrf task (LAPACKE_dpotrf2 'L',
 // core/src/cpu/adapter_cblas_fp64.cpp:14-22; cusolverDnXpotrf,
-// core/src/gpu/adapter_cublas.cu:9-79).  One CTA loads the lower triangle
-// of a bs x bs (bs <= 128) diagonal block into shared memory, factors it
-// column by column (right-looking), writes L back (the strict upper
-// triangle in global memory is never touched, matching dpotrf2('L')), then
-// inverts L in place by forward elimination on the identity and stores
-// Linv (zero above the diagonal).  The inverse turns every later triangular
-// solve against this block (panel trsm, trsv, variance solve) into a
-// tensor-core GEMM.  A non-positive or NaN pivot is recorded in the status
-// word (first failing global row, 1-based); the reference silently returns
-// NaNs instead.
+// core/src/gpu/adapter_cublas.cu:9-79).  One CTA of 16 warps loads the lower
+// triangle of a bs x bs (bs <= 128) diagonal block into shared memory and
+// factors it in 32-wide sub-blocks:
+//   1. warp 0 factors the 32 x 32 diagonal sub-block in registers (lane i
+//      holds row i; column values are exchanged with shuffles) and inverts
+//      it the same way (lane c holds column c of the inverse);
+//   2. the rows below are solved against it with the inverse (all warps);
+//   3. the trailing lower triangle is updated (all warps).
+// L is written back (the strict upper triangle in global memory is never
+// touched, matching dpotrf2('L')).  The full inverse Linv (zero above the
+// diagonal) is then assembled block row by block row,
+//   Linv_ss = X_s,  Linv_st = -X_s * sum_p L_s,p Linv_p,t,
+// which turns every later triangular solve against this block (panel trsm,
+// trsv, variance solve) into a tensor-core GEMM.  A non-positive or NaN
+// pivot is recorded in the status word (first failing global row, 1-based);
+// the reference silently returns NaNs instead.
 #include "common.cuh"
 
 namespace gprat_cu
@@ -19,18 +25,113 @@ namespace gprat_cu
 namespace
 {
 
-constexpr int PB = 128;         // max block size
-constexpr int PS = PB + 1;      // smem row stride (conflict-free columns)
+constexpr int PB = 128;     // max block size
+constexpr int PS = PB + 1;  // smem row stride of the block
+constexpr int SB = 32;      // sub-block width
+constexpr int XS = SB + 1;  // smem row stride of a sub-block inverse
+constexpr int TS = 96 + 1;  // smem row stride of the inverse temporary
+constexpr int XBLK = (SB + 1) * XS;  // one sub-block inverse plus its 1/L_ii row
 constexpr int PTHREADS = 512;
+
+// Warp 0: factor a[c0.., c0..] (w x w, w <= 32) in registers, write L back
+// to smem, and store X = L^-1 (32 x 32, zero above the diagonal) in xinv.
+__device__ __forceinline__ void warp_factor_invert(double *a, int c0, int w, int row0, int *bad, double *xinv)
+{
+    const int lane = threadIdx.x & 31;
+    double r[SB];
+#pragma unroll
+    for (int c = 0; c < SB; ++c)
+    {
+        double v;
+        if (lane < w && c < w)
+        {
+            v = (c <= lane) ? a[(c0 + lane) * PS + c0 + c] : 0.0;
+        }
+        else
+        {
+            v = (c == lane) ? 1.0 : 0.0;  // identity padding beyond w
+        }
+        r[c] = v;
+    }
+    double my_inv = 1.0;
+#pragma unroll
+    for (int j = 0; j < SB; ++j)
+    {
+        const double ajj = __shfl_sync(0xffffffffu, r[j], j);
+        if (lane == 0 && j < w && !(ajj > 0.0) && *bad == 0)
+        {
+            *bad = row0 + c0 + j + 1;
+        }
+        const double d = sqrt(ajj);
+        const double inv = 1.0 / d;
+        if (lane == j)
+        {
+            r[j] = d;
+            my_inv = inv;
+        }
+        else if (lane > j)
+        {
+            r[j] *= inv;
+        }
+#pragma unroll
+        for (int c = j + 1; c < SB; ++c)
+        {
+            const double lcj = __shfl_sync(0xffffffffu, r[j], c);
+            if (lane >= c)
+            {
+                r[c] -= r[j] * lcj;
+            }
+        }
+    }
+    if (lane < w)
+    {
+#pragma unroll
+        for (int c = 0; c < SB; ++c)
+        {
+            if (c <= lane)
+            {
+                a[(c0 + lane) * PS + c0 + c] = r[c];
+            }
+        }
+    }
+    // stage 1/L_ii for the inverse, then drop r (registers) and read L from smem
+    xinv[SB * XS + lane] = my_inv;
+    __syncwarp();
+    // inverse: lane c solves L x = e_c (column c of X); L rows are smem broadcasts
+    double x[SB];
+#pragma unroll
+    for (int i = 0; i < SB; ++i)
+    {
+        double s = (i == lane) ? 1.0 : 0.0;
+        const double *li = a + (c0 + i) * PS + c0;
+#pragma unroll
+        for (int k = 0; k < i; ++k)
+        {
+            s -= ((i < w) ? li[k] : 0.0) * x[k];
+        }
+        x[i] = s * xinv[SB * XS + i];
+    }
+#pragma unroll
+    for (int i = 0; i < SB; ++i)
+    {
+        xinv[i * XS + lane] = x[i];
+    }
+}
 
 __global__ void __launch_bounds__(PTHREADS) potrf_inv_kernel(double *__restrict__ A, int64_t lda, int bs, int row0,
                                                              double *__restrict__ Linv, int64_t ldi,
                                                              DeviceStatus *__restrict__ status)
 {
-    extern __shared__ double sa[];  // [PB][PS] + col[PB]
-    double *col = sa + PB * PS;
+    extern __shared__ double sa[];     // [PB][PS]
+    double *xall = sa + PB * PS;       // 4 x [SB+1][XS]: sub-block inverses + 1/L_ii row
+    double *tmp = xall + 4 * XBLK;     // [SB][TS]
+    __shared__ int bad;
     const int tid = threadIdx.x;
-    const int tx = tid & 31, ty = tid >> 5;
+    const int lane = tid & 31, warp = tid >> 5;
+    if (tid == 0)
+    {
+        bad = 0;
+    }
     for (int q = tid; q < bs * bs; q += PTHREADS)
     {
         int i = q / bs, c = q % bs;
@@ -38,38 +139,72 @@ __global__ void __launch_bounds__(PTHREADS) potrf_inv_kernel(double *__restrict_
     }
     __syncthreads();
 
-    // --- Cholesky, right-looking ---------------------------------------
-    __shared__ int bad;
-    if (tid == 0)
+    const int nsub = (bs + SB - 1) / SB;
+    for (int s = 0; s < nsub; ++s)
     {
-        bad = 0;
-    }
-    for (int j = 0; j < bs; ++j)
-    {
-        double ajj = sa[j * PS + j];
-        double dj = sqrt(ajj);
-        if (tid == 0 && !(ajj > 0.0) && bad == 0)
+        const int c0 = s * SB;
+        const int w = min(SB, bs - c0);
+        double *xs = xall + s * XBLK;
+        if (warp == 0)
         {
-            bad = row0 + j + 1;
-        }
-        // scale column j below the diagonal
-        for (int i = j + 1 + tid; i < bs; i += PTHREADS)
-        {
-            sa[i * PS + j] = sa[i * PS + j] / dj;
+            warp_factor_invert(sa, c0, w, row0, &bad, xs);
         }
         __syncthreads();
-        if (tid == 0)
+        const int r0 = c0 + w;
+        const int R = bs - r0;
+        if (R <= 0)
         {
-            sa[j * PS + j] = dj;
+            break;
         }
-        // rank-1 update of the trailing lower triangle (warp ty owns rows
-        // j+1+ty, j+1+ty+16, ...; lanes walk the columns)
-        for (int i = j + 1 + ty; i < bs; i += PTHREADS / 32)
+        // panel solve: P = P X^T (4 threads per row, 8 output columns each)
         {
-            const double lij = sa[i * PS + j];
-            for (int c = j + 1 + tx; c <= i; c += 32)
+            const int row = tid >> 2, grp = tid & 3;
+            double v[SB];
+            if (row < R)
             {
-                sa[i * PS + c] = sa[i * PS + c] - lij * sa[c * PS + j];
+#pragma unroll
+                for (int k = 0; k < SB; ++k)
+                {
+                    v[k] = (k < w) ? sa[(r0 + row) * PS + c0 + k] : 0.0;
+                }
+            }
+            __syncthreads();
+            if (row < R)
+            {
+#pragma unroll
+                for (int cc = 0; cc < 8; ++cc)
+                {
+                    const int c = grp * 8 + cc;
+                    if (c < w)
+                    {
+                        double acc = 0.0;
+#pragma unroll
+                        for (int k = 0; k < SB; ++k)
+                        {
+                            if (k <= c)
+                            {
+                                acc += v[k] * xs[c * XS + k];
+                            }
+                        }
+                        sa[(r0 + row) * PS + c0 + c] = acc;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // trailing update of the lower triangle rows/cols [r0, bs)
+        for (int i = r0 + warp; i < bs; i += PTHREADS / 32)
+        {
+            const double *pi = sa + i * PS + c0;
+            for (int c = r0 + lane; c <= i; c += 32)
+            {
+                const double *pc = sa + c * PS + c0;
+                double acc = 0.0;
+                for (int k = 0; k < w; ++k)
+                {
+                    acc += pi[k] * pc[k];
+                }
+                sa[i * PS + c] -= acc;
             }
         }
         __syncthreads();
@@ -89,29 +224,44 @@ __global__ void __launch_bounds__(PTHREADS) potrf_inv_kernel(double *__restrict_
     }
     __syncthreads();
 
-    // --- inverse: solve L X = I in place (row p of X replaces row p of L) --
-    for (int p = 0; p < bs; ++p)
+    // --- full inverse, block row by block row (rows < c0 already hold Linv) --
+    for (int s = 0; s < nsub; ++s)
     {
-        double d = sa[p * PS + p];
-        for (int i = p + 1 + tid; i < bs; i += PTHREADS)
+        const int c0 = s * SB;
+        const int w = min(SB, bs - c0);
+        const double *xs = xall + s * XBLK;
+        if (s > 0)
         {
-            col[i] = sa[i * PS + p];
-        }
-        // finalise row p of X: X[p][j] /= L[p][p] for j < p, X[p][p] = 1/L[p][p]
-        for (int c = tid; c <= p; c += PTHREADS)
-        {
-            sa[p * PS + c] = (c == p) ? 1.0 / d : sa[p * PS + c] / d;
-        }
-        __syncthreads();
-        // X[i][c] -= L[i][p] * X[p][c] for i > p, c <= p (X[i][p] starts at 0)
-        for (int i = p + 1 + ty; i < bs; i += PTHREADS / 32)
-        {
-            const double lip = col[i];
-            for (int c = tx; c <= p; c += 32)
+            // tmp[i][j] = sum_{p=j}^{c0-1} L[c0+i][p] * Linv[p][j],  j < c0
+            for (int q = tid; q < w * c0; q += PTHREADS)
             {
-                double base = (c == p) ? 0.0 : sa[i * PS + c];
-                sa[i * PS + c] = base - lip * sa[p * PS + c];
+                const int i = q / c0, j = q % c0;
+                const double *li = sa + (c0 + i) * PS;
+                double acc = 0.0;
+                for (int p = j; p < c0; ++p)
+                {
+                    acc += li[p] * sa[p * PS + j];
+                }
+                tmp[i * TS + j] = acc;
             }
+            __syncthreads();
+            // Linv[c0+i][j] = -sum_k X[i][k] tmp[k][j]
+            for (int q = tid; q < w * c0; q += PTHREADS)
+            {
+                const int i = q / c0, j = q % c0;
+                double acc = 0.0;
+                for (int k = 0; k <= i; ++k)
+                {
+                    acc += xs[i * XS + k] * tmp[k * TS + j];
+                }
+                sa[(c0 + i) * PS + j] = -acc;
+            }
+        }
+        // diagonal block: X_s
+        for (int q = tid; q < w * w; q += PTHREADS)
+        {
+            const int i = q / w, j = q % w;
+            sa[(c0 + i) * PS + c0 + j] = (j <= i) ? xs[i * XS + j] : 0.0;
         }
         __syncthreads();
     }
@@ -131,7 +281,7 @@ void potrf_diag(double *A, int64_t lda, int bs, int row0, double *Linv, int64_t 
     {
         throw Error(1, "potrf_diag: block size must be in [1, 128]");
     }
-    constexpr size_t smem = static_cast<size_t>(PB * PS + PB) * sizeof(double);
+    constexpr size_t smem = static_cast<size_t>(PB * PS + 4 * XBLK + SB * TS) * sizeof(double);
     ensure_smem_attr(reinterpret_cast<const void *>(potrf_inv_kernel), static_cast<int>(smem));
     potrf_inv_kernel<<<1, PTHREADS, smem, s>>>(A, lda, bs, row0, Linv, ldi, status);
     GPRAT_LAUNCH_CHECK();

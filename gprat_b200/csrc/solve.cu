@@ -75,7 +75,9 @@ __global__ void __launch_bounds__(128) diag_bwd_kernel(const double *__restrict_
 
 // r[i] -= L[i][0:bs] . z for rows i in [0, rows) (L points at the block
 // column, rows start right below the diagonal block).  One warp per row.
-__global__ void __launch_bounds__(256) fwd_update_kernel(const double *__restrict__ L, int64_t ldl, int rows, int bs,
+// L may be FP64 or FP32 (the mixed-precision factor); arithmetic is FP64.
+template <typename T>
+__global__ void __launch_bounds__(256) fwd_update_kernel(const T *__restrict__ L, int64_t ldl, int rows, int bs,
                                                          const double *__restrict__ z, double *__restrict__ r)
 {
     __shared__ double zs[128];
@@ -90,11 +92,11 @@ __global__ void __launch_bounds__(256) fwd_update_kernel(const double *__restric
     {
         return;
     }
-    const double *lr = L + static_cast<int64_t>(row) * ldl;
+    const T *lr = L + static_cast<int64_t>(row) * ldl;
     double s = 0.0;
     for (int c = lane; c < bs; c += 32)
     {
-        s += lr[c] * zs[c];
+        s += static_cast<double>(lr[c]) * zs[c];
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
@@ -109,7 +111,8 @@ __global__ void __launch_bounds__(256) fwd_update_kernel(const double *__restric
 
 // r[c] -= sum_p L[p][c] * a[p] for c in [0, cols) (L points at the first
 // row of the block row; rows p < bs).  Threads own columns.
-__global__ void __launch_bounds__(256) bwd_update_kernel(const double *__restrict__ L, int64_t ldl, int cols, int bs,
+template <typename T>
+__global__ void __launch_bounds__(256) bwd_update_kernel(const T *__restrict__ L, int64_t ldl, int cols, int bs,
                                                          const double *__restrict__ a, double *__restrict__ r)
 {
     __shared__ double as[128];
@@ -126,7 +129,7 @@ __global__ void __launch_bounds__(256) bwd_update_kernel(const double *__restric
     double s = 0.0;
     for (int p = 0; p < bs; ++p)
     {
-        s += L[static_cast<int64_t>(p) * ldl + c] * as[p];
+        s += static_cast<double>(L[static_cast<int64_t>(p) * ldl + c]) * as[p];
     }
     r[c] -= s;
 }
@@ -191,7 +194,11 @@ __global__ void diag_ones_kernel(double *A, int64_t lda, int n)
 
 }  // namespace
 
-void trsv_forward(const double *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, double *, cudaStream_t s)
+namespace
+{
+
+template <typename T>
+void trsv_forward_t(const T *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s)
 {
     const int nblk = ceil_div(n, nb);
     for (int k = 0; k < nblk; ++k)
@@ -210,8 +217,8 @@ void trsv_forward(const double *L, int64_t ldl, const double *Linv, int nb, int 
     }
 }
 
-void trsv_backward(const double *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, double *,
-                   cudaStream_t s)
+template <typename T>
+void trsv_backward_t(const T *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s)
 {
     const int nblk = ceil_div(n, nb);
     for (int k = nblk - 1; k >= 0; --k)
@@ -227,6 +234,29 @@ void trsv_backward(const double *L, int64_t ldl, const double *Linv, int nb, int
             GPRAT_LAUNCH_CHECK();
         }
     }
+}
+
+}  // namespace
+
+void trsv_forward(const double *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, double *, cudaStream_t s)
+{
+    trsv_forward_t(L, ldl, Linv, nb, n, rhs, s);
+}
+
+void trsv_backward(const double *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, double *,
+                   cudaStream_t s)
+{
+    trsv_backward_t(L, ldl, Linv, nb, n, rhs, s);
+}
+
+void trsv_forward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s)
+{
+    trsv_forward_t(L, ldl, Linv, nb, n, rhs, s);
+}
+
+void trsv_backward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s)
+{
+    trsv_backward_t(L, ldl, Linv, nb, n, rhs, s);
 }
 
 void loss_kernel(const double *y, const double *alpha, const double *L, int64_t ldl, int n, DeviceParams *p,

@@ -1,0 +1,628 @@
+// tcgen05 tensor-core GEMM for the mixed-precision path (sm_100a).
+//
+//   C[MxN] (FP32, row-major) = beta*C + alpha * A B^T
+//   A (M x K), B (N x K): K-contiguous FP32 (kind::tf32) or BF16 (kind::f16)
+//
+// Persistent, warp-specialised CTA (192 threads, one CTA per SM):
+//   warp 0, one lane : TMA producer -- 128x128-byte tiles of A and B per
+//                      stage (128-byte swizzle), 6-stage ring, mbarrier
+//                      complete_tx accounting; no multicast;
+//   warp 1, one lane : MMA issuer -- 4 x tcgen05.mma (M=128, N=128) per
+//                      stage into a TMEM accumulator, tcgen05.commit frees the
+//                      smem stage; two accumulators (256 TMEM columns) so the
+//                      epilogue of tile i overlaps the MMAs of tile i+1;
+//   warps 2..5       : epilogue -- tcgen05.ld (32 lanes x 32 columns) of the
+//                      accumulator, release it, then C = beta*C + alpha*acc
+//                      (lower-triangle mask, optional FP64 row sums of squares).
+// Every mbarrier wait is bounded (about 2 s of device time); a wait that gives
+// up raises a CTA-wide abort flag, the roles leave their loops, in-flight
+// TMA copies are given time to land, the MMA issuer drains its own MMAs, the
+// TMEM is freed and the status word's timeout flag is set.
+#include "tc_gemm.cuh"
+
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+namespace gprat_cu
+{
+namespace
+{
+
+constexpr int TM = 128;
+constexpr int TN = 128;
+constexpr int TILE_BYTES = 128 * 128;  // one 128-row x 128-byte operand tile
+constexpr int STAGE_BYTES = 2 * TILE_BYTES;
+constexpr int STAGES = 6;
+constexpr int NUM_THREADS = 192;
+constexpr int TMEM_COLS = 2 * TN;
+constexpr unsigned long long WAIT_NS = 2000000000ull;  // bounded waits: 2 s
+constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity; false if it gave up
+// (or another role already aborted).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag)
+{
+    const unsigned long long t0 = global_ns();
+    for (uint32_t i = 0;; ++i)
+    {
+        if (mbar_try_wait(bar, parity))
+        {
+            return true;
+        }
+        if (*abort_flag)
+        {
+            return false;
+        }
+        if ((i & 255u) == 255u && global_ns() - t0 > WAIT_NS)
+        {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major operand tile with 128-byte swizzle: rows of 128 B, 8-row groups
+// 1024 B apart (stride byte offset), descriptor version 1 (sm_100).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+    d |= static_cast<uint64_t>(1) << 16;             // leading byte offset (unused for swizzled K-major)
+    d |= static_cast<uint64_t>(1024 >> 4) << 32;     // stride byte offset
+    d |= static_cast<uint64_t>(1) << 46;             // descriptor version
+    d |= static_cast<uint64_t>(2) << 61;             // SWIZZLE_128B
+    return d;
+}
+
+// Instruction descriptor: D = F32, A/B format (1 = BF16, 2 = TF32), both
+// K-major, N = 128, M = 128.
+__host__ __device__ constexpr uint32_t make_idesc(uint32_t fmt)
+{
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | (static_cast<uint32_t>(TN >> 3) << 17) |
+           (static_cast<uint32_t>(TM >> 4) << 24);
+}
+
+template <int KIND>
+__device__ __forceinline__ void mma_issue(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate)
+{
+    if (KIND == static_cast<int>(TcKind::TF32))
+    {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+    }
+    else
+    {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+    }
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v)
+{
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+    {
+        v[j] = __uint_as_float(r[j]);
+    }
+}
+
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void tile_of(int t, bool lower, int tiles_n, int &m0, int &n0)
+{
+    if (lower)
+    {
+        int i = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+        while ((i + 1) * (i + 2) / 2 <= t)
+        {
+            ++i;
+        }
+        while (i > 0 && i * (i + 1) / 2 > t)
+        {
+            --i;
+        }
+        m0 = i * TM;
+        n0 = (t - i * (i + 1) / 2) * TN;
+    }
+    else
+    {
+        m0 = (t / tiles_n) * TM;
+        n0 = (t % tiles_n) * TN;
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcGemmArgs p,
+                   int tiles_n, int ntiles)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t *tiles = smem;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *tfull = empty + STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint64_t *drain = tempty + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    constexpr int KSTAGE = (KIND == static_cast<int>(TcKind::TF32)) ? 32 : 64;  // elements per 128 bytes
+    constexpr uint32_t IDESC = make_idesc(KIND == static_cast<int>(TcKind::TF32) ? 2u : 1u);
+    const int kiters = p.K / KSTAGE;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < STAGES; ++s)
+        {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b)
+        {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 128);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            // ---------------- TMA producer ----------------
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+            int s = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; ok && t < ntiles; t += gridDim.x)
+            {
+                int m0, n0;
+                tile_of(t, p.lower, tiles_n, m0, n0);
+                for (int k = 0; k < kiters; ++k)
+                {
+                    if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(&full[s], STAGE_BYTES);
+                    uint8_t *st = tiles + s * STAGE_BYTES;
+                    tma_load_2d(st, &tmA, &full[s], p.a_col0 + k * KSTAGE, p.a_row0 + m0);
+                    tma_load_2d(st + TILE_BYTES, &tmB, &full[s], p.b_col0 + k * KSTAGE, p.b_row0 + n0);
+                    if (++s == STAGES)
+                    {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+            if (*abort_flag)
+            {
+                // give copies already in flight time to land before the CTA exits
+                const unsigned long long t0 = global_ns();
+                while (global_ns() - t0 < 200000ull)
+                {
+                }
+            }
+        }
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0)
+        {
+            // ---------------- MMA issuer ----------------
+            int s = 0;
+            uint32_t ph = 0;
+            uint32_t acc_ph[2] = { 0u, 0u };
+            bool ok = true;
+            int it = 0;
+            for (int t = blockIdx.x; ok && t < ntiles; t += gridDim.x, ++it)
+            {
+                const int b = it & 1;
+                if (!mbar_wait(&tempty[b], acc_ph[b] ^ 1u, abort_flag))
+                {
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem_base + static_cast<uint32_t>(b * TN);
+                for (int k = 0; k < kiters; ++k)
+                {
+                    if (!mbar_wait(&full[s], ph, abort_flag))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_addr = smem_u32(tiles + s * STAGE_BYTES);
+                    const uint64_t adesc = sw128_desc(a_addr);
+                    const uint64_t bdesc = sw128_desc(a_addr + TILE_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk)
+                    {
+                        // 32 bytes of K per instruction: advance the start address by 2 x 16 B
+                        mma_issue<KIND>(d, adesc + 2 * kk, bdesc + 2 * kk, IDESC, (k | kk) != 0 ? 1u : 0u);
+                    }
+                    mma_commit(&empty[s]);
+                    if (++s == STAGES)
+                    {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok)
+                {
+                    break;
+                }
+                mma_commit(&tfull[b]);
+                acc_ph[b] ^= 1u;
+            }
+            // drain: arrives once every MMA issued above has completed
+            mma_commit(drain);
+            mbar_wait(drain, 0u, abort_flag);
+        }
+    }
+    else
+    {
+        // ---------------- epilogue (warps 2..5) ----------------
+        const int q = warp & 3;  // TMEM lane quarter this warp may access
+        const int r_in = q * 32 + lane;
+        uint32_t acc_ph[2] = { 0u, 0u };
+        int it = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it)
+        {
+            const int b = it & 1;
+            int m0, n0;
+            tile_of(t, p.lower, tiles_n, m0, n0);
+            if (!mbar_wait(&tfull[b], acc_ph[b], abort_flag))
+            {
+                break;
+            }
+            tc_fence_after();
+            float v[TN];
+            const uint32_t taddr = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(b * TN);
+#pragma unroll
+            for (int c = 0; c < TN / 32; ++c)
+            {
+                tmem_ld32(taddr + c * 32, v + c * 32);
+            }
+            tmem_ld_wait();
+            tc_fence_before();
+            mbar_arrive(&tempty[b]);
+            acc_ph[b] ^= 1u;
+
+            const int row = m0 + r_in;
+            if (row < p.M)
+            {
+                float *crow = p.C + static_cast<int64_t>(row) * p.ldc + n0;
+                double sq = 0.0;
+#pragma unroll
+                for (int j4 = 0; j4 < TN; j4 += 4)
+                {
+                    const int col = n0 + j4;
+                    const bool full4 = (col + 3 < p.N) && (!p.lower || col + 3 <= row);
+                    if (full4)
+                    {
+                        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (p.beta != 0.0f)
+                        {
+                            o = *reinterpret_cast<const float4 *>(crow + j4);
+                        }
+                        float4 nv;
+                        nv.x = o.x + p.alpha * v[j4 + 0];
+                        nv.y = o.y + p.alpha * v[j4 + 1];
+                        nv.z = o.z + p.alpha * v[j4 + 2];
+                        nv.w = o.w + p.alpha * v[j4 + 3];
+                        *reinterpret_cast<float4 *>(crow + j4) = nv;
+                        sq += static_cast<double>(nv.x) * nv.x + static_cast<double>(nv.y) * nv.y +
+                              static_cast<double>(nv.z) * nv.z + static_cast<double>(nv.w) * nv.w;
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int e = 0; e < 4; ++e)
+                        {
+                            const int cc = col + e;
+                            if (cc < p.N && (!p.lower || cc <= row))
+                            {
+                                const float o = (p.beta != 0.0f) ? crow[j4 + e] : 0.0f;
+                                const float nv = o + p.alpha * v[j4 + e];
+                                crow[j4 + e] = nv;
+                                sq += static_cast<double>(nv) * nv;
+                            }
+                        }
+                    }
+                }
+                if (p.rowsq != nullptr)
+                {
+                    p.rowsq[row] += sq;
+                }
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+    {
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+    }
+    if (threadIdx.x == 0 && *abort_flag && p.status != nullptr)
+    {
+        atomicExch(&p.status->timeout, 1);
+    }
+}
+
+template <typename T>
+__global__ void convert_kernel(const T *__restrict__ src, int64_t lds, void *__restrict__ dst, int64_t ldd, int rows,
+                               int cols, int mode)
+{
+    const int64_t total = static_cast<int64_t>(rows) * cols;
+    for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < total;
+         q += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        const int64_t r = q / cols, c = q % cols;
+        const T v = src[r * lds + c];
+        if (mode == 0)
+        {
+            static_cast<float *>(dst)[r * ldd + c] = static_cast<float>(v);
+        }
+        else if (mode == 1)
+        {
+            static_cast<double *>(dst)[r * ldd + c] = static_cast<double>(v);
+        }
+        else
+        {
+            static_cast<__nv_bfloat16 *>(dst)[r * ldd + c] = __float2bfloat16_rn(static_cast<float>(v));
+        }
+    }
+}
+
+template <typename T>
+void launch_convert(const T *src, int64_t lds, void *dst, int64_t ldd, int rows, int cols, int mode, cudaStream_t s)
+{
+    if (rows <= 0 || cols <= 0)
+    {
+        return;
+    }
+    const int64_t total = static_cast<int64_t>(rows) * cols;
+    const int blocks = static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 16));
+    convert_kernel<T><<<blocks, 256, 0, s>>>(src, lds, dst, ldd, rows, cols, mode);
+    GPRAT_LAUNCH_CHECK();
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode()
+{
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once,
+                   []
+                   {
+                       void *p = nullptr;
+                       cudaDriverEntryPointQueryResult q;
+                       if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
+                                                            &q) == cudaSuccess &&
+                           q == cudaDriverEntryPointSuccess)
+                       {
+                           fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+                       }
+                   });
+    if (fn == nullptr)
+    {
+        throw Error(4, "cuTensorMapEncodeTiled is not available from the driver");
+    }
+    return fn;
+}
+
+int sm_count()
+{
+    int dev = 0, n = 0;
+    GPRAT_CUDA_CHECK(cudaGetDevice(&dev));
+    GPRAT_CUDA_CHECK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    return n;
+}
+
+}  // namespace
+
+void tc_make_operand(TcOperand &op, const void *base, int rows, int cols, int64_t ld, TcKind kind)
+{
+    const int esize = (kind == TcKind::TF32) ? 4 : 2;
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || ((ld * esize) & 15) || rows <= 0 || cols <= 0)
+    {
+        throw Error(1, "tc_make_operand: base must be 16-byte aligned and ld * element size a multiple of 16");
+    }
+    op.base = base;
+    op.rows = rows;
+    op.cols = cols;
+    op.ld = ld;
+    op.kind = kind;
+    cuuint64_t dims[2] = { static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows) };
+    cuuint64_t strides[1] = { static_cast<cuuint64_t>(ld * esize) };
+    cuuint32_t box[2] = { static_cast<cuuint32_t>(128 / esize), 128u };
+    cuuint32_t estrides[2] = { 1u, 1u };
+    CUresult r = get_encode()(&op.map, kind == TcKind::TF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                            : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16,
+                              2, const_cast<void *>(base), dims, strides, box, estrides,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+    {
+        throw Error(4, "cuTensorMapEncodeTiled failed with code " + std::to_string(static_cast<int>(r)));
+    }
+}
+
+void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cudaStream_t s)
+{
+    if (args.M <= 0 || args.N <= 0)
+    {
+        return;
+    }
+    if (A.kind != B.kind)
+    {
+        throw Error(1, "tc_gemm: A and B must have the same element type");
+    }
+    const int kstage = (A.kind == TcKind::TF32) ? 32 : 64;
+    if (args.K <= 0 || args.K % kstage != 0)
+    {
+        throw Error(1, "tc_gemm: K must be a positive multiple of " + std::to_string(kstage));
+    }
+    if ((args.a_col0 % kstage) || (args.b_col0 % kstage) || (args.ldc & 3) ||
+        (reinterpret_cast<uintptr_t>(args.C) & 15))
+    {
+        throw Error(1, "tc_gemm: K offsets must be stage aligned, C 16-byte aligned with ldc % 4 == 0");
+    }
+    if (args.a_col0 + args.K > A.cols || args.b_col0 + args.K > B.cols || args.a_row0 + args.M > A.rows ||
+        args.b_row0 + args.N > B.rows)
+    {
+        throw Error(1, "tc_gemm: tile range exceeds an operand");
+    }
+    if (args.lower && args.M != args.N)
+    {
+        throw Error(1, "tc_gemm: lower mode needs M == N");
+    }
+    if (args.rowsq != nullptr && (args.N > TN || args.lower))
+    {
+        throw Error(1, "tc_gemm: rowsq needs N <= 128");
+    }
+    if (!(args.beta == 0.0f || args.beta == 1.0f))
+    {
+        throw Error(1, "tc_gemm: beta must be 0 or 1");
+    }
+    const int tiles_m = ceil_div(args.M, TM);
+    const int tiles_n = ceil_div(args.N, TN);
+    const int ntiles = args.lower ? tiles_m * (tiles_m + 1) / 2 : tiles_m * tiles_n;
+    const int grid = std::min(ntiles, sm_count());
+    const bool timed = gemm_timing_enabled();
+    if (timed)
+    {
+        gemm_timing_begin(s);
+    }
+    if (A.kind == TcKind::TF32)
+    {
+        ensure_smem_attr(reinterpret_cast<const void *>(tc_gemm_kernel<0>), SMEM_BYTES);
+        tc_gemm_kernel<0><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(A.map, B.map, args, tiles_n, ntiles);
+    }
+    else
+    {
+        ensure_smem_attr(reinterpret_cast<const void *>(tc_gemm_kernel<1>), SMEM_BYTES);
+        tc_gemm_kernel<1><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(A.map, B.map, args, tiles_n, ntiles);
+    }
+    GPRAT_LAUNCH_CHECK();
+    if (timed)
+    {
+        const double mn = args.lower ? 0.5 * static_cast<double>(args.M) * (args.M + 1)
+                                     : static_cast<double>(args.M) * args.N;
+        gemm_timing_end(s, 2.0 * mn * args.K);
+    }
+}
+
+void convert_f64_to_f32(const double *src, int64_t lds, float *dst, int64_t ldd, int rows, int cols, cudaStream_t s)
+{
+    launch_convert<double>(src, lds, dst, ldd, rows, cols, 0, s);
+}
+
+void convert_f32_to_f64(const float *src, int64_t lds, double *dst, int64_t ldd, int rows, int cols, cudaStream_t s)
+{
+    launch_convert<float>(src, lds, dst, ldd, rows, cols, 1, s);
+}
+
+void convert_f32_to_bf16(const float *src, int64_t lds, void *dst, int64_t ldd, int rows, int cols, cudaStream_t s)
+{
+    launch_convert<float>(src, lds, dst, ldd, rows, cols, 2, s);
+}
+
+}  // namespace gprat_cu

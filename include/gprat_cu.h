@@ -232,6 +232,30 @@ int gprat_cu_stats_reset(void);
 int gprat_cu_stats_enable_timing(int enable);
 int gprat_cu_stats_read(int64_t *launches, int64_t *gemm_launches, double *gemm_ms, double *gemm_flops);
 
+/*
+ * Kernel-level test entry (no counterpart in the reference): runs the
+ * tcgen05 tensor-core GEMM of the mixed-precision path on the current
+ * device, C = beta*C + alpha * A B^T with host buffers A (M x K, lda),
+ * B (N x K, ldb), C (M x N, ldc; read when beta = 1, written back).
+ * kind 0 = TF32 operands, 1 = BF16 operands (rounded from the FP32 input).
+ * lower != 0: M == N and only C[i][j], i >= j, is written.  rowsq (optional,
+ * N <= 128): rowsq[i] += sum_j C_new[i][j]^2.  K must be a multiple of 64.
+ */
+int gprat_cu_test_tc_gemm(int kind,
+                          int M,
+                          int N,
+                          int K,
+                          const float *A,
+                          int64_t lda,
+                          const float *B,
+                          int64_t ldb,
+                          float *C,
+                          int64_t ldc,
+                          float alpha,
+                          float beta,
+                          int lower,
+                          double *rowsq);
+
 #ifdef __cplusplus
 }
 #endif
