@@ -320,6 +320,7 @@ def run_ours(args, wl):
         "gpu_launches": int(stats["launches"]),
         "clocks": clk,
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
+        "pcg_iterations": gp.pcg_iterations(),
         "sanity": sane,
     }
     print(json.dumps(line), flush=True)

@@ -69,11 +69,22 @@ def _load() -> ctypes.CDLL:
     lib.gprat_cu_fit_predict_device.argtypes = [ctypes.c_void_p, _dp, ctypes.c_void_p, _i64, ctypes.c_int,
                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     lib.gprat_cu_check_status.argtypes = [ctypes.c_void_p]
+    lib.gprat_cu_gp_pcg_iterations.argtypes = [ctypes.c_void_p, _ip]
     lib.gprat_cu_stats_enable_timing.argtypes = [ctypes.c_int]
     lib.gprat_cu_stats_read.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _dp, _dp]
     _fp = ctypes.POINTER(ctypes.c_float)
     lib.gprat_cu_test_tc_gemm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _fp, _i64, _fp,
                                           _i64, _fp, _i64, ctypes.c_float, ctypes.c_float, ctypes.c_int, _dp]
+    _vp, _i64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)
+    lib.gprat_cu_server_create.argtypes = [ctypes.c_int, _i64, ctypes.c_int, ctypes.POINTER(_vp)]
+    lib.gprat_cu_server_destroy.argtypes = [_vp]
+    lib.gprat_cu_server_add_model.argtypes = [_vp, _dp, _i64, _dp, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              _dp, _ip]
+    lib.gprat_cu_server_submit_predict.argtypes = [_vp, ctypes.c_int, _dp, _i64, ctypes.c_int, _i64p]
+    lib.gprat_cu_server_submit_fit.argtypes = [_vp, _dp, _i64, _dp, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               _dp, _i64p]
+    lib.gprat_cu_server_wait.argtypes = [_vp, _i64, _dp, _dp, _ip, _dp]
+    lib.gprat_cu_server_stats.argtypes = [_vp, _dp, _dp, _dp, _i64p, _i64p]
     return lib
 
 
@@ -248,3 +259,8 @@ class CudaGP:
 
     def check_status(self) -> None:
         check(lib.gprat_cu_check_status(self._h))
+
+    def pcg_iterations(self) -> int:
+        v = ctypes.c_int()
+        check(lib.gprat_cu_gp_pcg_iterations(self._h, ctypes.byref(v)))
+        return v.value

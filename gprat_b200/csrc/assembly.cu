@@ -29,7 +29,10 @@ __device__ __forceinline__ double se_entry(double dist, double neg_half_inv_l2, 
 }
 
 // Computes RB distances for rows i..i+RB-1 (local) and column j (local).
-__device__ __forceinline__ void distances(const double *xr, const double *xc, int i, int j, int d, double (&acc)[RB])
+// Row r's window starts at xr[r * rs]: rs = 1 for the sliding window of one
+// series, rs = d when every row's window was staged separately.
+__device__ __forceinline__ void distances(const double *xr, const double *xc, int i, int j, int d, int rs,
+                                          double (&acc)[RB])
 {
 #pragma unroll
     for (int r = 0; r < RB; ++r)
@@ -42,7 +45,7 @@ __device__ __forceinline__ void distances(const double *xr, const double *xc, in
 #pragma unroll
         for (int r = 0; r < RB; ++r)
         {
-            double z = __dsub_rn(xr[i + r + k], c);
+            double z = __dsub_rn(xr[(i + r) * rs + k], c);
             acc[r] = __dadd_rn(acc[r], __dmul_rn(z, z));
         }
     }
@@ -62,7 +65,8 @@ __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
                                                int64_t ldo,
                                                const double *__restrict__ alpha,
                                                double *__restrict__ mean_partial,
-                                               int mean_parts)
+                                               int mean_parts,
+                                               const int64_t *__restrict__ row_offsets)
 {
     extern __shared__ double sh[];
     const int i0 = blockIdx.y * AR;
@@ -76,13 +80,29 @@ __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
             return;
         }
     }
-    double *xr = sh;             // AR + d - 1
-    double *xc = sh + AR + d;    // AC + d - 1
-    double *red = xc + AC + d;   // AR x (AC/32) mean partials
-    for (int q = threadIdx.x; q < AR + d - 1; q += AC)
+    // Row windows: the sliding window of one series (xr[r .. r+d-1]), or, with
+    // row_offsets, each row's own window xrow[row_offsets[g] ..] staged at xr[r*d].
+    const int rs = (row_offsets != nullptr) ? d : 1;
+    const int xr_size = (row_offsets != nullptr) ? AR * d : AR + d;
+    double *xr = sh;                 // xr_size
+    double *xc = sh + xr_size;       // AC + d - 1
+    double *red = xc + AC + d;       // AR x (AC/32) mean partials
+    if (row_offsets != nullptr)
     {
-        int g = i0 + q;
-        xr[q] = (g < rows + d - 1) ? xrow[g] : 0.0;
+        for (int q = threadIdx.x; q < AR * d; q += AC)
+        {
+            const int r = q / d, k = q % d;
+            const int g = i0 + r;
+            xr[q] = (g < rows) ? xrow[row_offsets[g] + k] : 0.0;
+        }
+    }
+    else
+    {
+        for (int q = threadIdx.x; q < AR + d - 1; q += AC)
+        {
+            int g = i0 + q;
+            xr[q] = (g < rows + d - 1) ? xrow[g] : 0.0;
+        }
     }
     for (int q = threadIdx.x; q < AC + d - 1; q += AC)
     {
@@ -103,7 +123,7 @@ __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
     for (int i = 0; i < AR; i += RB)
     {
         double acc[RB];
-        distances(xr, xc, i, j, d, acc);
+        distances(xr, xc, i, j, d, rs, acc);
 #pragma unroll
         for (int r = 0; r < RB; ++r)
         {
@@ -171,17 +191,22 @@ __global__ void reduce_rows_kernel(const double *__restrict__ part, int m, int p
     }
 }
 
-size_t se_smem(int d) { return static_cast<size_t>(AR + d + AC + d + AR * (AC / 32)) * sizeof(double); }
+size_t se_smem(int d, bool per_row)
+{
+    const size_t xr = per_row ? static_cast<size_t>(AR) * d : static_cast<size_t>(AR + d);
+    return (xr + AC + d + AR * (AC / 32)) * sizeof(double);
+}
 
 template <int MODE, typename OutT>
 void launch_se(const double *xrow, int rows, const double *xcol, int cols, int d, int T, const DeviceParams *p,
-               OutT *out, int64_t ldo, const double *alpha, double *mean_partial, int parts, cudaStream_t s)
+               OutT *out, int64_t ldo, const double *alpha, double *mean_partial, int parts, cudaStream_t s,
+               const int64_t *row_offsets = nullptr)
 {
     if (rows <= 0 || cols <= 0)
     {
         return;
     }
-    size_t smem = se_smem(d);
+    size_t smem = se_smem(d, row_offsets != nullptr);
     if (smem > 227 * 1024)
     {
         throw Error(1, "too many regressors for the assembly kernel");
@@ -192,7 +217,7 @@ void launch_se(const double *xrow, int rows, const double *xcol, int cols, int d
     }
     dim3 grid(ceil_div(cols, AC), ceil_div(rows, AR));
     se_kernel<MODE, OutT><<<grid, AC, smem, s>>>(xrow, rows, xcol, cols, d, T, p, out, ldo, alpha, mean_partial,
-                                                 parts);
+                                                 parts, row_offsets);
     GPRAT_LAUNCH_CHECK();
 }
 
@@ -205,23 +230,25 @@ void assemble_covariance(const double *x, int n, int n_reg, int tile, const Devi
 }
 
 void assemble_cross(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, double *Kx,
-                    int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s)
+                    int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s,
+                    const int64_t *row_offsets)
 {
     if (mean_partial != nullptr && mean_parts != ceil_div(n, AC))
     {
         throw Error(1, "assemble_cross: mean_parts must be ceil(n/128)");
     }
-    launch_se<1>(xt, m, x, n, n_reg, 1, p, Kx, ldx, alpha, mean_partial, mean_parts, s);
+    launch_se<1>(xt, m, x, n, n_reg, 1, p, Kx, ldx, alpha, mean_partial, mean_parts, s, row_offsets);
 }
 
 void assemble_cross_f32(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, float *Kx,
-                        int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s)
+                        int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s,
+                        const int64_t *row_offsets)
 {
     if (mean_partial != nullptr && mean_parts != ceil_div(n, AC))
     {
         throw Error(1, "assemble_cross: mean_parts must be ceil(n/128)");
     }
-    launch_se<1>(xt, m, x, n, n_reg, 1, p, Kx, ldx, alpha, mean_partial, mean_parts, s);
+    launch_se<1>(xt, m, x, n, n_reg, 1, p, Kx, ldx, alpha, mean_partial, mean_parts, s, row_offsets);
 }
 
 void reduce_mean(const double *mean_partial, int m, int parts, double *mean, cudaStream_t s)

@@ -5,7 +5,7 @@
 #include <stdint.h>
 
 #include <mutex>
-#include <set>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -71,20 +71,22 @@ bool gemm_timing_enabled();
 void gemm_timing_begin(cudaStream_t s);
 void gemm_timing_end(cudaStream_t s, double flops);
 
-// Raises the dynamic shared-memory limit of `func` once per device.
+// Raises the dynamic shared-memory limit of `func` on the current device to
+// at least `bytes` (remembers the largest limit set per kernel and device).
 inline void ensure_smem_attr(const void *func, int bytes)
 {
     static std::mutex mtx;
-    static std::set<std::pair<const void *, int>> done;
+    static std::map<std::pair<const void *, int>, int> granted;
     int dev = 0;
     GPRAT_CUDA_CHECK(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lk(mtx);
-    if (done.count({ func, dev }) != 0)
+    auto it = granted.find({ func, dev });
+    if (it != granted.end() && it->second >= bytes)
     {
         return;
     }
     GPRAT_CUDA_CHECK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    done.insert({ func, dev });
+    granted[{ func, dev }] = bytes;
 }
 
 // Writes the whole parameter block from a kernel argument (no host staging
@@ -133,11 +135,15 @@ void assemble_covariance(const double *x, int n, int n_reg, int tile, const Devi
 // (gen_tile_cross_covariance, core/src/cpu/gp_algorithms.cpp:113-140).  If
 // alpha != nullptr, also mean[r] = sum_c Kx[r][c]*alpha[c]; if Kx == nullptr
 // the matrix is not stored.
+// row_offsets (optional, device, m entries): row r's window starts at
+// xt[row_offsets[r]] instead of xt[r] (rows gathered from several series).
 void assemble_cross(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, double *Kx,
-                    int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s);
+                    int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s,
+                    const int64_t *row_offsets = nullptr);
 // Same with the matrix stored in FP32 (the mean partials stay FP64).
 void assemble_cross_f32(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, float *Kx,
-                        int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s);
+                        int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s,
+                        const int64_t *row_offsets = nullptr);
 void reduce_mean(const double *mean_partial, int m, int parts, double *mean, cudaStream_t s);
 
 // Prior covariance matrix K**[r][c] = k(xt_r, xt_c) (gen_tile_full_prior_covariance,
@@ -157,6 +163,17 @@ void trsv_forward(const double *L, int64_t ldl, const double *Linv, int nb, int 
                   cudaStream_t s);
 void trsv_backward(const double *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, double *tmp,
                    cudaStream_t s);
+// Single-launch solves (trsv_fused.cu): one kernel per solve, row blocks
+// claimed by ticket, a progress counter between blocks.  flags: 2 ints of
+// scratch (zeroed by the call).  L in FP64 or FP32; x is FP64, in place.
+void trsv_fused_forward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+                        DeviceStatus *st, cudaStream_t s);
+void trsv_fused_backward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+                         DeviceStatus *st, cudaStream_t s);
+void trsv_fused_forward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+                            DeviceStatus *st, cudaStream_t s);
+void trsv_fused_backward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+                             DeviceStatus *st, cudaStream_t s);
 // Same with an FP32 factor (mixed precision); FP64 right-hand side and arithmetic.
 void trsv_forward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s);
 void trsv_backward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s);
@@ -165,8 +182,9 @@ void trsv_backward_f32(const float *L, int64_t ldl, const double *Linv, int nb, 
 void loss_kernel(const double *y, const double *alpha, const double *L, int64_t ldl, int n, DeviceParams *p,
                  cudaStream_t s);
 
-// var[r] = v - acc[r]
-void finalize_variance(const double *acc, int m, const DeviceParams *p, double *var, cudaStream_t s);
+// var[r] = v - acc[r] (- acc2[r] when acc2 != nullptr, added to acc[r] first)
+void finalize_variance(const double *acc, int m, const DeviceParams *p, double *var, cudaStream_t s,
+                       const double *acc2 = nullptr);
 
 // Fill helpers
 void set_identity(double *A, int64_t lda, int n, cudaStream_t s);

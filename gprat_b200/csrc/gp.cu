@@ -200,8 +200,9 @@ void solve_alpha_fp64(gprat_cu_gp *gp, cudaStream_t s)
 {
     GPRAT_CUDA_CHECK(
         cudaMemcpyAsync(gp->alpha.ptr, gp->y.ptr, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    trsv_forward(gp->K.ptr, gp->ld, gp->Linv.ptr, NB, gp->n, gp->alpha.ptr, nullptr, s);
-    trsv_backward(gp->K.ptr, gp->ld, gp->Linv.ptr, NB, gp->n, gp->alpha.ptr, nullptr, s);
+    gp->flags.ensure(gp->nblk + 1);
+    trsv_fused_forward(gp->K.ptr, gp->ld, gp->Linv.ptr, gp->n, gp->alpha.ptr, gp->flags.ptr, gp->status.ptr, s);
+    trsv_fused_backward(gp->K.ptr, gp->ld, gp->Linv.ptr, gp->n, gp->alpha.ptr, gp->flags.ptr, gp->status.ptr, s);
 }
 
 bool mixed(const gprat_cu_gp *gp) { return gp->precision != GPRAT_CU_PREC_FP64; }
@@ -272,7 +273,9 @@ void solve_right_lt(gprat_cu_gp *gp, double *W, int64_t ldw, int rows, double *r
 }
 
 // Mean (and variance if var != nullptr) for m test points at d_xt.
-void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
+// row_offsets (optional, device): row r's window starts at d_xt[row_offsets[r]].
+void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s,
+                    const int64_t *row_offsets = nullptr)
 {
     if (m <= 0)
     {
@@ -281,21 +284,21 @@ void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     const int parts = ceil_div(gp->n, 128);
     if (mixed(gp) && d_var != nullptr)
     {
-        variance_mixed(gp, d_xt, m, d_mean, d_var, s);
+        variance_mixed(gp, d_xt, m, d_mean, d_var, s, row_offsets);
         return;
     }
     gp->mean_part.ensure(static_cast<int64_t>(m) * parts);
     if (d_var == nullptr)
     {
         assemble_cross(d_xt, m, gp->x.ptr, gp->n, gp->d, gp->params.ptr, nullptr, 0, gp->alpha.ptr,
-                       gp->mean_part.ptr, parts, s);
+                       gp->mean_part.ptr, parts, s, row_offsets);
         reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
         return;
     }
     gp->W.ensure(static_cast<int64_t>(m) * gp->ld);
     gp->vacc.ensure(m);
     assemble_cross(d_xt, m, gp->x.ptr, gp->n, gp->d, gp->params.ptr, gp->W.ptr, gp->ld, gp->alpha.ptr,
-                   gp->mean_part.ptr, parts, s);
+                   gp->mean_part.ptr, parts, s, row_offsets);
     reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
     GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->vacc.ptr, 0, m * sizeof(double), s));
     solve_right_lt(gp, gp->W.ptr, gp->ld, m, gp->vacc.ptr, [m](int) { return m; }, s);
@@ -366,6 +369,54 @@ namespace gprat_cu
 {
 // Lets other entry points of the library report through gprat_cu_last_error().
 void set_last_error(const std::string &message) { g_last_error = message; }
+}  // namespace gprat_cu
+
+namespace gprat_cu
+{
+// Internal entry points used by the serving layer (serve.cu).
+void gp_fit(gprat_cu_gp *gp, const double hyper[3], cudaStream_t s)
+{
+    upload_hyper(gp, hyper, s);
+    fit(gp, s);
+}
+
+void gp_predict_batch(gprat_cu_gp *gp, const double *d_series, const int64_t *d_row_offsets, int m, double *d_mean,
+                      double *d_var, cudaStream_t s)
+{
+    predict_device(gp, d_series, m, d_mean, d_var, s, d_row_offsets);
+}
+
+void gp_check(gprat_cu_gp *gp, cudaStream_t s)
+{
+    GPRAT_CUDA_CHECK(cudaMemcpyAsync(gp->h_status, gp->status.ptr, sizeof(DeviceStatus), cudaMemcpyDeviceToHost, s));
+    GPRAT_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (gp->h_status->not_spd_row != 0)
+    {
+        throw Error(GPRAT_CU_ERR_NOT_SPD, "Cholesky factorisation failed: covariance matrix is not positive definite");
+    }
+    if (gp->h_status->timeout != 0)
+    {
+        throw Error(GPRAT_CU_ERR_TIMEOUT, "a bounded device wait timed out");
+    }
+}
+
+int64_t gp_resident_bytes(const gprat_cu_gp *gp)
+{
+    int64_t b = static_cast<int64_t>(gp->n) * gp->ld * 8 + static_cast<int64_t>(gp->nblk) * NB * NB * 8;
+    if (gp->precision != GPRAT_CU_PREC_FP64)
+    {
+        b += static_cast<int64_t>(gp->n) * gp->ld32 * (gp->precision == GPRAT_CU_PREC_MIXED_BF16 ? 6 : 4);
+    }
+    return b;
+}
+
+int64_t gp_predict_bytes(const gprat_cu_gp *gp, int m)
+{
+    // solve matrix + mean partials + variance accumulator for m rows
+    const int64_t w = gp->precision == GPRAT_CU_PREC_FP64 ? static_cast<int64_t>(m) * gp->ld * 8
+                                                          : static_cast<int64_t>(m) * gp->ld32 * 4;
+    return w + static_cast<int64_t>(m) * (ceil_div(gp->n, 128) + 2) * 8;
+}
 }  // namespace gprat_cu
 
 extern "C" {
@@ -763,6 +814,17 @@ int gprat_cu_fit_predict_device(gprat_cu_gp *gp, const double hyper[3], const do
             upload_hyper(gp, hyper, s);
             fit(gp, s);
             predict_device(gp, d_test_in, m, d_mean, d_var, s);
+        });
+}
+
+int gprat_cu_gp_pcg_iterations(gprat_cu_gp *gp, int *iterations)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(iterations != nullptr, "iterations must not be NULL");
+            *iterations = mixed(gp) ? gp->pcg_last_iters : 0;
         });
 }
 

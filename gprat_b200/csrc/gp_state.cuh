@@ -84,6 +84,7 @@ struct gprat_cu_gp
     gprat_cu::DevBuf<double> pcg_r, pcg_z, pcg_p, pcg_q, symv_part;
     gprat_cu::DevBuf<gprat_cu::PcgScalars> pcg_s;
     int pcg_last_iters = 0;
+    gprat_cu::DevBuf<int> flags;  // ticket + ready flags of the single-launch solves
 
     ~gprat_cu_gp()
     {
@@ -105,6 +106,7 @@ struct gprat_cu_gp
         Lb.release();
         Wb.release();
         pcg_s.release();
+        flags.release();
         params.release();
         status.release();
         if (h_params != nullptr)
@@ -132,7 +134,16 @@ namespace gprat_cu
 // mixed.cu
 void factor_mixed(gprat_cu_gp *gp, cudaStream_t s);
 void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s);
-void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s);
+void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s,
+                    const int64_t *row_offsets = nullptr);
+
+// gp.cu: internal entry points for the serving layer (serve.cu)
+void gp_fit(gprat_cu_gp *gp, const double hyper[3], cudaStream_t s);
+void gp_predict_batch(gprat_cu_gp *gp, const double *d_series, const int64_t *d_row_offsets, int m, double *d_mean,
+                      double *d_var, cudaStream_t s);
+void gp_check(gprat_cu_gp *gp, cudaStream_t s);
+int64_t gp_resident_bytes(const gprat_cu_gp *gp);
+int64_t gp_predict_bytes(const gprat_cu_gp *gp, int m);
 void loss_mixed(gprat_cu_gp *gp, cudaStream_t s);
 
 }  // namespace gprat_cu

@@ -72,6 +72,7 @@ TcGemmArgs tc_args(int M, int N, int K, int ar, int ac, int br, int bc, float *C
     g.beta = beta;
     g.lower = lower;
     g.rowsq = rowsq;
+    g.rowsq_half = M;
     g.status = st;
     return g;
 }
@@ -313,8 +314,9 @@ void symv(gprat_cu_gp *gp, const double *p, double *q, cudaStream_t s)
 void precondition(gprat_cu_gp *gp, const double *r, double *z, cudaStream_t s)
 {
     GPRAT_CUDA_CHECK(cudaMemcpyAsync(z, r, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    trsv_forward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, NB, gp->n, z, s);
-    trsv_backward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, NB, gp->n, z, s);
+    gp->flags.ensure(gp->nblk + 1);
+    trsv_fused_forward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, gp->n, z, gp->flags.ptr, gp->status.ptr, s);
+    trsv_fused_backward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, gp->n, z, gp->flags.ptr, gp->status.ptr, s);
 }
 
 }  // namespace
@@ -455,14 +457,15 @@ void loss_mixed(gprat_cu_gp *gp, cudaStream_t s)
     loss_kernel(gp->y.ptr, gp->alpha.ptr, gp->D64.ptr + NB * NB, 0, gp->n, gp->params.ptr, s);
 }
 
-void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
+void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s,
+                    const int64_t *row_offsets)
 {
     const int n = gp->n;
     const int64_t ld32 = gp->ld32;
     const int parts = ceil_div(n, 128);
     gp->mean_part.ensure(static_cast<int64_t>(m) * parts);
     gp->W32.ensure(static_cast<int64_t>(m) * ld32);
-    gp->vacc.ensure(m);
+    gp->vacc.ensure(2 * static_cast<int64_t>(m));  // one accumulator per column half of the GEMM tile
     const bool bf16 = gp->precision == GPRAT_CU_PREC_MIXED_BF16;
     if (bf16)
     {
@@ -470,13 +473,13 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     }
     float *W = gp->W32.ptr;
     assemble_cross_f32(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, W, ld32, gp->alpha.ptr, gp->mean_part.ptr,
-                       parts, s);
+                       parts, s, row_offsets);
     reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
     if (d_var == nullptr)
     {
         return;
     }
-    GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->vacc.ptr, 0, m * sizeof(double), s));
+    GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->vacc.ptr, 0, 2 * m * sizeof(double), s));
     const MixedOps ops = make_ops(gp);
     TcOperand opW, opWb;
     tc_make_operand(opW, W, m, static_cast<int>(ld32), ld32, TcKind::TF32);
@@ -518,7 +521,7 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
                     s);
         }
     }
-    finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, s);
+    finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, s, gp->vacc.ptr + m);
 }
 
 }  // namespace gprat_cu

@@ -2,7 +2,7 @@
 //
 // Replaces the per-tile potrf task (LAPACKE_dpotrf2 'L',
 // core/src/cpu/adapter_cblas_fp64.cpp:14-22; cusolverDnXpotrf,
-// core/src/gpu/adapter_cublas.cu:9-79).  One CTA of 16 warps loads the lower
+// core/src/gpu/adapter_cublas.cu:9-79).  One CTA of 8 warps loads the lower
 // triangle of a bs x bs (bs <= 128) diagonal block into shared memory and
 // factors it in 32-wide sub-blocks:
 //   1. warp 0 factors the 32 x 32 diagonal sub-block in registers (lane i
@@ -31,7 +31,7 @@ constexpr int SB = 32;      // sub-block width
 constexpr int XS = SB + 1;  // smem row stride of a sub-block inverse
 constexpr int TS = 96 + 1;  // smem row stride of the inverse temporary
 constexpr int XBLK = (SB + 1) * XS;  // one sub-block inverse plus its 1/L_ii row
-constexpr int PTHREADS = 512;
+constexpr int PTHREADS = 256;
 
 // Warp 0: factor a[c0.., c0..] (w x w, w <= 32) in registers, write L back
 // to smem, and store X = L^-1 (32 x 32, zero above the diagonal) in xinv.
@@ -62,8 +62,9 @@ __device__ __forceinline__ void warp_factor_invert(double *a, int c0, int w, int
         {
             *bad = row0 + c0 + j + 1;
         }
-        const double d = sqrt(ajj);
-        const double inv = 1.0 / d;
+        // one reciprocal square root per pivot keeps the serial chain short
+        const double inv = rsqrt(ajj);
+        const double d = ajj * inv;
         if (lane == j)
         {
             r[j] = d;
@@ -132,6 +133,7 @@ __global__ void __launch_bounds__(PTHREADS) potrf_inv_kernel(double *__restrict_
     {
         bad = 0;
     }
+#pragma unroll 8
     for (int q = tid; q < bs * bs; q += PTHREADS)
     {
         int i = q / bs, c = q % bs;
@@ -156,9 +158,11 @@ __global__ void __launch_bounds__(PTHREADS) potrf_inv_kernel(double *__restrict_
         {
             break;
         }
-        // panel solve: P = P X^T (4 threads per row, 8 output columns each)
+        // panel solve: P = P X^T (4 threads per row, 8 output columns each;
+        // rows in passes of PTHREADS/4, each pass reads before it writes)
+        for (int pass = 0; pass * (PTHREADS / 4) < R; ++pass)
         {
-            const int row = tid >> 2, grp = tid & 3;
+            const int row = pass * (PTHREADS / 4) + (tid >> 2), grp = tid & 3;
             double v[SB];
             if (row < R)
             {
@@ -214,6 +218,7 @@ __global__ void __launch_bounds__(PTHREADS) potrf_inv_kernel(double *__restrict_
         atomicCAS(&status->not_spd_row, 0, bad);
     }
     // write L (lower triangle incl. diagonal) back
+#pragma unroll 8
     for (int q = tid; q < bs * bs; q += PTHREADS)
     {
         int i = q / bs, c = q % bs;
@@ -265,6 +270,7 @@ __global__ void __launch_bounds__(PTHREADS) potrf_inv_kernel(double *__restrict_
         }
         __syncthreads();
     }
+#pragma unroll 8
     for (int q = tid; q < bs * bs; q += PTHREADS)
     {
         int i = q / bs, c = q % bs;

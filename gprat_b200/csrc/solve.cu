@@ -170,14 +170,15 @@ __global__ void __launch_bounds__(1024) loss_kernel_impl(const double *__restric
     }
 }
 
-__global__ void finalize_var_kernel(const double *__restrict__ acc, int m, const DeviceParams *__restrict__ p,
-                                    double *__restrict__ var)
+__global__ void finalize_var_kernel(const double *__restrict__ acc, const double *__restrict__ acc2, int m,
+                                    const DeviceParams *__restrict__ p, double *__restrict__ var)
 {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < m)
     {
         // gen_tile_prior_covariance gives k(x,x) = v (core/src/cpu/gp_algorithms.cpp:90-111)
-        var[r] = p->hyper[1] - acc[r];
+        const double a = acc2 != nullptr ? acc[r] + acc2[r] : acc[r];
+        var[r] = p->hyper[1] - a;
     }
 }
 
@@ -266,13 +267,14 @@ void loss_kernel(const double *y, const double *alpha, const double *L, int64_t 
     GPRAT_LAUNCH_CHECK();
 }
 
-void finalize_variance(const double *acc, int m, const DeviceParams *p, double *var, cudaStream_t s)
+void finalize_variance(const double *acc, int m, const DeviceParams *p, double *var, cudaStream_t s,
+                       const double *acc2)
 {
     if (m <= 0)
     {
         return;
     }
-    finalize_var_kernel<<<ceil_div(m, 256), 256, 0, s>>>(acc, m, p, var);
+    finalize_var_kernel<<<ceil_div(m, 256), 256, 0, s>>>(acc, acc2, m, p, var);
     GPRAT_LAUNCH_CHECK();
 }
 

@@ -3,17 +3,19 @@
 //   C[MxN] (FP32, row-major) = beta*C + alpha * A B^T
 //   A (M x K), B (N x K): K-contiguous FP32 (kind::tf32) or BF16 (kind::f16)
 //
-// Persistent, warp-specialised CTA (192 threads, one CTA per SM):
+// Persistent, warp-specialised CTA (320 threads, one CTA per SM):
 //   warp 0, one lane : TMA producer -- 128x128-byte tiles of A and B per
-//                      stage (128-byte swizzle), 6-stage ring, mbarrier
+//                      stage (128-byte swizzle), 7-stage ring, mbarrier
 //                      complete_tx accounting; no multicast;
 //   warp 1, one lane : MMA issuer -- 4 x tcgen05.mma (M=128, N=128) per
 //                      stage into a TMEM accumulator, tcgen05.commit frees the
 //                      smem stage; two accumulators (256 TMEM columns) so the
 //                      epilogue of tile i overlaps the MMAs of tile i+1;
-//   warps 2..5       : epilogue -- tcgen05.ld (32 lanes x 32 columns) of the
-//                      accumulator, release it, then C = beta*C + alpha*acc
-//                      (lower-triangle mask, optional FP64 row sums of squares).
+//   warps 2..9       : epilogue -- two warps per TMEM lane quarter, 64 columns
+//                      each: tcgen05.ld of the accumulator, release it, then
+//                      C = beta*C + alpha*acc with every C load of the row
+//                      segment issued before the first store (lower-triangle
+//                      mask, optional FP64 row sums of squares).
 // Every mbarrier wait is bounded (about 2 s of device time); a wait that gives
 // up raises a CTA-wide abort flag, the roles leave their loops, in-flight
 // TMA copies are given time to land, the MMA issuer drains its own MMAs, the
@@ -34,8 +36,9 @@ constexpr int TM = 128;
 constexpr int TN = 128;
 constexpr int TILE_BYTES = 128 * 128;  // one 128-row x 128-byte operand tile
 constexpr int STAGE_BYTES = 2 * TILE_BYTES;
-constexpr int STAGES = 6;
-constexpr int NUM_THREADS = 192;
+constexpr int STAGES = 7;
+constexpr int NUM_THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
+constexpr int EPI_COLS = 64;     // columns per epilogue warp
 constexpr int TMEM_COLS = 2 * TN;
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // bounded waits: 2 s
 constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256;
@@ -240,7 +243,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         for (int b = 0; b < 2; ++b)
         {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 128);
+            mbar_init(&tempty[b], 256);
         }
         mbar_init(drain, 1);
         *abort_flag = 0;
@@ -356,8 +359,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     }
     else
     {
-        // ---------------- epilogue (warps 2..5) ----------------
+        // ---------------- epilogue (warps 2..9) ----------------
+        // two warps per TMEM lane quarter, each owning 64 of the 128 columns
+        const int ew = warp - 2;
         const int q = warp & 3;  // TMEM lane quarter this warp may access
+        const int h = ew >> 2;   // column half
         const int r_in = q * 32 + lane;
         uint32_t acc_ph[2] = { 0u, 0u };
         int it = 0;
@@ -371,10 +377,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 break;
             }
             tc_fence_after();
-            float v[TN];
-            const uint32_t taddr = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(b * TN);
+            float v[EPI_COLS];
+            const uint32_t taddr = tmem_base + (static_cast<uint32_t>(q * 32) << 16) +
+                                   static_cast<uint32_t>(b * TN + h * EPI_COLS);
 #pragma unroll
-            for (int c = 0; c < TN / 32; ++c)
+            for (int c = 0; c < EPI_COLS / 32; ++c)
             {
                 tmem_ld32(taddr + c * 32, v + c * 32);
             }
@@ -384,50 +391,53 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             acc_ph[b] ^= 1u;
 
             const int row = m0 + r_in;
-            if (row < p.M)
+            const int c0 = n0 + h * EPI_COLS;
+            if (row < p.M && c0 < p.N)
             {
-                float *crow = p.C + static_cast<int64_t>(row) * p.ldc + n0;
+                float *crow = p.C + static_cast<int64_t>(row) * p.ldc + c0;
                 double sq = 0.0;
-#pragma unroll
-                for (int j4 = 0; j4 < TN; j4 += 4)
+                const bool fast = (c0 + EPI_COLS - 1 < p.N) && (!p.lower || c0 + EPI_COLS - 1 <= row);
+                if (fast)
                 {
-                    const int col = n0 + j4;
-                    const bool full4 = (col + 3 < p.N) && (!p.lower || col + 3 <= row);
-                    if (full4)
+                    // issue every load of the segment before the first store
+                    float4 cv[EPI_COLS / 4];
+#pragma unroll
+                    for (int j = 0; j < EPI_COLS / 4; ++j)
                     {
-                        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (p.beta != 0.0f)
-                        {
-                            o = *reinterpret_cast<const float4 *>(crow + j4);
-                        }
+                        cv[j] = (p.beta != 0.0f) ? __ldcg(reinterpret_cast<const float4 *>(crow) + j)
+                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+#pragma unroll
+                    for (int j = 0; j < EPI_COLS / 4; ++j)
+                    {
                         float4 nv;
-                        nv.x = o.x + p.alpha * v[j4 + 0];
-                        nv.y = o.y + p.alpha * v[j4 + 1];
-                        nv.z = o.z + p.alpha * v[j4 + 2];
-                        nv.w = o.w + p.alpha * v[j4 + 3];
-                        *reinterpret_cast<float4 *>(crow + j4) = nv;
+                        nv.x = cv[j].x + p.alpha * v[4 * j + 0];
+                        nv.y = cv[j].y + p.alpha * v[4 * j + 1];
+                        nv.z = cv[j].z + p.alpha * v[4 * j + 2];
+                        nv.w = cv[j].w + p.alpha * v[4 * j + 3];
+                        __stcg(reinterpret_cast<float4 *>(crow) + j, nv);
                         sq += static_cast<double>(nv.x) * nv.x + static_cast<double>(nv.y) * nv.y +
                               static_cast<double>(nv.z) * nv.z + static_cast<double>(nv.w) * nv.w;
                     }
-                    else
-                    {
+                }
+                else
+                {
 #pragma unroll
-                        for (int e = 0; e < 4; ++e)
+                    for (int j = 0; j < EPI_COLS; ++j)
+                    {
+                        const int cc = c0 + j;
+                        if (cc < p.N && (!p.lower || cc <= row))
                         {
-                            const int cc = col + e;
-                            if (cc < p.N && (!p.lower || cc <= row))
-                            {
-                                const float o = (p.beta != 0.0f) ? crow[j4 + e] : 0.0f;
-                                const float nv = o + p.alpha * v[j4 + e];
-                                crow[j4 + e] = nv;
-                                sq += static_cast<double>(nv) * nv;
-                            }
+                            const float o = (p.beta != 0.0f) ? crow[j] : 0.0f;
+                            const float nv = o + p.alpha * v[j];
+                            crow[j] = nv;
+                            sq += static_cast<double>(nv) * nv;
                         }
                     }
                 }
                 if (p.rowsq != nullptr)
                 {
-                    p.rowsq[row] += sq;
+                    p.rowsq[h * p.rowsq_half + row] += sq;  // single writer per word and launch
                 }
             }
         }
@@ -574,9 +584,9 @@ void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cud
     {
         throw Error(1, "tc_gemm: lower mode needs M == N");
     }
-    if (args.rowsq != nullptr && (args.N > TN || args.lower))
+    if (args.rowsq != nullptr && (args.N > TN || args.lower || args.rowsq_half < args.M))
     {
-        throw Error(1, "tc_gemm: rowsq needs N <= 128");
+        throw Error(1, "tc_gemm: rowsq needs N <= 128 and rowsq_half >= M");
     }
     if (!(args.beta == 0.0f || args.beta == 1.0f))
     {

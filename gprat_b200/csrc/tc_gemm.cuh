@@ -42,7 +42,11 @@ struct TcGemmArgs
     int64_t ldc;
     float alpha, beta;  // beta must be 0 or 1
     bool lower;         // M == N; only C[i][j] with i >= j is written, tiles above the diagonal skipped
-    double *rowsq;      // optional (N <= 128): rowsq[i] += sum_j C_new[i][j]^2
+    // optional (N <= 128): per-row sums of squares of the new C, split by
+    // column half so that no two threads add into one word (deterministic):
+    // rowsq[i] += sum_{j<64} C_new[i][j]^2, rowsq[rowsq_half + i] += sum_{j>=64} ...
+    double *rowsq;
+    int64_t rowsq_half;  // >= M when rowsq is set
     DeviceStatus *status;  // receives the timeout flag if a bounded wait gives up
 };
 

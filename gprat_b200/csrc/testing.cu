@@ -56,9 +56,11 @@ extern "C" int gprat_cu_test_tc_gemm(int kind, int M, int N, int K, const float 
         GPRAT_CUDA_CHECK(cudaMemcpy2D(dC.p, lc * 4, C, ldc * 4, N * 4, M, cudaMemcpyHostToDevice));
         Buf dStatus(sizeof(DeviceStatus));
         GPRAT_CUDA_CHECK(cudaMemset(dStatus.p, 0, sizeof(DeviceStatus)));
-        Buf dRow(static_cast<size_t>(M) * sizeof(double));
+        // two column-half accumulators: the caller's values in the first, zeros in the second
+        Buf dRow(2 * static_cast<size_t>(M) * sizeof(double));
         if (rowsq != nullptr)
         {
+            GPRAT_CUDA_CHECK(cudaMemset(dRow.p, 0, 2 * static_cast<size_t>(M) * sizeof(double)));
             GPRAT_CUDA_CHECK(cudaMemcpy(dRow.p, rowsq, M * sizeof(double), cudaMemcpyHostToDevice));
         }
         TcOperand oa, ob;
@@ -85,6 +87,7 @@ extern "C" int gprat_cu_test_tc_gemm(int kind, int M, int N, int K, const float 
         g.beta = beta;
         g.lower = lower != 0;
         g.rowsq = rowsq != nullptr ? static_cast<double *>(dRow.p) : nullptr;
+        g.rowsq_half = M;
         g.status = static_cast<DeviceStatus *>(dStatus.p);
         tc_gemm(oa, ob, g, s);
         GPRAT_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -97,7 +100,12 @@ extern "C" int gprat_cu_test_tc_gemm(int kind, int M, int N, int K, const float 
         GPRAT_CUDA_CHECK(cudaMemcpy2D(C, ldc * 4, dC.p, lc * 4, N * 4, M, cudaMemcpyDeviceToHost));
         if (rowsq != nullptr)
         {
-            GPRAT_CUDA_CHECK(cudaMemcpy(rowsq, dRow.p, M * sizeof(double), cudaMemcpyDeviceToHost));
+            std::vector<double> halves(2 * static_cast<size_t>(M));
+            GPRAT_CUDA_CHECK(cudaMemcpy(halves.data(), dRow.p, halves.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int i = 0; i < M; ++i)
+            {
+                rowsq[i] = halves[i] + halves[M + i];
+            }
         }
         set_last_error("");
         return GPRAT_CU_OK;

@@ -1,0 +1,379 @@
+// Single-launch blocked triangular solves L x = b and L^T x = b (FP64 right-
+// hand side; L in FP64 or FP32, row-major lower triangle; FP64 inverses of
+// the 128 x 128 diagonal blocks).
+//
+// forward_solve_tiled / backward_solve_tiled (core/src/cpu/tiled_algorithms.cpp:61-115)
+// walk the block columns one after another.  Launching one kernel per block
+// makes the solve launch-latency bound (two launches per 128 rows).  Here one
+// kernel does the whole solve:
+//   * every CTA takes a row block by atomic ticket (tickets follow launch
+//     order, so a CTA only ever waits for CTAs that are already running);
+//   * before it waits for anything it starts the asynchronous copy of its
+//     diagonal inverse into shared memory (lower triangle, packed);
+//   * it accumulates L_ij x_j over the blocks j it depends on; the loads of
+//     each tile of L are issued before the wait for x_j, so the DRAM latency
+//     overlaps the wait;
+//   * x_i = Linv_ii (b_i - sum_j L_ij x_j) from shared memory, then x_i is
+//     published by a release (threadfence) and the progress counter (number of
+//     finished blocks; blocks finish in solve order) is advanced.
+// L is read exactly once per solve.  Waits are bounded; a wait that runs out
+// sets the status word's timeout flag (the caller reports an error).
+#include "common.cuh"
+
+namespace gprat_cu
+{
+namespace
+{
+
+constexpr int FT = 256;  // threads per CTA (8 warps)
+constexpr int FB = 128;  // block size
+constexpr long long SPIN_LIMIT = 1ll << 24;  // with 64 ns sleeps: about 1-2 s
+
+// Packed lower triangle of a 128 x 128 FP64 block: row r holds columns
+// 0..r padded to an even count, so every row starts on a 16-byte boundary.
+__host__ __device__ constexpr int packed_off(int r)
+{
+    return (r >> 1) * (r >> 1) * 2 + 2 * (r >> 1) + (r & 1) * (2 * (r >> 1) + 2);
+}
+constexpr int PACKED = packed_off(FB);  // 8320 doubles
+constexpr size_t SMEM_BYTES = (PACKED + 2 * FB + (FT / 32) * FB) * sizeof(double) + 16;
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Starts the copy of Linv_ii's lower triangle into the packed layout.
+__device__ __forceinline__ void load_diag_inverse(double *dst, const double *Li)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int r = warp; r < FB; r += FT / 32)
+    {
+        const int pairs = (r + 2) >> 1;
+        for (int c2 = lane; c2 < pairs; c2 += 32)
+        {
+            cp_async16(dst + packed_off(r) + 2 * c2, Li + r * FB + 2 * c2);
+        }
+    }
+}
+
+// Thread 0 waits until *progress >= target; returns the value it saw (or
+// target after a timeout, with the status flag set).
+__device__ __forceinline__ int wait_progress(const volatile int *progress, int target, DeviceStatus *st)
+{
+    long long spins = 0;
+    int v = *progress;
+    while (v < target)
+    {
+        if (++spins > SPIN_LIMIT)
+        {
+            if (st != nullptr)
+            {
+                atomicExch(&st->timeout, 1);
+            }
+            return target;
+        }
+        __nanosleep(64);
+        v = *progress;
+    }
+    __threadfence();
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ double to_d(T v)
+{
+    return static_cast<double>(v);
+}
+
+// flags[0] = ticket counter, flags[1] = progress (finished blocks).
+template <typename T>
+__global__ void __launch_bounds__(FT, 1) trsv_fwd_fused_kernel(const T *__restrict__ L, int64_t ld,
+                                                               const double *__restrict__ Linv, int n, double *x,
+                                                               int *flags, DeviceStatus *st)
+{
+    extern __shared__ __align__(16) double sm[];
+    double *linv_s = sm;              // packed lower triangle of Linv_ii
+    double *rhs = linv_s + PACKED;    // b_i, then b_i - sum_j L_ij x_j
+    int *shared_int = reinterpret_cast<int *>(rhs + 2 * FB + (FT / 32) * FB);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0)
+    {
+        shared_int[0] = atomicAdd(flags, 1);
+    }
+    __syncthreads();
+    const int i = shared_int[0];
+    const int r0 = i * FB;
+    const int bs = min(FB, n - r0);
+    load_diag_inverse(linv_s, Linv + static_cast<int64_t>(i) * FB * FB);
+    if (tid < FB)
+    {
+        rhs[tid] = (tid < bs) ? x[r0 + tid] : 0.0;
+    }
+    __syncthreads();  // rhs rows are updated below by other threads
+
+    // rows warp + 8q of the block; lanes own columns lane + 32c
+    constexpr int QB = sizeof(T) == 4 ? 16 : 8;  // rows per batch (registers)
+    double part[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+    {
+        part[q] = 0.0;
+    }
+    int seen = 0;  // progress observed so far
+    for (int j = 0; j < i; ++j)
+    {
+        const int c0 = j * FB;
+#pragma unroll
+        for (int qb = 0; qb < 16; qb += QB)
+        {
+            T v[QB][4];
+#pragma unroll
+            for (int q = 0; q < QB; ++q)
+            {
+                const int r = warp + 8 * (qb + q);
+                const T *lr = L + static_cast<int64_t>(r0 + min(r, bs - 1)) * ld + c0 + lane;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                {
+                    v[q][c] = lr[32 * c];
+                }
+            }
+            if (qb == 0 && j >= seen)
+            {
+                if (tid == 0)
+                {
+                    shared_int[1] = wait_progress(flags + 1, j + 1, st);
+                }
+                __syncthreads();
+                seen = shared_int[1];
+                __syncthreads();
+            }
+            double xv[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                xv[c] = __ldcg(x + c0 + lane + 32 * c);
+            }
+#pragma unroll
+            for (int q = 0; q < QB; ++q)
+            {
+                double s = 0.0;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                {
+                    s += to_d(v[q][c]) * xv[c];
+                }
+                part[qb + q] += s;
+            }
+        }
+    }
+    // reduce the lane partials of each row
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+    {
+        double s = part[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+        }
+        part[q] = s;
+    }
+    if (lane == 0)
+    {
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+        {
+            rhs[warp + 8 * q] -= part[q];
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // x_i[r] = sum_{c <= r} Linv[r][c] rhs[c]; two threads per row, 64 columns each
+    {
+        const int r = tid >> 1, h = tid & 1;
+        const double *lr = linv_s + packed_off(r);
+        double s = 0.0;
+        const int cend = min(r, 64 * h + 63);
+        for (int c = 64 * h; c <= cend; ++c)
+        {
+            s += lr[c] * rhs[c];
+        }
+        s += __shfl_xor_sync(0xffffffffu, s, 1);
+        if (h == 0 && r < bs)
+        {
+            x[r0 + r] = s;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0)
+    {
+        atomicMax(flags + 1, i + 1);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FT, 1) trsv_bwd_fused_kernel(const T *__restrict__ L, int64_t ld,
+                                                               const double *__restrict__ Linv, int n, int nblk,
+                                                               double *x, int *flags, DeviceStatus *st)
+{
+    extern __shared__ __align__(16) double sm[];
+    double *linv_s = sm;
+    double *rhs = linv_s + PACKED;
+    double *colpart = rhs + 2 * FB;  // [8][FB]
+    int *shared_int = reinterpret_cast<int *>(colpart + (FT / 32) * FB);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0)
+    {
+        shared_int[0] = nblk - 1 - atomicAdd(flags, 1);
+    }
+    __syncthreads();
+    const int i = shared_int[0];
+    const int c0 = i * FB;
+    const int bs = min(FB, n - c0);
+    load_diag_inverse(linv_s, Linv + static_cast<int64_t>(i) * FB * FB);
+    if (tid < FB)
+    {
+        rhs[tid] = (tid < bs) ? x[c0 + tid] : 0.0;
+    }
+    // lanes own columns lane + 32c of block i; warps own rows warp + 8q of each block j
+    constexpr int QB = sizeof(T) == 4 ? 16 : 8;
+    double part[4] = { 0.0, 0.0, 0.0, 0.0 };
+    int seen = 0;
+    for (int j = nblk - 1; j > i; --j)
+    {
+        const int r0 = j * FB;
+        const int rs = min(FB, n - r0);
+        const int need = nblk - j;  // blocks nblk-1 .. j finished
+#pragma unroll
+        for (int qb = 0; qb < 16; qb += QB)
+        {
+            T v[QB][4];
+#pragma unroll
+            for (int q = 0; q < QB; ++q)
+            {
+                const int r = warp + 8 * (qb + q);
+                const T *lr = L + static_cast<int64_t>(r0 + min(r, rs - 1)) * ld + c0 + lane;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                {
+                    v[q][c] = (lane + 32 * c < bs) ? lr[32 * c] : T(0);
+                }
+            }
+            if (qb == 0 && need > seen)
+            {
+                if (tid == 0)
+                {
+                    shared_int[1] = wait_progress(flags + 1, need, st);
+                }
+                __syncthreads();
+                seen = shared_int[1];
+                __syncthreads();
+            }
+#pragma unroll
+            for (int q = 0; q < QB; ++q)
+            {
+                const int r = warp + 8 * (qb + q);
+                const double xv = (r < rs) ? __ldcg(x + r0 + r) : 0.0;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                {
+                    part[c] += to_d(v[q][c]) * xv;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+    {
+        colpart[warp * FB + lane + 32 * c] = part[c];
+    }
+    __syncthreads();
+    if (tid < FB)
+    {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < FT / 32; ++w)
+        {
+            s += colpart[w * FB + tid];
+        }
+        rhs[tid] -= s;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // x_i[c] = sum_{p >= c} Linv[p][c] rhs[p]; two threads per column, 64 rows each
+    {
+        const int c = tid >> 1, h = tid & 1;
+        double s = 0.0;
+        const int pbeg = max(c, 64 * h);
+        const int pend = min(bs - 1, 64 * h + 63);
+        for (int p = pbeg; p <= pend; ++p)
+        {
+            s += linv_s[packed_off(p) + c] * rhs[p];
+        }
+        s += __shfl_xor_sync(0xffffffffu, s, 1);
+        if (h == 0 && c < bs)
+        {
+            x[c0 + c] = s;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0)
+    {
+        atomicMax(flags + 1, nblk - i);
+    }
+}
+
+template <typename T>
+void fwd(const T *L, int64_t ld, const double *Linv, int n, double *x, int *flags, DeviceStatus *st, cudaStream_t s)
+{
+    const int nblk = ceil_div(n, FB);
+    ensure_smem_attr(reinterpret_cast<const void *>(trsv_fwd_fused_kernel<T>), static_cast<int>(SMEM_BYTES));
+    GPRAT_CUDA_CHECK(cudaMemsetAsync(flags, 0, 2 * sizeof(int), s));
+    trsv_fwd_fused_kernel<T><<<nblk, FT, SMEM_BYTES, s>>>(L, ld, Linv, n, x, flags, st);
+    GPRAT_LAUNCH_CHECK();
+}
+
+template <typename T>
+void bwd(const T *L, int64_t ld, const double *Linv, int n, double *x, int *flags, DeviceStatus *st, cudaStream_t s)
+{
+    const int nblk = ceil_div(n, FB);
+    ensure_smem_attr(reinterpret_cast<const void *>(trsv_bwd_fused_kernel<T>), static_cast<int>(SMEM_BYTES));
+    GPRAT_CUDA_CHECK(cudaMemsetAsync(flags, 0, 2 * sizeof(int), s));
+    trsv_bwd_fused_kernel<T><<<nblk, FT, SMEM_BYTES, s>>>(L, ld, Linv, n, nblk, x, flags, st);
+    GPRAT_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void trsv_fused_forward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+                        DeviceStatus *st, cudaStream_t s)
+{
+    fwd(L, ld, Linv, n, x, flags, st, s);
+}
+
+void trsv_fused_backward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+                         DeviceStatus *st, cudaStream_t s)
+{
+    bwd(L, ld, Linv, n, x, flags, st, s);
+}
+
+void trsv_fused_forward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+                            DeviceStatus *st, cudaStream_t s)
+{
+    fwd(L, ld, Linv, n, x, flags, st, s);
+}
+
+void trsv_fused_backward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+                             DeviceStatus *st, cudaStream_t s)
+{
+    bwd(L, ld, Linv, n, x, flags, st, s);
+}
+
+}  // namespace gprat_cu

@@ -189,6 +189,11 @@ int gprat_cu_fit_predict_device(gprat_cu_gp *gp,
  * pivot, timeouts); synchronises the handle's stream. */
 int gprat_cu_check_status(gprat_cu_gp *gp);
 
+/* Number of preconditioned-CG iterations the last mixed-precision alpha
+ * solve of this handle took (0 in FP64 mode).  No counterpart in the
+ * reference. */
+int gprat_cu_gp_pcg_iterations(gprat_cu_gp *gp, int *iterations);
+
 /*
  * Loss without any memory allocation.  No counterpart in the reference.
  * For callers that cannot call cudaMalloc -- code running under an allocator
@@ -255,6 +260,73 @@ int gprat_cu_test_tc_gemm(int kind,
                           float beta,
                           int lower,
                           double *rowsq);
+
+/*
+ * Serving (no counterpart in the reference, whose every predict call
+ * re-assembles and re-factorises K, core/src/cpu/gp_functions.cpp:110-189).
+ * A server owns fitted models resident on one GPU (factor L and alpha stay
+ * in HBM) and answers asynchronous requests:
+ *   submit_predict: m test points of one model (sliding windows of d values
+ *                   over test_in, as in gprat_cu_predict_with_uncertainty);
+ *                   result = mean and variance.
+ *   submit_fit:     a new model from training data and hyper-parameters;
+ *                   result = its model id (ready for predict requests).
+ * Pending predict requests of the same model are batched into one launch
+ * sequence (continuous batching: a batch forms whenever the model's previous
+ * batch has finished); batches of different models and fits run
+ * concurrently on separate streams.  Admission: resident models plus the
+ * working set of in-flight batches stay within memory_budget_bytes
+ * (<= 0: 80 % of the free device memory at creation); a fit that can never
+ * fit fails with GPRAT_CU_ERR_OOM.  Every predict result is bit-identical to
+ * the same request run alone.  precision: GPRAT_CU_PREC_* for every model.
+ * wait() blocks until the request is done, copies mean/var (m doubles each,
+ * NULL to skip), the model id and the request's latency (submit to
+ * completion, ms); each request id can be waited on once.  stats():
+ * latency percentiles of completed predict requests, test points per second
+ * since the first submit, completed requests and launched batches.
+ */
+typedef struct gprat_cu_server gprat_cu_server;
+
+int gprat_cu_server_create(int device, int64_t memory_budget_bytes, int precision, gprat_cu_server **out);
+int gprat_cu_server_destroy(gprat_cu_server *server);
+int gprat_cu_server_add_model(gprat_cu_server *server,
+                              const double *train_in,
+                              int64_t n_in,
+                              const double *train_out,
+                              int64_t n_out,
+                              int n_tiles,
+                              int n_tile_size,
+                              int n_regressors,
+                              const double hyper[3],
+                              int *model_id);
+int gprat_cu_server_submit_predict(gprat_cu_server *server,
+                                   int model_id,
+                                   const double *test_in,
+                                   int64_t n_test_in,
+                                   int m,
+                                   int64_t *request_id);
+int gprat_cu_server_submit_fit(gprat_cu_server *server,
+                               const double *train_in,
+                               int64_t n_in,
+                               const double *train_out,
+                               int64_t n_out,
+                               int n_tiles,
+                               int n_tile_size,
+                               int n_regressors,
+                               const double hyper[3],
+                               int64_t *request_id);
+int gprat_cu_server_wait(gprat_cu_server *server,
+                         int64_t request_id,
+                         double *mean,
+                         double *var,
+                         int *model_id,
+                         double *latency_ms);
+int gprat_cu_server_stats(gprat_cu_server *server,
+                          double *p50_ms,
+                          double *p99_ms,
+                          double *predictions_per_s,
+                          int64_t *completed,
+                          int64_t *batches);
 
 #ifdef __cplusplus
 }
