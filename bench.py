@@ -5,9 +5,13 @@ Workload (default "c2"): n_train=32768, n_test=8192, n_regressors=64,
 lengthscale=4.0, vertical_lengthscale=1.0, noise_variance=0.01, seeded
 synthetic series (x ~ N(0,1), y_i = sum_j sin(X_ij)/8 + N(0, 0.01^2)).
 One step = SE assembly of K + Cholesky + alpha solves + predictive mean
-(cross covariance . alpha) + per-point variance (K* L^-T row sums), all in
-FP64 unless --precision selects a mixed mode.  K alone is 8.6 GB (> L2), so
-no L2 flush is needed between steps.
+(cross covariance . alpha) + per-point variance (K* L^-T row sums).  The
+default precision is mixed-tf32 (TF32 tensor-core trailing updates, FP64
+diagonal blocks and FP64-refined alpha); the same run also times the plain
+FP64 path on the same inputs ("fp64"), reports the mixed results' error
+against it, and runs the serving stream ("serving": four resident models,
+Poisson requests, p50/p99 latency).  K alone is 8.6 GB (> L2), so no L2 flush
+is needed between steps.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -118,6 +122,28 @@ def measured_peaks():
         return {}
 
 
+def measure_gemm_peak(torch, device, dtype) -> float:
+    """cuBLAS GEMM throughput (torch.matmul 8192^3, best of 5), TF/s; fp32
+    inputs run as TF32 (allow_tf32)."""
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    a = torch.randn(8192, 8192, dtype=dtype, device=device)
+    b = torch.randn(8192, 8192, dtype=dtype, device=device)
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (s.elapsed_time(e) / 1e3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    torch.backends.cuda.matmul.allow_tf32 = old
+    return best
+
+
 def measure_fp64_gemm_peak(torch, device) -> float:
     """cuBLAS DGEMM throughput (torch.matmul fp64 8192^3, best of 5), TF/s:
     the FP64 counterpart of the driver's bf16 GEMM peak."""
@@ -176,19 +202,122 @@ def run_reference(args, wl):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_of(wl, "fp64"),
+        "config": config_of(wl),
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference", "sample": desc},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def config_of(wl, precision):
+def config_of(wl):
     return {"workload": f"GP fit+predict_with_uncertainty n_train={wl['n']} n_test={wl['m']} "
                         f"n_regressors={wl['d']}", "n_train": wl["n"], "n_test": wl["m"], "n_regressors": wl["d"],
-            "tile": wl["T"], "hyper": list(wl["hyper"]), "precision": precision,
+            "tile": wl["T"], "hyper": list(wl["hyper"]),
             "l2": "inputs larger than L2 (K alone is %.1f GB)" % (wl["n"] ** 2 * 8 / 1e9),
             "parallelism": "replicas"}
+
+
+PRECISIONS = {"fp64": 0, "mixed-tf32": 1, "mixed-bf16": 2}
+
+# Serving stream (resident models n in SERVE_MODELS, d=8, Poisson arrivals):
+# 90 % predict_with_uncertainty with m log-uniform in [1, 8192] on a uniformly
+# chosen model, 10 % fits with n log-uniform in [1024, 16384] (rounded to 128).
+SERVE_MODELS = (2048, 8192, 16384, 32768)
+SERVE_REQUESTS = 200
+SERVE_RATE = 40.0  # requests per second
+
+
+def time_device_steps(torch, gp, hyper, dxt, m, dmean, dvar, stream, steps, warmup, barrier, local):
+    """Device-timed fit+predict steps (CUDA events on the launching stream)."""
+    from gprat_b200 import capi
+
+    def step():
+        gp.fit_predict_device(hyper, dxt.data_ptr(), dxt.numel(), m, dmean.data_ptr(), dvar.data_ptr(),
+                              stream.cuda_stream)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    gp.check_status()
+    capi.stats_reset()
+    capi.stats_enable_timing(True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(steps):
+            step()
+        end.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    capi.stats_enable_timing(False)
+    stats = capi.stats_read()
+    gp.check_status()
+    return start.elapsed_time(end), stats, clocks.summary()
+
+
+def serving_bench(precision: int, seed: int = 7):
+    """Runs the serving stream against a fresh server; returns latency and
+    throughput figures (device 0 / the current device)."""
+    from gprat_b200 import serving
+    from oracle import gprat_oracle as O  # input generator only (seeded numpy)
+
+    d, hyper, T = 8, (1.0, 1.0, 0.1), 512
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(SERVE_REQUESTS):
+        if rng.random() < 0.1:
+            nf = max(1024, int(np.exp(rng.uniform(np.log(1024), np.log(16384)))) // 128 * 128)
+            xf, yf, _ = O.synthetic(nf, 16, d, seeds=(1000 + i, 2000 + i, 3000 + i))
+            reqs.append(("fit", xf, yf, nf))
+        else:
+            m = int(np.exp(rng.uniform(0.0, np.log(8192))))
+            reqs.append(("predict", int(rng.integers(0, len(SERVE_MODELS))), rng.standard_normal(m + d - 1), m))
+    gaps = rng.exponential(1.0 / SERVE_RATE, SERVE_REQUESTS)
+    with serving.Server(precision=precision) as sv:
+        t0 = time.perf_counter()
+        mids = []
+        for n in SERVE_MODELS:
+            x, y, _ = O.synthetic(n, 16, d, seeds=(n, n + 1, n + 2))
+            mids.append(sv.add_model(x, y, n // T, T, d, hyper))
+        setup_s = time.perf_counter() - t0
+        for mid in mids:  # warm-up: size the batch buffers of every model
+            sv.wait(sv.submit_predict(mid, rng.standard_normal(8192 + d - 1), 8192))
+        ids, kinds, sizes, t_sub = [], [], [], []
+        t_start = time.perf_counter()
+        t_next = t_start
+        for (kind, *rest), gap in zip(reqs, gaps):
+            t_next += gap
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            t_sub.append(time.perf_counter())
+            if kind == "fit":
+                xf, yf, nf = rest
+                ids.append(sv.submit_fit(xf, yf, nf // 128, 128, d, hyper))
+                sizes.append(nf)
+            else:
+                mi, series, m = rest
+                ids.append(sv.submit_predict(mids[mi], series, m))
+                sizes.append(m)
+            kinds.append(kind)
+        lat_p, lat_f, t_done = [], [], []
+        for rid, kind, ts in zip(ids, kinds, t_sub):
+            _, _, _, lat = sv.wait(rid)
+            (lat_f if kind == "fit" else lat_p).append(lat)
+            t_done.append(ts + lat / 1e3)
+        wall = max(t_done) - t_start
+        st = sv.stats()
+    points = sum(sz for sz, k in zip(sizes, kinds) if k == "predict")
+    return {
+        "requests": SERVE_REQUESTS, "rate_per_s": SERVE_RATE,
+        "predict_p50_ms": float(np.percentile(lat_p, 50)), "predict_p99_ms": float(np.percentile(lat_p, 99)),
+        "fit_p50_ms": float(np.percentile(lat_f, 50)) if lat_f else None,
+        "fit_p99_ms": float(np.percentile(lat_f, 99)) if lat_f else None,
+        "predictions_per_s": points / wall, "predict_requests": len(lat_p), "fit_requests": len(lat_f),
+        "batches": st.batches, "model_setup_s": setup_s,
+    }
 
 
 def run_ours(args, wl):
@@ -206,47 +335,22 @@ def run_ours(args, wl):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
     n, m, d, T, hyper = wl["n"], wl["m"], wl["d"], wl["T"], wl["hyper"]
     x, y, xt = synthetic(n, m, d)
     gp = capi.CudaGP(x, y, n // T, T, d, device=local)
-    precision = {"fp64": capi.PREC_FP64, "mixed-tf32": capi.PREC_MIXED_TF32,
-                 "mixed-bf16": capi.PREC_MIXED_BF16}[args.precision]
-    gp.set_precision(precision)
+    gp.set_precision(PRECISIONS[args.precision])
 
     dxt = torch.tensor(xt, device=device)
     dmean = torch.empty(m, dtype=torch.float64, device=device)
     dvar = torch.empty(m, dtype=torch.float64, device=device)
     stream = torch.cuda.current_stream(device)
 
-    def step():
-        gp.fit_predict_device(hyper, dxt.data_ptr(), dxt.numel(), m, dmean.data_ptr(), dvar.data_ptr(),
-                              stream.cuda_stream)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    gp.check_status()
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    capi.stats_reset()
-    capi.stats_enable_timing(True)
-    with ClockSampler(local) as clocks:
-        barrier()
-        torch.cuda.synchronize()
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        start.record(stream)
-        for _ in range(args.steps):
-            step()
-        end.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-    capi.stats_enable_timing(False)
-    stats = capi.stats_read()
-    gp.check_status()
-    elapsed_ms = start.elapsed_time(end)
+    elapsed_ms, stats, clk = time_device_steps(torch, gp, hyper, dxt, m, dmean, dvar, stream, args.steps,
+                                               args.warmup, barrier, local)
     t = torch.tensor([elapsed_ms], dtype=torch.float64, device=device)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -269,6 +373,36 @@ def run_ours(args, wl):
         gp.predict_with_uncertainty(hyper, xt_pinned, 1, m)
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = float(np.mean(e2e_times))
+    loss = gp.compute_loss(hyper)
+    pcg_iters = gp.pcg_iterations()
+
+    # the plain FP64 path on the same inputs (timed the same way), and the
+    # mixed results' error against it
+    fp64 = None
+    if args.precision != "fp64" and not args.skip_fp64:
+        gp.set_precision(capi.PREC_FP64)
+        m64 = torch.empty_like(dmean)
+        v64 = torch.empty_like(dvar)
+        el64, st64, clk64 = time_device_steps(torch, gp, hyper, dxt, m, m64, v64, stream, args.steps, args.warmup,
+                                              barrier, local)
+        t64 = torch.tensor([el64], dtype=torch.float64, device=device)
+        if world > 1:
+            dist.all_reduce(t64, op=dist.ReduceOp.MAX)
+        ms64 = float(t64.item()) / args.steps
+        mean64, var64 = m64.cpu().numpy(), v64.cpu().numpy()
+        loss64 = gp.compute_loss(hyper)
+        fp64 = {
+            "value": ms64 / 1e3 / world, "ms_per_step": ms64,
+            "gemm_tflops": st64["gemm_flops"] / (st64["gemm_ms"] / 1e3) / 1e12 if st64["gemm_ms"] > 0 else None,
+            "clocks": clk64,
+            "speedup_of_mixed": ms64 / ms_per_step,
+            "mixed_error_vs_fp64": {
+                "mean_max_rel": float(np.max(np.abs(mean_h - mean64)) / np.max(np.abs(mean64))),
+                "var_max_rel": float(np.max(np.abs(var_h - var64) / var64)),
+                "loss_rel": float(abs(loss - loss64) / abs(loss64)),
+            },
+        }
+        gp.set_precision(PRECISIONS[args.precision])
 
     if rank != 0:
         if world > 1:
@@ -277,7 +411,21 @@ def run_ours(args, wl):
         return
 
     peaks = measured_peaks()
-    fp64_peak = measure_fp64_gemm_peak(torch, device)
+    if args.precision == "fp64":
+        peak = measure_fp64_gemm_peak(torch, device)
+        kernel = "dgemm_kernel (FP64 DMMA m16n8k8: Cholesky panel/trailing updates + variance solve)"
+        peak_source = ("cuBLAS DGEMM (torch.matmul fp64 8192^3, best of 5) measured in this run; "
+                       "MEASURED_PEAKS.json holds no FP64 figure")
+    elif args.precision == "mixed-tf32":
+        peak = measure_gemm_peak(torch, device, torch.float32)
+        kernel = ("tc_gemm_kernel<TF32> (tcgen05.mma kind::tf32, TMA-staged, TMEM accumulators: panel solves, "
+                  "trailing updates, variance solve)")
+        peak_source = ("cuBLAS TF32 GEMM (torch.matmul fp32 8192^3 with allow_tf32, best of 5) measured in this "
+                       "run; MEASURED_PEAKS.json holds only the bf16 figure")
+    else:
+        peak = peaks.get("bf16_tflops") or measure_gemm_peak(torch, device, torch.bfloat16)
+        kernel = "tc_gemm_kernel<BF16> (tcgen05.mma kind::f16 with bf16 operands)"
+        peak_source = "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks.get("bf16_tflops") else "cuBLAS bf16 in-run"
     gemm_tflops = stats["gemm_flops"] / (stats["gemm_ms"] / 1e3) / 1e12 if stats["gemm_ms"] > 0 else None
     step_flops = algorithmic_flops(n, m)
     if world == 1 and not args.skip_cpu_baseline:
@@ -285,7 +433,11 @@ def run_ours(args, wl):
         cpu = {"value": sample_s * scale, "unit": "s", "cores": threads, "kind": "reference", "sample": desc}
     else:
         cpu = None
-    clk = clocks.summary()
+    serve = None
+    if world == 1 and not args.skip_serving:
+        serve = {args.precision: serving_bench(PRECISIONS[args.precision])}
+        if args.precision != "fp64" and not args.skip_fp64:
+            serve["fp64"] = serving_bench(capi.PREC_FP64)
     line = {
         "metric": METRIC,
         "value": ms_per_step / 1e3 / world,
@@ -299,17 +451,16 @@ def run_ours(args, wl):
         "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else args.precision,
         "data": "synthetic",
-        "config": config_of(wl, args.precision),
+        "config": config_of(wl),
         "pipeline_tflops": step_flops / (ms_per_step / 1e3) / 1e12,
         "roofline": {
-            "kernel": "dgemm_kernel (FP64 DMMA m16n8k8: Cholesky panel/trailing updates + variance solve)",
+            "kernel": kernel,
             "bound": "tensor",
             "achieved": gemm_tflops,
-            "peak": fp64_peak,
-            "peak_source": "cuBLAS DGEMM (torch.matmul fp64 8192^3, best of 5) measured in this run; "
-                           "MEASURED_PEAKS.json holds no FP64 figure",
+            "peak": peak,
+            "peak_source": peak_source,
             "unit": "TFLOP/s",
-            "frac": (gemm_tflops / fp64_peak) if gemm_tflops else None,
+            "frac": (gemm_tflops / peak) if gemm_tflops else None,
             "traffic": None,
             "gemm_share_of_step": (stats["gemm_ms"] / args.steps) / ms_per_step,
             "gemm_launches_per_step": stats["gemm_launches"] / args.steps,
@@ -319,8 +470,10 @@ def run_ours(args, wl):
                 "d2h_bytes_per_step": int(2 * m * 8)},
         "gpu_launches": int(stats["launches"]),
         "clocks": clk,
+        "fp64": fp64,
+        "serving": serve,
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
-        "pcg_iterations": gp.pcg_iterations(),
+        "pcg_iterations": pcg_iters,
         "sanity": sane,
     }
     print(json.dumps(line), flush=True)
@@ -332,13 +485,15 @@ def run_ours(args, wl):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
-    ap.add_argument("--precision", choices=["fp64", "mixed-tf32", "mixed-bf16"], default="fp64")
+    ap.add_argument("--precision", choices=sorted(PRECISIONS), default="mixed-tf32")
     ap.add_argument("--skip-cpu-baseline", action="store_true",
                     help="omit the CPU reference sample (cpu_baseline becomes null)")
+    ap.add_argument("--skip-fp64", action="store_true", help="omit the FP64 comparison arm")
+    ap.add_argument("--skip-serving", action="store_true", help="omit the serving stream")
     ap.add_argument("--profile", action="store_true",
                     help="device steps only (no CPU sample, e2e loop or peak measurement): for ncu captures")
     args = ap.parse_args()

@@ -2,22 +2,26 @@
 //
 // Replaces the per-tile potrf task (LAPACKE_dpotrf2 'L',
 // core/src/cpu/adapter_cblas_fp64.cpp:14-22; cusolverDnXpotrf,
-// core/src/gpu/adapter_cublas.cu:9-79).  One CTA of 8 warps loads the lower
-// triangle of a bs x bs (bs <= 128) diagonal block into shared memory and
-// factors it in 32-wide sub-blocks:
+// core/src/gpu/adapter_cublas.cu:9-79).  One CTA of 8 warps factors a
+// bs x bs (bs <= 128) diagonal block; a block smaller than 128 is padded with
+// the identity, so every loop below has a fixed trip count.  Right-looking in
+// 32-wide sub-blocks s = 0..3:
 //   1. warp 0 factors the 32 x 32 diagonal sub-block in registers (lane i
-//      holds row i; column values are exchanged with shuffles) and inverts
-//      it the same way (lane c holds column c of the inverse);
-//   2. the rows below are solved against it with the inverse (all warps);
-//   3. the trailing lower triangle is updated (all warps).
-// L is written back (the strict upper triangle in global memory is never
-// touched, matching dpotrf2('L')).  The full inverse Linv (zero above the
-// diagonal) is then assembled block row by block row,
-//   Linv_ss = X_s,  Linv_st = -X_s * sum_p L_s,p Linv_p,t,
+//      holds row i; the pivot travels by shuffle, the new column of L through
+//      shared memory; branch-free) and forms its inverse X_s column by column
+//      (lane c solves L x = e_c in axpy order, so the 31 updates of a step are
+//      independent);
+//   2. panel solve P = A_rs X_s^T and trailing update A_rr -= P P^T on the
+//      FP64 tensor cores (mma.sync m16n8k8 f64; upper-triangular zero blocks
+//      of X_s are skipped);
+// then the full inverse is assembled block row by block row on the tensor
+// cores,  Linv_s,<s = -X_s (L_s,<s Linv_<s,<s),  Linv_ss = X_s,
 // which turns every later triangular solve against this block (panel trsm,
-// trsv, variance solve) into a tensor-core GEMM.  A non-positive or NaN
-// pivot is recorded in the status word (first failing global row, 1-based);
-// the reference silently returns NaNs instead.
+// trsv, variance solve) into a GEMM.  L is written back to the lower
+// triangle only (the strict upper triangle in global memory is never
+// touched, matching dpotrf2('L')).  A non-positive or NaN pivot is recorded
+// in the status word (first failing global row, 1-based); the reference
+// silently returns NaNs instead.
 #include "common.cuh"
 
 namespace gprat_cu
@@ -25,190 +29,252 @@ namespace gprat_cu
 namespace
 {
 
-constexpr int PB = 128;     // max block size
-constexpr int PS = PB + 1;  // smem row stride of the block
-constexpr int SB = 32;      // sub-block width
-constexpr int XS = SB + 1;  // smem row stride of a sub-block inverse
-constexpr int TS = 96 + 1;  // smem row stride of the inverse temporary
-constexpr int XBLK = (SB + 1) * XS;  // one sub-block inverse plus its 1/L_ii row
+constexpr int PB = 128;                   // block size (padded)
+constexpr int PS = PB + 4;                // smem row stride of the block (conflict-free fragment loads)
+constexpr int SB = 32;                    // sub-block width
+constexpr int XS = SB + 4;                // smem row stride of a sub-block inverse
+constexpr int TS = 3 * SB + 4;            // smem row stride of the assembly temporary
 constexpr int PTHREADS = 256;
+constexpr int NWARPS = PTHREADS / 32;
+constexpr size_t SMEM_DOUBLES = PB * PS + 4 * SB * XS + PB + SB * TS + SB;
 
-// Warp 0: factor a[c0.., c0..] (w x w, w <= 32) in registers, write L back
-// to smem, and store X = L^-1 (32 x 32, zero above the diagonal) in xinv.
-__device__ __forceinline__ void warp_factor_invert(double *a, int c0, int w, int row0, int *bad, double *xinv)
+__device__ __forceinline__ void dmma(double (&c)[4], const double (&a)[4], const double (&b)[2])
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// Fragment loads from row-major shared matrices (g = lane / 4, t = lane % 4).
+// A: rows m0.., k-columns k0..
+__device__ __forceinline__ void frag_a(double (&a)[4], const double *M, int ld, int m0, int k0, int g, int t)
+{
+    a[0] = M[(m0 + g) * ld + k0 + t];
+    a[1] = M[(m0 + g + 8) * ld + k0 + t];
+    a[2] = M[(m0 + g) * ld + k0 + t + 4];
+    a[3] = M[(m0 + g + 8) * ld + k0 + t + 4];
+}
+// B = M^T with M row-major (N x K): B[k][n] = M[n][k]
+__device__ __forceinline__ void frag_bt(double (&b)[2], const double *M, int ld, int n0, int k0, int g, int t)
+{
+    b[0] = M[(n0 + g) * ld + k0 + t];
+    b[1] = M[(n0 + g) * ld + k0 + t + 4];
+}
+// B row-major (K x N)
+__device__ __forceinline__ void frag_b(double (&b)[2], const double *M, int ld, int n0, int k0, int g, int t)
+{
+    b[0] = M[(k0 + t) * ld + n0 + g];
+    b[1] = M[(k0 + t + 4) * ld + n0 + g];
+}
+
+// Warp 0: factor the 32 x 32 sub-block at (c0, c0), write L back to smem,
+// and store X = L^-1 (zero above the diagonal) in xinv and the pivot
+// reciprocals 1/L_jj in dinv[0..31].
+//
+// Both loops are rolled and branch-free.  Each lane keeps a window of its row
+// in registers that shifts left by one column per step, so the current column
+// is always r[0] and every register index is a compile-time constant.  The
+// updates are unconditional: a lane's entries above the diagonal (and window
+// slots past column 31) receive values that are never read, which keeps the
+// warp converged (per-lane conditional updates compile to divergent branches
+// that cost more than the arithmetic).  colbuf (32 doubles) broadcasts the
+// new column of L.
+__device__ __forceinline__ void diag_factor_invert(double *a, int c0, int bs, int row0, int *bad, double *xinv,
+                                                   double *dinv, double *colbuf)
 {
     const int lane = threadIdx.x & 31;
-    double r[SB];
-#pragma unroll
-    for (int c = 0; c < SB; ++c)
+    double r[SB];  // r[c] = A[lane][j + c] during step j
     {
-        double v;
-        if (lane < w && c < w)
-        {
-            v = (c <= lane) ? a[(c0 + lane) * PS + c0 + c] : 0.0;
-        }
-        else
-        {
-            v = (c == lane) ? 1.0 : 0.0;  // identity padding beyond w
-        }
-        r[c] = v;
-    }
-    double my_inv = 1.0;
-#pragma unroll
-    for (int j = 0; j < SB; ++j)
-    {
-        const double ajj = __shfl_sync(0xffffffffu, r[j], j);
-        if (lane == 0 && j < w && !(ajj > 0.0) && *bad == 0)
-        {
-            *bad = row0 + c0 + j + 1;
-        }
-        // one reciprocal square root per pivot keeps the serial chain short
-        const double inv = rsqrt(ajj);
-        const double d = ajj * inv;
-        if (lane == j)
-        {
-            r[j] = d;
-            my_inv = inv;
-        }
-        else if (lane > j)
-        {
-            r[j] *= inv;
-        }
-#pragma unroll
-        for (int c = j + 1; c < SB; ++c)
-        {
-            const double lcj = __shfl_sync(0xffffffffu, r[j], c);
-            if (lane >= c)
-            {
-                r[c] -= r[j] * lcj;
-            }
-        }
-    }
-    if (lane < w)
-    {
+        const double *arow = a + (c0 + lane) * PS + c0;
 #pragma unroll
         for (int c = 0; c < SB; ++c)
         {
-            if (c <= lane)
-            {
-                a[(c0 + lane) * PS + c0 + c] = r[c];
-            }
+            r[c] = (c <= lane) ? arow[c] : 0.0;
         }
     }
-    // stage 1/L_ii for the inverse, then drop r (registers) and read L from smem
-    xinv[SB * XS + lane] = my_inv;
+    int first_bad = 0;
+#pragma unroll 1
+    for (int j = 0; j < SB; ++j)
+    {
+        const double ajj = __shfl_sync(0xffffffffu, r[0], j);
+        first_bad = (first_bad == 0 && !(ajj > 0.0) && c0 + j < bs) ? row0 + c0 + j + 1 : first_bad;
+        const double inv = rsqrt(ajj);
+        const double l = (lane == j) ? ajj * inv : r[0] * inv;  // L[lane][j] for lane >= j
+        colbuf[lane] = l;
+        a[(c0 + lane) * PS + c0 + j] = l;  // above the diagonal: a value nobody reads
+        if (lane == 0)
+        {
+            dinv[j] = inv;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int c = 1; c < SB; ++c)
+        {
+            r[c] -= l * colbuf[(j + c) & (SB - 1)];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < SB - 1; ++c)
+        {
+            r[c] = r[c + 1];
+        }
+        r[SB - 1] = 0.0;
+    }
+    if (lane == 0 && first_bad != 0 && *bad == 0)
+    {
+        *bad = first_bad;
+    }
     __syncwarp();
-    // inverse: lane c solves L x = e_c (column c of X); L rows are smem broadcasts
+    // X column `lane`: x = e_lane; step k: x_k *= 1/L_kk, x_i -= L_ik x_k (i > k).
+    // x[c] holds x_{k + c} during step k.
     double x[SB];
 #pragma unroll
-    for (int i = 0; i < SB; ++i)
+    for (int c = 0; c < SB; ++c)
     {
-        double s = (i == lane) ? 1.0 : 0.0;
-        const double *li = a + (c0 + i) * PS + c0;
-#pragma unroll
-        for (int k = 0; k < i; ++k)
-        {
-            s -= ((i < w) ? li[k] : 0.0) * x[k];
-        }
-        x[i] = s * xinv[SB * XS + i];
+        x[c] = (c == lane) ? 1.0 : 0.0;
     }
-#pragma unroll
-    for (int i = 0; i < SB; ++i)
+#pragma unroll 1
+    for (int k = 0; k < SB; ++k)
     {
-        xinv[i * XS + lane] = x[i];
+        const double xk = x[0] * dinv[k];
+        xinv[k * XS + lane] = xk;
+        const double *col = a + c0 * PS + c0 + k;  // column k of L: L[i][k] at col[i * PS]
+#pragma unroll
+        for (int c = 1; c < SB; ++c)
+        {
+            x[c] -= col[min(k + c, SB - 1) * PS] * xk;  // rows past 31: unused window slots
+        }
+#pragma unroll
+        for (int c = 0; c < SB - 1; ++c)
+        {
+            x[c] = x[c + 1];
+        }
+        x[SB - 1] = 0.0;
     }
 }
 
-__global__ void __launch_bounds__(PTHREADS) potrf_inv_kernel(double *__restrict__ A, int64_t lda, int bs, int row0,
-                                                             double *__restrict__ Linv, int64_t ldi,
-                                                             DeviceStatus *__restrict__ status)
+__global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(double *__restrict__ A, int64_t lda, int bs, int row0,
+                                                                double *__restrict__ Linv, int64_t ldi,
+                                                                DeviceStatus *__restrict__ status)
 {
-    extern __shared__ double sa[];     // [PB][PS]
-    double *xall = sa + PB * PS;       // 4 x [SB+1][XS]: sub-block inverses + 1/L_ii row
-    double *tmp = xall + 4 * XBLK;     // [SB][TS]
+    extern __shared__ double sa[];  // [PB][PS]
+    double *xall = sa + PB * PS;    // 4 x [SB][XS] sub-block inverses
+    double *dinv = xall + 4 * SB * XS;       // [PB] pivot reciprocals
+    double *tbuf = dinv + PB;                // [SB][TS]
+    double *colbuf = tbuf + SB * TS;         // [SB] column broadcast of the diagonal factorisation
     __shared__ int bad;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
     if (tid == 0)
     {
         bad = 0;
     }
-#pragma unroll 8
-    for (int q = tid; q < bs * bs; q += PTHREADS)
+    // load the lower triangle; pad with the identity beyond bs
+#pragma unroll 16
+    for (int q = 0; q < PB * PB / PTHREADS; ++q)
     {
-        int i = q / bs, c = q % bs;
-        sa[i * PS + c] = (c <= i) ? A[static_cast<int64_t>(i) * lda + c] : 0.0;
+        const int idx = q * PTHREADS + tid;
+        const int i = idx >> 7, c = idx & (PB - 1);
+        double v = (i == c) ? 1.0 : 0.0;
+        if (i < bs && c <= i)
+        {
+            v = A[static_cast<int64_t>(i) * lda + c];
+        }
+        sa[i * PS + c] = v;
     }
     __syncthreads();
 
-    const int nsub = (bs + SB - 1) / SB;
-    for (int s = 0; s < nsub; ++s)
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s)
     {
         const int c0 = s * SB;
-        const int w = min(SB, bs - c0);
-        double *xs = xall + s * XBLK;
+        double *xs = xall + s * SB * XS;
         if (warp == 0)
         {
-            warp_factor_invert(sa, c0, w, row0, &bad, xs);
+            diag_factor_invert(sa, c0, bs, row0, &bad, xs, dinv + c0, colbuf);
         }
         __syncthreads();
-        const int r0 = c0 + w;
-        const int R = bs - r0;
-        if (R <= 0)
+        if (s == 3)
         {
             break;
         }
-        // panel solve: P = P X^T (4 threads per row, 8 output columns each;
-        // rows in passes of PTHREADS/4, each pass reads before it writes)
-        for (int pass = 0; pass * (PTHREADS / 4) < R; ++pass)
+        const int r0 = c0 + SB;
+        const int R = PB - r0;  // 96, 64, 32 rows below
+        // panel: P = A[r0.., c0..c0+31] X^T  (warp w owns rows r0 + 16w .. +15)
+        if (warp < R / 16)
         {
-            const int row = pass * (PTHREADS / 4) + (tid >> 2), grp = tid & 3;
-            double v[SB];
-            if (row < R)
+            const int m0 = r0 + 16 * warp;
+            double af[4][4];
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+            {
+                frag_a(af[kk], sa, PS, m0, c0 + 8 * kk, g, t);
+            }
+            double cf[4][4];
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt)
             {
 #pragma unroll
-                for (int k = 0; k < SB; ++k)
+                for (int e = 0; e < 4; ++e)
                 {
-                    v[k] = (k < w) ? sa[(r0 + row) * PS + c0 + k] : 0.0;
+                    cf[nt][e] = 0.0;
+                }
+#pragma unroll
+                for (int kk = 0; kk <= nt; ++kk)  // X^T is zero where k > n
+                {
+                    double bf[2];
+                    frag_bt(bf, xs, XS, 8 * nt, 8 * kk, g, t);
+                    dmma(cf[nt], af[kk], bf);
                 }
             }
-            __syncthreads();
-            if (row < R)
+            __syncwarp();
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt)
             {
-#pragma unroll
-                for (int cc = 0; cc < 8; ++cc)
-                {
-                    const int c = grp * 8 + cc;
-                    if (c < w)
-                    {
-                        double acc = 0.0;
-#pragma unroll
-                        for (int k = 0; k < SB; ++k)
-                        {
-                            if (k <= c)
-                            {
-                                acc += v[k] * xs[c * XS + k];
-                            }
-                        }
-                        sa[(r0 + row) * PS + c0 + c] = acc;
-                    }
-                }
+                double *c = sa + (m0 + g) * PS + c0 + 8 * nt + 2 * t;
+                c[0] = cf[nt][0];
+                c[1] = cf[nt][1];
+                c[8 * PS] = cf[nt][2];
+                c[8 * PS + 1] = cf[nt][3];
             }
         }
         __syncthreads();
-        // trailing update of the lower triangle rows/cols [r0, bs)
-        for (int i = r0 + warp; i < bs; i += PTHREADS / 32)
+        // trailing update of the lower tiles: A[r0.., r0..] -= P P^T
         {
-            const double *pi = sa + i * PS + c0;
-            for (int c = r0 + lane; c <= i; c += 32)
+            const int mt = R / 16;
+            const int ntiles = mt * (mt + 1);  // sum over mi of (2 mi + 2)
+            for (int tile = warp; tile < ntiles; tile += NWARPS)
             {
-                const double *pc = sa + c * PS + c0;
-                double acc = 0.0;
-                for (int k = 0; k < w; ++k)
+                // tile -> (mi, ni) with ni <= 2 mi + 1
+                int mi = 0, base = 0;
+                while (base + 2 * mi + 2 <= tile)
                 {
-                    acc += pi[k] * pc[k];
+                    base += 2 * mi + 2;
+                    ++mi;
                 }
-                sa[i * PS + c] -= acc;
+                const int ni = tile - base;
+                const int m0 = r0 + 16 * mi, n0 = r0 + 8 * ni;
+                double *c = sa + (m0 + g) * PS + n0 + 2 * t;
+                double cf[4] = { c[0], c[1], c[8 * PS], c[8 * PS + 1] };
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk)
+                {
+                    double af[4], bf[2];
+                    frag_a(af, sa, PS, m0, c0 + 8 * kk, g, t);
+                    frag_bt(bf, sa, PS, n0, c0 + 8 * kk, g, t);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                    {
+                        af[e] = -af[e];
+                    }
+                    dmma(cf, af, bf);
+                }
+                c[0] = cf[0];
+                c[1] = cf[1];
+                c[8 * PS] = cf[2];
+                c[8 * PS + 1] = cf[3];
             }
         }
         __syncthreads();
@@ -218,11 +284,12 @@ __global__ void __launch_bounds__(PTHREADS) potrf_inv_kernel(double *__restrict_
         atomicCAS(&status->not_spd_row, 0, bad);
     }
     // write L (lower triangle incl. diagonal) back
-#pragma unroll 8
-    for (int q = tid; q < bs * bs; q += PTHREADS)
+#pragma unroll 16
+    for (int q = 0; q < PB * PB / PTHREADS; ++q)
     {
-        int i = q / bs, c = q % bs;
-        if (c <= i)
+        const int idx = q * PTHREADS + tid;
+        const int i = idx >> 7, c = idx & (PB - 1);
+        if (i < bs && c <= i)
         {
             A[static_cast<int64_t>(i) * lda + c] = sa[i * PS + c];
         }
@@ -230,51 +297,78 @@ __global__ void __launch_bounds__(PTHREADS) potrf_inv_kernel(double *__restrict_
     __syncthreads();
 
     // --- full inverse, block row by block row (rows < c0 already hold Linv) --
-    for (int s = 0; s < nsub; ++s)
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s)
     {
         const int c0 = s * SB;
-        const int w = min(SB, bs - c0);
-        const double *xs = xall + s * XBLK;
+        const double *xs = xall + s * SB * XS;
         if (s > 0)
         {
-            // tmp[i][j] = sum_{p=j}^{c0-1} L[c0+i][p] * Linv[p][j],  j < c0
-            for (int q = tid; q < w * c0; q += PTHREADS)
+            // T = L[c0.., 0..c0) Linv[0..c0, 0..c0)   (32 x c0; Linv lower: k >= n)
+            const int nt_count = c0 / 8;
+            for (int tile = warp; tile < 2 * nt_count; tile += NWARPS)
             {
-                const int i = q / c0, j = q % c0;
-                const double *li = sa + (c0 + i) * PS;
-                double acc = 0.0;
-                for (int p = j; p < c0; ++p)
+                const int mi = tile / nt_count, nt = tile % nt_count;
+                double cf[4] = { 0.0, 0.0, 0.0, 0.0 };
+                for (int kk = nt; kk < nt_count; ++kk)
                 {
-                    acc += li[p] * sa[p * PS + j];
+                    double af[4], bf[2];
+                    frag_a(af, sa, PS, c0 + 16 * mi, 8 * kk, g, t);
+                    frag_b(bf, sa, PS, 8 * nt, 8 * kk, g, t);
+                    dmma(cf, af, bf);
                 }
-                tmp[i * TS + j] = acc;
+                double *c = tbuf + (16 * mi + g) * TS + 8 * nt + 2 * t;
+                c[0] = cf[0];
+                c[1] = cf[1];
+                c[8 * TS] = cf[2];
+                c[8 * TS + 1] = cf[3];
             }
             __syncthreads();
-            // Linv[c0+i][j] = -sum_k X[i][k] tmp[k][j]
-            for (int q = tid; q < w * c0; q += PTHREADS)
+            // Linv[c0.., 0..c0) = -X T   (X lower: k <= row)
+            for (int tile = warp; tile < 2 * nt_count; tile += NWARPS)
             {
-                const int i = q / c0, j = q % c0;
-                double acc = 0.0;
-                for (int k = 0; k <= i; ++k)
+                const int mi = tile / nt_count, nt = tile % nt_count;
+                double cf[4] = { 0.0, 0.0, 0.0, 0.0 };
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk)
                 {
-                    acc += xs[i * XS + k] * tmp[k * TS + j];
+                    if (kk <= 2 * mi + 1)
+                    {
+                        double af[4], bf[2];
+                        frag_a(af, xs, XS, 16 * mi, 8 * kk, g, t);
+                        frag_b(bf, tbuf, TS, 8 * nt, 8 * kk, g, t);
+#pragma unroll
+                        for (int e = 0; e < 4; ++e)
+                        {
+                            af[e] = -af[e];
+                        }
+                        dmma(cf, af, bf);
+                    }
                 }
-                sa[(c0 + i) * PS + j] = -acc;
+                double *c = sa + (c0 + 16 * mi + g) * PS + 8 * nt + 2 * t;
+                c[0] = cf[0];
+                c[1] = cf[1];
+                c[8 * PS] = cf[2];
+                c[8 * PS + 1] = cf[3];
             }
         }
-        // diagonal block: X_s
-        for (int q = tid; q < w * w; q += PTHREADS)
+        // diagonal block: X_s (zero above the diagonal)
+        for (int q = tid; q < SB * SB; q += PTHREADS)
         {
-            const int i = q / w, j = q % w;
+            const int i = q / SB, j = q % SB;
             sa[(c0 + i) * PS + c0 + j] = (j <= i) ? xs[i * XS + j] : 0.0;
         }
         __syncthreads();
     }
-#pragma unroll 8
-    for (int q = tid; q < bs * bs; q += PTHREADS)
+#pragma unroll 16
+    for (int q = 0; q < PB * PB / PTHREADS; ++q)
     {
-        int i = q / bs, c = q % bs;
-        Linv[static_cast<int64_t>(i) * ldi + c] = (c <= i) ? sa[i * PS + c] : 0.0;
+        const int idx = q * PTHREADS + tid;
+        const int i = idx >> 7, c = idx & (PB - 1);
+        if (i < bs && c < bs)
+        {
+            Linv[static_cast<int64_t>(i) * ldi + c] = (c <= i) ? sa[i * PS + c] : 0.0;
+        }
     }
 }
 
@@ -287,7 +381,7 @@ void potrf_diag(double *A, int64_t lda, int bs, int row0, double *Linv, int64_t 
     {
         throw Error(1, "potrf_diag: block size must be in [1, 128]");
     }
-    constexpr size_t smem = static_cast<size_t>(PB * PS + 4 * XBLK + SB * TS) * sizeof(double);
+    constexpr size_t smem = SMEM_DOUBLES * sizeof(double);
     ensure_smem_attr(reinterpret_cast<const void *>(potrf_inv_kernel), static_cast<int>(smem));
     potrf_inv_kernel<<<1, PTHREADS, smem, s>>>(A, lda, bs, row0, Linv, ldi, status);
     GPRAT_LAUNCH_CHECK();

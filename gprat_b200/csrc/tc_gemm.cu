@@ -12,10 +12,13 @@
 //                      smem stage; two accumulators (256 TMEM columns) so the
 //                      epilogue of tile i overlaps the MMAs of tile i+1;
 //   warps 2..9       : epilogue -- two warps per TMEM lane quarter, 64 columns
-//                      each: tcgen05.ld of the accumulator, release it, then
-//                      C = beta*C + alpha*acc with every C load of the row
-//                      segment issued before the first store (lower-triangle
-//                      mask, optional FP64 row sums of squares).
+//                      each: tcgen05.ld of the accumulator, release it, scale
+//                      (and mask above the diagonal), stage each 32 x 32
+//                      sub-tile in shared memory in the TMA box layout, then
+//                      one TMA bulk tensor store (beta = 0) or reduce-add
+//                      (beta = 1) per sub-tile: C is never read by the SM, and
+//                      its rows are written as whole 128-byte lines
+//                      (optional FP64 row sums of squares, beta = 0 only).
 // Every mbarrier wait is bounded (about 2 s of device time); a wait that gives
 // up raises a CTA-wide abort flag, the roles leave their loops, in-flight
 // TMA copies are given time to land, the MMA issuer drains its own MMAs, the
@@ -36,12 +39,14 @@ constexpr int TM = 128;
 constexpr int TN = 128;
 constexpr int TILE_BYTES = 128 * 128;  // one 128-row x 128-byte operand tile
 constexpr int STAGE_BYTES = 2 * TILE_BYTES;
-constexpr int STAGES = 7;
+constexpr int STAGES = 6;
 constexpr int NUM_THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
 constexpr int EPI_COLS = 64;     // columns per epilogue warp
+constexpr int EPI_WARPS = 8;
+constexpr int EPI_BUF_BYTES = 32 * 128;  // one 32 x 32 FP32 sub-tile (TMA box, 128-byte swizzle)
 constexpr int TMEM_COLS = 2 * TN;
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // bounded waits: 2 s
-constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256;
+constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + EPI_WARPS * EPI_BUF_BYTES + 256;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -115,6 +120,27 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, u
         "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
         : "memory");
 }
+
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, const void *src, int x, int y)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(smem_u32(src)), "r"(x), "r"(y)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap *map, const void *src, int x, int y)
+{
+    asm volatile("cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(smem_u32(src)), "r"(x), "r"(y)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
@@ -213,13 +239,14 @@ __device__ __forceinline__ void tile_of(int t, bool lower, int tiles_n, int &m0,
 
 template <int KIND>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
-    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcGemmArgs p,
-                   int tiles_n, int ntiles)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   const __grid_constant__ CUtensorMap tmC, TcGemmArgs p, int tiles_n, int ntiles)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t *tiles = smem;
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint8_t *epi_smem = smem + STAGES * STAGE_BYTES;  // 1024-byte aligned sub-tile buffers
+    uint64_t *full = reinterpret_cast<uint64_t *>(epi_smem + EPI_WARPS * EPI_BUF_BYTES);
     uint64_t *empty = full + STAGES;
     uint64_t *tfull = empty + STAGES;
     uint64_t *tempty = tfull + 2;
@@ -309,13 +336,13 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             // ---------------- MMA issuer ----------------
             int s = 0;
             uint32_t ph = 0;
-            uint32_t acc_ph[2] = { 0u, 0u };
+            uint32_t acc_bits = 0u;
             bool ok = true;
             int it = 0;
             for (int t = blockIdx.x; ok && t < ntiles; t += gridDim.x, ++it)
             {
                 const int b = it & 1;
-                if (!mbar_wait(&tempty[b], acc_ph[b] ^ 1u, abort_flag))
+                if (!mbar_wait(&tempty[b], ((acc_bits >> b) & 1u) ^ 1u, abort_flag))
                 {
                     break;
                 }
@@ -350,7 +377,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     break;
                 }
                 mma_commit(&tfull[b]);
-                acc_ph[b] ^= 1u;
+                acc_bits ^= 1u << b;
             }
             // drain: arrives once every MMA issued above has completed
             mma_commit(drain);
@@ -365,14 +392,16 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         const int q = warp & 3;  // TMEM lane quarter this warp may access
         const int h = ew >> 2;   // column half
         const int r_in = q * 32 + lane;
-        uint32_t acc_ph[2] = { 0u, 0u };
+        uint8_t *buf = epi_smem + ew * EPI_BUF_BYTES;
+        const uint32_t buf_row = smem_u32(buf) + static_cast<uint32_t>(lane) * 128u;
+        uint32_t acc_bits = 0u;  // phase bit of each accumulator
         int it = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it)
         {
             const int b = it & 1;
             int m0, n0;
             tile_of(t, p.lower, tiles_n, m0, n0);
-            if (!mbar_wait(&tfull[b], acc_ph[b], abort_flag))
+            if (!mbar_wait(&tfull[b], (acc_bits >> b) & 1u, abort_flag))
             {
                 break;
             }
@@ -388,59 +417,75 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             tmem_ld_wait();
             tc_fence_before();
             mbar_arrive(&tempty[b]);
-            acc_ph[b] ^= 1u;
+            acc_bits ^= 1u << b;
 
             const int row = m0 + r_in;
-            const int c0 = n0 + h * EPI_COLS;
-            if (row < p.M && c0 < p.N)
+            const int row0 = m0 + q * 32;  // first row of this warp's sub-tiles
+            const bool diag = p.lower && m0 == n0;
+            double sq = 0.0;
+#pragma unroll
+            for (int c = 0; c < EPI_COLS / 32; ++c)
             {
-                float *crow = p.C + static_cast<int64_t>(row) * p.ldc + c0;
-                double sq = 0.0;
-                const bool fast = (c0 + EPI_COLS - 1 < p.N) && (!p.lower || c0 + EPI_COLS - 1 <= row);
-                if (fast)
+                const int col0 = n0 + h * EPI_COLS + c * 32;
+                // warp-uniform: sub-tile outside C, or entirely above the diagonal
+                if (col0 >= p.N || (diag && col0 >= row0 + 32))
                 {
-                    // issue every load of the segment before the first store
-                    float4 cv[EPI_COLS / 4];
+                    continue;
+                }
+                float w[32];
 #pragma unroll
-                    for (int j = 0; j < EPI_COLS / 4; ++j)
+                for (int j = 0; j < 32; ++j)
+                {
+                    float val = p.alpha * v[c * 32 + j];
+                    if (diag && col0 + j > row)
                     {
-                        cv[j] = (p.beta != 0.0f) ? __ldcg(reinterpret_cast<const float4 *>(crow) + j)
-                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+                        val = 0.0f;
                     }
-#pragma unroll
-                    for (int j = 0; j < EPI_COLS / 4; ++j)
+                    w[j] = val;
+                    if (p.rowsq != nullptr && col0 + j < p.N)
                     {
-                        float4 nv;
-                        nv.x = cv[j].x + p.alpha * v[4 * j + 0];
-                        nv.y = cv[j].y + p.alpha * v[4 * j + 1];
-                        nv.z = cv[j].z + p.alpha * v[4 * j + 2];
-                        nv.w = cv[j].w + p.alpha * v[4 * j + 3];
-                        __stcg(reinterpret_cast<float4 *>(crow) + j, nv);
-                        sq += static_cast<double>(nv.x) * nv.x + static_cast<double>(nv.y) * nv.y +
-                              static_cast<double>(nv.z) * nv.z + static_cast<double>(nv.w) * nv.w;
+                        sq += static_cast<double>(val) * val;
                     }
                 }
-                else
+                // the previous bulk operation of this warp must have read the buffer
+                if (lane == 0)
                 {
-#pragma unroll
-                    for (int j = 0; j < EPI_COLS; ++j)
-                    {
-                        const int cc = c0 + j;
-                        if (cc < p.N && (!p.lower || cc <= row))
-                        {
-                            const float o = (p.beta != 0.0f) ? crow[j] : 0.0f;
-                            const float nv = o + p.alpha * v[j];
-                            crow[j] = nv;
-                            sq += static_cast<double>(nv) * nv;
-                        }
-                    }
+                    bulk_wait_read_all();
                 }
-                if (p.rowsq != nullptr)
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
                 {
-                    p.rowsq[h * p.rowsq_half + row] += sq;  // single writer per word and launch
+                    const uint32_t addr = buf_row + (static_cast<uint32_t>(j ^ (lane & 7)) << 4);
+                    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(w[4 * j]),
+                                 "f"(w[4 * j + 1]), "f"(w[4 * j + 2]), "f"(w[4 * j + 3])
+                                 : "memory");
+                }
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0)
+                {
+                    if (p.beta != 0.0f)
+                    {
+                        tma_reduce_add_2d(&tmC, buf, col0, row0);
+                    }
+                    else
+                    {
+                        tma_store_2d(&tmC, buf, col0, row0);
+                    }
+                    bulk_commit();
                 }
             }
+            if (p.rowsq != nullptr && row < p.M)
+            {
+                p.rowsq[h * p.rowsq_half + row] += sq;  // single writer per word and launch
+            }
         }
+        if (lane == 0)
+        {
+            bulk_wait_all();
+        }
+        __syncwarp();
     }
 
     tc_fence_before();
@@ -584,13 +629,33 @@ void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cud
     {
         throw Error(1, "tc_gemm: lower mode needs M == N");
     }
-    if (args.rowsq != nullptr && (args.N > TN || args.lower || args.rowsq_half < args.M))
+    if (args.rowsq != nullptr && (args.N > TN || args.lower || args.rowsq_half < args.M || args.beta != 0.0f))
     {
-        throw Error(1, "tc_gemm: rowsq needs N <= 128 and rowsq_half >= M");
+        throw Error(1, "tc_gemm: rowsq needs N <= 128, beta = 0 and rowsq_half >= M");
+    }
+    if (args.ldc < args.N)
+    {
+        throw Error(1, "tc_gemm: ldc must be >= N");
     }
     if (!(args.beta == 0.0f || args.beta == 1.0f))
     {
         throw Error(1, "tc_gemm: beta must be 0 or 1");
+    }
+    // C as a TMA tensor (FP32, 32 x 32 boxes with 128-byte swizzle) for the
+    // epilogue's bulk stores / reduce-adds
+    CUtensorMap tmC;
+    {
+        cuuint64_t dims[2] = { static_cast<cuuint64_t>(args.N), static_cast<cuuint64_t>(args.M) };
+        cuuint64_t strides[1] = { static_cast<cuuint64_t>(args.ldc * 4) };
+        cuuint32_t box[2] = { 32u, 32u };
+        cuuint32_t estrides[2] = { 1u, 1u };
+        CUresult r = get_encode()(&tmC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, static_cast<void *>(args.C), dims, strides,
+                                  box, estrides, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+        {
+            throw Error(4, "cuTensorMapEncodeTiled (C) failed with code " + std::to_string(static_cast<int>(r)));
+        }
     }
     const int tiles_m = ceil_div(args.M, TM);
     const int tiles_n = ceil_div(args.N, TN);
@@ -604,12 +669,12 @@ void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cud
     if (A.kind == TcKind::TF32)
     {
         ensure_smem_attr(reinterpret_cast<const void *>(tc_gemm_kernel<0>), SMEM_BYTES);
-        tc_gemm_kernel<0><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(A.map, B.map, args, tiles_n, ntiles);
+        tc_gemm_kernel<0><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(A.map, B.map, tmC, args, tiles_n, ntiles);
     }
     else
     {
         ensure_smem_attr(reinterpret_cast<const void *>(tc_gemm_kernel<1>), SMEM_BYTES);
-        tc_gemm_kernel<1><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(A.map, B.map, args, tiles_n, ntiles);
+        tc_gemm_kernel<1><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(A.map, B.map, tmC, args, tiles_n, ntiles);
     }
     GPRAT_LAUNCH_CHECK();
     if (timed)

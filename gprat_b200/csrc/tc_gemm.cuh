@@ -41,8 +41,9 @@ struct TcGemmArgs
     float *C;
     int64_t ldc;
     float alpha, beta;  // beta must be 0 or 1
-    bool lower;         // M == N; only C[i][j] with i >= j is written, tiles above the diagonal skipped
-    // optional (N <= 128): per-row sums of squares of the new C, split by
+    bool lower;         // M == N; only C[i][j] with i >= j is updated, tiles above the diagonal skipped
+                        // (within diagonal tiles, beta = 0 writes 0 above the diagonal)
+    // optional (N <= 128, beta = 0): per-row sums of squares of the new C, split by
     // column half so that no two threads add into one word (deterministic):
     // rowsq[i] += sum_{j<64} C_new[i][j]^2, rowsq[rowsq_half + i] += sum_{j>=64} ...
     double *rowsq;

@@ -67,3 +67,15 @@ def test_persistent_multi_tile(capi, kind):
     # 16 x 16 tiles > 148 SMs: every CTA processes several tiles and both
     # TMEM accumulators
     run_case(capi, kind, 2048, 2048, 512, -1.0, 1.0, seed=4)
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_reduce_add_ragged_edges(capi, kind):
+    # beta = 1 goes through the TMA reduce-add: partial tiles must be clipped
+    run_case(capi, kind, 200, 130, 192, -1.0, 1.0, seed=5)
+    run_case(capi, kind, 5, 7, 64, 1.0, 1.0, seed=6)
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_lower_triangle_ragged(capi, kind):
+    run_case(capi, kind, 300, 300, 128, -1.0, 1.0, lower=True, seed=7)
