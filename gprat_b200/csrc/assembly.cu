@@ -6,12 +6,21 @@
 //
 // One CTA produces a 64-row x 128-column block.  The two windows of the
 // series it needs (64+d-1 and 128+d-1 values) are staged in shared memory
-// once; each thread owns one column and walks the rows four at a time, so
-// row values are shared-memory broadcasts and column values are
-// conflict-free.  Every row of the block is written by whole warps as
-// contiguous 256-byte segments (coalesced).  The distance sum keeps the
-// reference's order and rounding (separate multiply and add, k ascending),
-// so entries differ from the reference only by exp()'s last-place rounding.
+// once; each thread owns one column and walks the rows, so row values are
+// shared-memory broadcasts and column values are conflict-free.  Every row of
+// the block is written by whole warps as contiguous 256-byte segments
+// (coalesced).
+//
+// Distances.  For d < 16 every entry sums its d squares directly, in the
+// reference's order and rounding (separate multiply and add, k ascending), so
+// entries differ from the reference only by exp()'s last-place rounding.  For
+// d >= 16 the sliding windows give an O(1) update along each diagonal,
+//   D(i, j) = D(i-1, j-1) - (x_{i-1} - x_{j-1})^2 + (x_{i+d-1} - x_{j+d-1})^2,
+// so only the block's first row and the first column of each warp are summed
+// directly (d terms); the other entries take the left neighbour's previous-row
+// distance by shuffle.  The drift over at most 63 steps is ~1e-14 of D.
+// Per-row windows (row_offsets, a serving batch) always sum directly, so an
+// entry does not depend on where its row falls in a batch.
 #include "common.cuh"
 
 namespace gprat_cu
@@ -51,8 +60,23 @@ __device__ __forceinline__ void distances(const double *xr, const double *xc, in
     }
 }
 
+// Direct distance of local row i (window at xr[i * rs]) and local column j.
+__device__ __forceinline__ double distance1(const double *xr, const double *xc, int i, int j, int d, int rs)
+{
+    double acc = 0.0;
+    for (int k = 0; k < d; ++k)
+    {
+        const double z = __dsub_rn(xr[i * rs + k], xc[j + k]);
+        acc = __dadd_rn(acc, __dmul_rn(z, z));
+    }
+    return acc;
+}
+
+constexpr int RECUR_MIN_D = 16;
+
 // mode 0: K (lower tiles of size T incl. full diagonal tiles, + noise on the
 //         global diagonal); mode 1: cross / prior (all entries, no noise).
+// out32 (optional, mode 0): the same entries rounded to FP32 (mixed path).
 template <int MODE, typename OutT>
 __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
                                                int rows,
@@ -66,7 +90,9 @@ __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
                                                const double *__restrict__ alpha,
                                                double *__restrict__ mean_partial,
                                                int mean_parts,
-                                               const int64_t *__restrict__ row_offsets)
+                                               const int64_t *__restrict__ row_offsets,
+                                               float *__restrict__ out32,
+                                               int64_t ld32)
 {
     extern __shared__ double sh[];
     const int i0 = blockIdx.y * AR;
@@ -87,6 +113,7 @@ __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
     double *xr = sh;                 // xr_size
     double *xc = sh + xr_size;       // AC + d - 1
     double *red = xc + AC + d;       // AR x (AC/32) mean partials
+    double *bnd = red + AR * (AC / 32);  // AR x (AC/32): direct distances of each warp's first column
     if (row_offsets != nullptr)
     {
         for (int q = threadIdx.x; q < AR * d; q += AC)
@@ -120,41 +147,77 @@ __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
     const double aj = (alpha != nullptr && gj < cols) ? alpha[gj] : 0.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-    for (int i = 0; i < AR; i += RB)
+    const bool recur = d >= RECUR_MIN_D && row_offsets == nullptr;
+    auto emit = [&](int r, double dist)
     {
-        double acc[RB];
-        distances(xr, xc, i, j, d, rs, acc);
-#pragma unroll
-        for (int r = 0; r < RB; ++r)
+        const int gi = i0 + r;
+        double val = se_entry(dist, nh, v);
+        bool inside = gi < rows && gj < cols;
+        if (MODE == 0)
         {
-            int gi = i0 + i + r;
-            double val = se_entry(acc[r], nh, v);
-            bool inside = gi < rows && gj < cols;
-            if (MODE == 0)
+            inside = inside && (gj / T <= gi / T);
+            if (gi == gj)
             {
-                inside = inside && (gj / T <= gi / T);
-                if (gi == gj)
-                {
-                    val += noise;
-                }
+                val += noise;
             }
-            if (inside && out != nullptr)
-            {
-                out[static_cast<int64_t>(gi) * ldo + gj] = static_cast<OutT>(val);
-            }
-            if (mean_partial != nullptr)
-            {
-                double prod = inside ? val * aj : 0.0;
+        }
+        if (inside && out != nullptr)
+        {
+            out[static_cast<int64_t>(gi) * ldo + gj] = static_cast<OutT>(val);
+        }
+        if (MODE == 0 && inside && out32 != nullptr)
+        {
+            out32[static_cast<int64_t>(gi) * ld32 + gj] = static_cast<float>(val);
+        }
+        if (mean_partial != nullptr)
+        {
+            double prod = inside ? val * aj : 0.0;
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1)
-                {
-                    prod += __shfl_xor_sync(0xffffffffu, prod, o);
-                }
-                if (lane == 0)
-                {
-                    red[(i + r) * (AC / 32) + warp] = prod;
-                }
+            for (int o = 16; o > 0; o >>= 1)
+            {
+                prod += __shfl_xor_sync(0xffffffffu, prod, o);
             }
+            if (lane == 0)
+            {
+                red[r * (AC / 32) + warp] = prod;
+            }
+        }
+    };
+
+    if (!recur)
+    {
+        for (int i = 0; i < AR; i += RB)
+        {
+            double acc[RB];
+            distances(xr, xc, i, j, d, rs, acc);
+#pragma unroll
+            for (int r = 0; r < RB; ++r)
+            {
+                emit(i + r, acc[r]);
+            }
+        }
+    }
+    else
+    {
+        // prologue: the first column of every warp, summed directly
+        for (int q = threadIdx.x; q < AR * (AC / 32); q += AC)
+        {
+            const int w = q / AR, r = q % AR;
+            bnd[r * (AC / 32) + w] = distance1(xr, xc, r, 32 * w, d, 1);
+        }
+        __syncthreads();
+        double dprev = distance1(xr, xc, 0, j, d, 1);
+        emit(0, dprev);
+        const int jl = max(j - 1, 0);  // lane 0 takes bnd instead
+        for (int r = 1; r < AR; ++r)
+        {
+            const double dleft = __shfl_up_sync(0xffffffffu, dprev, 1);
+            const double z1 = __dsub_rn(xr[r - 1], xc[jl]);
+            const double z2 = __dsub_rn(xr[r + d - 1], xc[j + d - 1]);
+            const double rec = __dadd_rn(__dsub_rn(dleft, __dmul_rn(z1, z1)), __dmul_rn(z2, z2));
+            const double dcur = (lane == 0) ? bnd[r * (AC / 32) + warp] : rec;
+            emit(r, dcur);
+            dprev = dcur;
         }
     }
     if (mean_partial != nullptr)
@@ -194,13 +257,13 @@ __global__ void reduce_rows_kernel(const double *__restrict__ part, int m, int p
 size_t se_smem(int d, bool per_row)
 {
     const size_t xr = per_row ? static_cast<size_t>(AR) * d : static_cast<size_t>(AR + d);
-    return (xr + AC + d + AR * (AC / 32)) * sizeof(double);
+    return (xr + AC + d + 2 * AR * (AC / 32)) * sizeof(double);
 }
 
 template <int MODE, typename OutT>
 void launch_se(const double *xrow, int rows, const double *xcol, int cols, int d, int T, const DeviceParams *p,
                OutT *out, int64_t ldo, const double *alpha, double *mean_partial, int parts, cudaStream_t s,
-               const int64_t *row_offsets = nullptr)
+               const int64_t *row_offsets = nullptr, float *out32 = nullptr, int64_t ld32 = 0)
 {
     if (rows <= 0 || cols <= 0)
     {
@@ -217,16 +280,16 @@ void launch_se(const double *xrow, int rows, const double *xcol, int cols, int d
     }
     dim3 grid(ceil_div(cols, AC), ceil_div(rows, AR));
     se_kernel<MODE, OutT><<<grid, AC, smem, s>>>(xrow, rows, xcol, cols, d, T, p, out, ldo, alpha, mean_partial,
-                                                 parts, row_offsets);
+                                                 parts, row_offsets, out32, ld32);
     GPRAT_LAUNCH_CHECK();
 }
 
 }  // namespace
 
 void assemble_covariance(const double *x, int n, int n_reg, int tile, const DeviceParams *p, double *K, int64_t ldk,
-                         cudaStream_t s)
+                         cudaStream_t s, float *K32, int64_t ld32)
 {
-    launch_se<0>(x, n, x, n, n_reg, tile, p, K, ldk, nullptr, nullptr, 0, s);
+    launch_se<0>(x, n, x, n, n_reg, tile, p, K, ldk, nullptr, nullptr, 0, s, nullptr, K32, ld32);
 }
 
 void assemble_cross(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, double *Kx,

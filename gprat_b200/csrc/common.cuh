@@ -95,6 +95,9 @@ void set_params(DeviceParams *p, const DeviceParams &value, cudaStream_t s);
 
 inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
+// Streaming multiprocessors of the current device.
+int device_sm_count();
+
 inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
 
 // ---------------------------------------------------------------------------
@@ -128,8 +131,9 @@ void dgemm(const GemmArgs &a, cudaStream_t s);
 // SE covariance assembly (gen_tile_covariance, core/src/cpu/gp_algorithms.cpp:30-62):
 // K[i][j] = v*exp(-0.5/l^2 * sum_k (x[i+k]-x[j+k])^2) (+ noise if i == j), for all
 // (i,j) with floor(j/T) <= floor(i/T) (lower tiles incl. full diagonal tiles).
+// K32 (optional): the same entries rounded to FP32 (row-major, ld32).
 void assemble_covariance(const double *x, int n, int n_reg, int tile, const DeviceParams *p, double *K, int64_t ldk,
-                         cudaStream_t s);
+                         cudaStream_t s, float *K32 = nullptr, int64_t ld32 = 0);
 
 // Cross covariance Kx[r][c] = k(xt_r, x_c), r < m, c < n
 // (gen_tile_cross_covariance, core/src/cpu/gp_algorithms.cpp:113-140).  If
@@ -156,6 +160,11 @@ void assemble_prior(const double *xt, int m, int n_reg, const DeviceParams *p, d
 // the diagonal).  Records the first failing pivot in status.
 void potrf_diag(double *A, int64_t lda, int bs, int row0, double *Linv, int64_t ldi, DeviceStatus *status,
                 cudaStream_t s);
+// Same for an FP32 block (factored in FP64 in shared memory, L written back
+// in FP32); also writes Linv in FP32 (Linv32, ldi32) and the FP64 diagonal of
+// L (diag, bs values).
+void potrf_diag_f32(float *A, int64_t lda, int bs, int row0, double *Linv, int64_t ldi, float *Linv32, int64_t ldi32,
+                    double *diag, DeviceStatus *status, cudaStream_t s);
 
 // Triangular solves with the blocked factor (L in Lmat, diagonal-block
 // inverses in Linv, block size nb).

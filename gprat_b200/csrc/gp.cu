@@ -410,6 +410,26 @@ int64_t gp_resident_bytes(const gprat_cu_gp *gp)
     return b;
 }
 
+void gp_reserve_predict(gprat_cu_gp *gp, int m)
+{
+    DeviceGuard guard(gp->device);
+    const int parts = ceil_div(gp->n, 128);
+    gp->mean_part.ensure(static_cast<int64_t>(m) * parts);
+    gp->vacc.ensure(2 * static_cast<int64_t>(m));
+    if (gp->precision == GPRAT_CU_PREC_FP64)
+    {
+        gp->W.ensure(static_cast<int64_t>(m) * gp->ld);
+    }
+    else
+    {
+        gp->W32.ensure(static_cast<int64_t>(m) * gp->ld32);
+        if (gp->precision == GPRAT_CU_PREC_MIXED_BF16)
+        {
+            gp->Wb.ensure(static_cast<int64_t>(m) * gp->ld32);
+        }
+    }
+}
+
 int64_t gp_predict_bytes(const gprat_cu_gp *gp, int m)
 {
     // solve matrix + mean partials + variance accumulator for m rows

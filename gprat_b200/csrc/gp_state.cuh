@@ -7,6 +7,7 @@
 #include "tc_gemm.cuh"
 
 #include <initializer_list>
+#include <vector>
 
 namespace gprat_cu
 {
@@ -62,6 +63,8 @@ struct gprat_cu_gp
 {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // high-priority stream of the look-ahead panel factorisation
+    std::vector<cudaEvent_t> events;  // look-ahead ordering events (created on first use)
     int n = 0, n_tiles = 0, T = 0, d = 0;
     int64_t n_in = 0;
     int64_t ld = 0;    // FP64 leading dimension
@@ -95,6 +98,10 @@ struct gprat_cu_gp
         {
             cudaStreamSynchronize(stream);
         }
+        if (side != nullptr)
+        {
+            cudaStreamSynchronize(side);
+        }
         for (gprat_cu::DevBuf<double> *b : { &x, &y, &K, &Linv, &alpha, &U, &partials, &xt, &W, &vacc, &mean_part,
                                              &mean, &var, &losses, &D64, &pcg_r, &pcg_z, &pcg_p, &pcg_q, &symv_part })
         {
@@ -116,6 +123,14 @@ struct gprat_cu_gp
         if (h_status != nullptr)
         {
             cudaFreeHost(h_status);
+        }
+        if (side != nullptr)
+        {
+            cudaStreamDestroy(side);
+        }
+        for (cudaEvent_t e : events)
+        {
+            cudaEventDestroy(e);
         }
         if (stream != nullptr)
         {
@@ -144,6 +159,8 @@ void gp_predict_batch(gprat_cu_gp *gp, const double *d_series, const int64_t *d_
 void gp_check(gprat_cu_gp *gp, cudaStream_t s);
 int64_t gp_resident_bytes(const gprat_cu_gp *gp);
 int64_t gp_predict_bytes(const gprat_cu_gp *gp, int m);
+// Allocates the predict working set for m test points now (no later growth).
+void gp_reserve_predict(gprat_cu_gp *gp, int m);
 void loss_mixed(gprat_cu_gp *gp, cudaStream_t s);
 
 }  // namespace gprat_cu

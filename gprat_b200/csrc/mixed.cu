@@ -321,6 +321,47 @@ void precondition(gprat_cu_gp *gp, const double *r, double *z, cudaStream_t s)
 
 }  // namespace
 
+namespace
+{
+
+constexpr int SIDE_SMS = 16;         // SMs kept free for the look-ahead stream next to a large update
+constexpr int LARGE_UPDATE = 16384;  // trailing-update size above which the look-ahead stream is limited
+
+void ensure_lookahead(gprat_cu_gp *gp, int nevents)
+{
+    if (gp->side == nullptr)
+    {
+        int least = 0, greatest = 0;
+        GPRAT_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        GPRAT_CUDA_CHECK(cudaStreamCreateWithPriority(&gp->side, cudaStreamNonBlocking, greatest));
+    }
+    while (static_cast<int>(gp->events.size()) < nevents)
+    {
+        cudaEvent_t e = nullptr;
+        GPRAT_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        gp->events.push_back(e);
+    }
+}
+
+TcGemmArgs limited(TcGemmArgs a, int max_ctas)
+{
+    a.max_ctas = max_ctas;
+    return a;
+}
+
+}  // namespace
+
+// Right-looking Cholesky of the FP32 working copy in outer panels of NBO
+// columns (inner blocks of NB), with a look-ahead of one panel:
+//   side stream (high priority): factor panel k (diagonal blocks in FP64,
+//     panel solves and the in-panel updates on tcgen05), then apply panel k
+//     to the columns of panel k+1 and factor panel k+1;
+//   main stream: the trailing update of everything right of panel k+1 with
+//     panel k (the bulk of the flops), on all but SIDE_SMS SMs while the side
+//     stream works next to it.
+// Events order the two streams: panel k+1's columns are written by the
+// update of panel k-1 (main) before the side stream touches them, and the
+// update of panel k waits for panel k's factorisation.
 void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
 {
     const int n = gp->n;
@@ -338,68 +379,114 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
     {
         gp->Lb.ensure(static_cast<int64_t>(n) * ld32);
     }
-    double *D = gp->D64.ptr;
     double *ldiag = gp->D64.ptr + NB * NB;
+    const int nout = ceil_div(n, NBO);
+    ensure_lookahead(gp, 2 * nout + 1);
+    cudaStream_t side = gp->side;
+    auto evF = [&](int k) { return gp->events[1 + k]; };
+    auto evR = [&](int k) { return gp->events[1 + nout + k]; };
+    const int sms = device_sm_count();
 
-    assemble_covariance(gp->x.ptr, n, gp->d, gp->T, gp->params.ptr, gp->K.ptr, gp->ld, s);
-    convert_f64_to_f32(gp->K.ptr, gp->ld, gp->K32.ptr, ld32, n, n, s);
+    assemble_covariance(gp->x.ptr, n, gp->d, gp->T, gp->params.ptr, gp->K.ptr, gp->ld, s, gp->K32.ptr, ld32);
+    GPRAT_CUDA_CHECK(cudaEventRecord(gp->events[0], s));
+    GPRAT_CUDA_CHECK(cudaStreamWaitEvent(side, gp->events[0], 0));
     const MixedOps ops = make_ops(gp);
     float *K32 = gp->K32.ptr;
     auto at = [&](int r, int c) { return K32 + static_cast<int64_t>(r) * ld32 + c; };
 
-    for (int K0 = 0; K0 < n; K0 += NBO)
+    // factor panel [K0, pend): diagonal blocks, panel solves, in-panel updates
+    auto factor_panel = [&](int K0, int pend, int ctas)
     {
-        const int bo = std::min(NBO, n - K0);
-        const int pend = K0 + bo;
         for (int r0 = K0; r0 < pend; r0 += NB)
         {
             const int k = r0 / NB;
             double *Lk = gp->Linv.ptr + static_cast<int64_t>(k) * NB * NB;
-            convert_f32_to_f64(at(r0, r0), ld32, D, NB, NB, NB, s);
-            potrf_diag(D, NB, NB, r0, Lk, NB, gp->status.ptr, s);
-            GPRAT_CUDA_CHECK(cudaMemcpy2DAsync(ldiag + r0, sizeof(double), D, (NB + 1) * sizeof(double),
-                                               sizeof(double), NB, cudaMemcpyDeviceToDevice, s));
-            convert_f64_to_f32(D, NB, at(r0, r0), ld32, NB, NB, s);
-            convert_f64_to_f32(Lk, NB, gp->Linv32.ptr + static_cast<int64_t>(k) * NB * NB, NB, NB, NB, s);
+            potrf_diag_f32(at(r0, r0), ld32, NB, r0, Lk, NB, gp->Linv32.ptr + static_cast<int64_t>(k) * NB * NB, NB,
+                           ldiag + r0, gp->status.ptr, side);
             const int rows = n - r0 - NB;
             if (rows > 0)
             {
                 // panel solve P = P Linv^T on the tensor cores (TF32), in place
                 tc_gemm(ops.L, ops.Linv,
-                        tc_args(rows, NB, NB, r0 + NB, r0, k * NB, 0, at(r0 + NB, r0), ld32, 1.0f, 0.0f, false,
-                                nullptr, gp->status.ptr),
-                        s);
+                        limited(tc_args(rows, NB, NB, r0 + NB, r0, k * NB, 0, at(r0 + NB, r0), ld32, 1.0f, 0.0f, false,
+                                        nullptr, gp->status.ptr),
+                                ctas),
+                        side);
             }
             if (ops.bf16)
             {
                 convert_f32_to_bf16(at(r0, r0), ld32, gp->Lb.ptr + static_cast<int64_t>(r0) * ld32 + r0, ld32,
-                                    n - r0, NB, s);
+                                    n - r0, NB, side);
             }
             const int ncols = pend - (r0 + NB);
             if (ncols > 0)
             {
                 tc_gemm(ops.trail(), ops.trail(),
-                        tc_args(ncols, ncols, NB, r0 + NB, r0, r0 + NB, r0, at(r0 + NB, r0 + NB), ld32, -1.0f, 1.0f,
-                                true, nullptr, gp->status.ptr),
-                        s);
+                        limited(tc_args(ncols, ncols, NB, r0 + NB, r0, r0 + NB, r0, at(r0 + NB, r0 + NB), ld32, -1.0f,
+                                        1.0f, true, nullptr, gp->status.ptr),
+                                ctas),
+                        side);
                 const int below = n - pend;
                 if (below > 0)
                 {
                     tc_gemm(ops.trail(), ops.trail(),
-                            tc_args(below, ncols, NB, pend, r0, r0 + NB, r0, at(pend, r0 + NB), ld32, -1.0f, 1.0f,
-                                    false, nullptr, gp->status.ptr),
-                            s);
+                            limited(tc_args(below, ncols, NB, pend, r0, r0 + NB, r0, at(pend, r0 + NB), ld32, -1.0f,
+                                            1.0f, false, nullptr, gp->status.ptr),
+                                    ctas),
+                            side);
                 }
             }
         }
-        const int rest = n - pend;
+    };
+
+    factor_panel(0, std::min(NBO, n), 0);
+    GPRAT_CUDA_CHECK(cudaEventRecord(evF(0), side));
+    for (int k = 0; k < nout; ++k)
+    {
+        const int K0 = k * NBO;
+        const int pend = std::min(K0 + NBO, n);
+        const int bo = pend - K0;
+        const int next_end = std::min(pend + NBO, n);  // end of panel k+1
+        const int rest = n - next_end;
+        const bool ahead = k + 1 < nout;
+        const bool large = rest >= LARGE_UPDATE;
+        // main: everything right of panel k+1, with panel k
+        GPRAT_CUDA_CHECK(cudaStreamWaitEvent(s, evF(k), 0));
         if (rest > 0)
         {
             tc_gemm(ops.trail(), ops.trail(),
-                    tc_args(rest, rest, bo, pend, K0, pend, K0, at(pend, pend), ld32, -1.0f, 1.0f, true, nullptr,
-                            gp->status.ptr),
+                    limited(tc_args(rest, rest, bo, next_end, K0, next_end, K0, at(next_end, next_end), ld32, -1.0f,
+                                    1.0f, true, nullptr, gp->status.ptr),
+                            ahead ? sms - SIDE_SMS : 0),
                     s);
         }
+        GPRAT_CUDA_CHECK(cudaEventRecord(evR(k), s));
+        if (!ahead)
+        {
+            break;
+        }
+        // side: panel k applied to panel k+1's columns, then panel k+1 factored
+        const int side_ctas = large ? SIDE_SMS : 0;
+        if (k >= 1)
+        {
+            GPRAT_CUDA_CHECK(cudaStreamWaitEvent(side, evR(k - 1), 0));
+        }
+        const int nb = next_end - pend;
+        tc_gemm(ops.trail(), ops.trail(),
+                limited(tc_args(nb, nb, bo, pend, K0, pend, K0, at(pend, pend), ld32, -1.0f, 1.0f, true, nullptr,
+                                gp->status.ptr),
+                        side_ctas),
+                side);
+        if (rest > 0)
+        {
+            tc_gemm(ops.trail(), ops.trail(),
+                    limited(tc_args(rest, nb, bo, next_end, K0, pend, K0, at(next_end, pend), ld32, -1.0f, 1.0f, false,
+                                    nullptr, gp->status.ptr),
+                            side_ctas),
+                    side);
+        }
+        factor_panel(pend, next_end, side_ctas);
+        GPRAT_CUDA_CHECK(cudaEventRecord(evF(k + 1), side));
     }
 }
 

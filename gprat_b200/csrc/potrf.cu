@@ -154,8 +154,13 @@ __device__ __forceinline__ void diag_factor_invert(double *a, int c0, int bs, in
     }
 }
 
-__global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(double *__restrict__ A, int64_t lda, int bs, int row0,
+// T: element type of the block in global memory (FP64, or FP32 for the
+// mixed path, which then also receives Linv in FP32 and the FP64 diagonal of L).
+template <typename T>
+__global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ A, int64_t lda, int bs, int row0,
                                                                 double *__restrict__ Linv, int64_t ldi,
+                                                                float *__restrict__ Linv32, int64_t ldi32,
+                                                                double *__restrict__ diag_out,
                                                                 DeviceStatus *__restrict__ status)
 {
     extern __shared__ double sa[];  // [PB][PS]
@@ -180,7 +185,7 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(double *__restri
         double v = (i == c) ? 1.0 : 0.0;
         if (i < bs && c <= i)
         {
-            v = A[static_cast<int64_t>(i) * lda + c];
+            v = static_cast<double>(A[static_cast<int64_t>(i) * lda + c]);
         }
         sa[i * PS + c] = v;
     }
@@ -291,8 +296,12 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(double *__restri
         const int i = idx >> 7, c = idx & (PB - 1);
         if (i < bs && c <= i)
         {
-            A[static_cast<int64_t>(i) * lda + c] = sa[i * PS + c];
+            A[static_cast<int64_t>(i) * lda + c] = static_cast<T>(sa[i * PS + c]);
         }
+    }
+    if (diag_out != nullptr && tid < bs)
+    {
+        diag_out[tid] = sa[tid * PS + tid];
     }
     __syncthreads();
 
@@ -367,7 +376,12 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(double *__restri
         const int i = idx >> 7, c = idx & (PB - 1);
         if (i < bs && c < bs)
         {
-            Linv[static_cast<int64_t>(i) * ldi + c] = (c <= i) ? sa[i * PS + c] : 0.0;
+            const double v = (c <= i) ? sa[i * PS + c] : 0.0;
+            Linv[static_cast<int64_t>(i) * ldi + c] = v;
+            if (Linv32 != nullptr)
+            {
+                Linv32[static_cast<int64_t>(i) * ldi32 + c] = static_cast<float>(v);
+            }
         }
     }
 }
@@ -382,8 +396,21 @@ void potrf_diag(double *A, int64_t lda, int bs, int row0, double *Linv, int64_t 
         throw Error(1, "potrf_diag: block size must be in [1, 128]");
     }
     constexpr size_t smem = SMEM_DOUBLES * sizeof(double);
-    ensure_smem_attr(reinterpret_cast<const void *>(potrf_inv_kernel), static_cast<int>(smem));
-    potrf_inv_kernel<<<1, PTHREADS, smem, s>>>(A, lda, bs, row0, Linv, ldi, status);
+    ensure_smem_attr(reinterpret_cast<const void *>(potrf_inv_kernel<double>), static_cast<int>(smem));
+    potrf_inv_kernel<double><<<1, PTHREADS, smem, s>>>(A, lda, bs, row0, Linv, ldi, nullptr, 0, nullptr, status);
+    GPRAT_LAUNCH_CHECK();
+}
+
+void potrf_diag_f32(float *A, int64_t lda, int bs, int row0, double *Linv, int64_t ldi, float *Linv32, int64_t ldi32,
+                    double *diag, DeviceStatus *status, cudaStream_t s)
+{
+    if (bs <= 0 || bs > PB)
+    {
+        throw Error(1, "potrf_diag_f32: block size must be in [1, 128]");
+    }
+    constexpr size_t smem = SMEM_DOUBLES * sizeof(double);
+    ensure_smem_attr(reinterpret_cast<const void *>(potrf_inv_kernel<float>), static_cast<int>(smem));
+    potrf_inv_kernel<float><<<1, PTHREADS, smem, s>>>(A, lda, bs, row0, Linv, ldi, Linv32, ldi32, diag, status);
     GPRAT_LAUNCH_CHECK();
 }
 

@@ -16,9 +16,13 @@
 //               allow.
 //   fitter    : fit requests (a new model) run on their own streams, so they
 //               overlap with predict batches on the device.
-// Memory: resident bytes of every model plus the working set of in-flight
-// batches stay below the budget; a batch takes requests in arrival order
-// while they fit.
+// Memory: every model reserves its factor, weights and the working set of a
+// batch of RESERVED_ROWS test points when it is created, so steady-state
+// batches allocate nothing (an allocation or free would synchronise the
+// device and stall every other stream).  A batch beyond the reservation (a
+// single request larger than RESERVED_ROWS) is charged its extra working set
+// while it runs.  Resident models plus those extras stay below the budget; a
+// batch takes requests in arrival order while they fit.
 #include "gp_state.cuh"
 
 #include <algorithm>
@@ -43,7 +47,8 @@ using Clock = std::chrono::steady_clock;
 namespace
 {
 
-constexpr int MAX_BATCH_ROWS = 16384;
+constexpr int MAX_BATCH_ROWS = 8192;  // rows per batch unless one request alone is larger
+constexpr int RESERVED_ROWS = MAX_BATCH_ROWS;
 
 struct Request
 {
@@ -178,7 +183,17 @@ std::unique_ptr<Model> make_model(gprat_cu_server *sv, const double *x, int64_t 
     }
     gp_fit(gp, hyper, gp->stream);
     gp_check(gp, gp->stream);
-    m->resident = gp_resident_bytes(gp);
+    // reserve a full batch: device working set, staging and pinned buffers
+    gp_reserve_predict(gp, RESERVED_ROWS);
+    m->d_series.ensure(static_cast<int64_t>(RESERVED_ROWS) * d);
+    m->d_offsets.ensure(RESERVED_ROWS);
+    m->d_mean.ensure(RESERVED_ROWS);
+    m->d_var.ensure(RESERVED_ROWS);
+    m->h_in.ensure(static_cast<size_t>(RESERVED_ROWS) * d * sizeof(double) + RESERVED_ROWS * sizeof(int64_t));
+    m->h_out.ensure(2 * static_cast<size_t>(RESERVED_ROWS) * sizeof(double));
+    GPRAT_CUDA_CHECK(cudaStreamSynchronize(gp->stream));
+    m->resident = gp_resident_bytes(gp) + gp_predict_bytes(gp, RESERVED_ROWS) +
+                  static_cast<int64_t>(RESERVED_ROWS) * (d + 4) * 8;
     GPRAT_CUDA_CHECK(cudaEventCreateWithFlags(&m->done_ev, cudaEventDisableTiming));
     return m;
 }
@@ -281,7 +296,13 @@ void launch(gprat_cu_server *sv, std::unique_lock<std::mutex> &lk)
                 ++it;
                 continue;
             }
-            const int64_t need = gp_predict_bytes(md.gp, rows + r->m) - gp_predict_bytes(md.gp, rows);
+            // working set beyond the model's reservation
+            auto extra = [&](int nrows)
+            {
+                return nrows <= RESERVED_ROWS ? int64_t{ 0 }
+                                              : gp_predict_bytes(md.gp, nrows) - gp_predict_bytes(md.gp, RESERVED_ROWS);
+            };
+            const int64_t need = extra(rows + r->m) - extra(rows);
             const bool fits_rows = rows + r->m <= MAX_BATCH_ROWS || batch.empty();
             const bool fits_mem = sv->used + bytes + need <= sv->budget || (batch.empty() && !anything_inflight);
             if (!fits_rows || !fits_mem)

@@ -563,15 +563,17 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode()
     return fn;
 }
 
-int sm_count()
+int sm_count() { return device_sm_count(); }
+
+}  // namespace
+
+int device_sm_count()
 {
     int dev = 0, n = 0;
     GPRAT_CUDA_CHECK(cudaGetDevice(&dev));
     GPRAT_CUDA_CHECK(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
     return n;
 }
-
-}  // namespace
 
 void tc_make_operand(TcOperand &op, const void *base, int rows, int cols, int64_t ld, TcKind kind)
 {
@@ -660,7 +662,11 @@ void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cud
     const int tiles_m = ceil_div(args.M, TM);
     const int tiles_n = ceil_div(args.N, TN);
     const int ntiles = args.lower ? tiles_m * (tiles_m + 1) / 2 : tiles_m * tiles_n;
-    const int grid = std::min(ntiles, sm_count());
+    int grid = std::min(ntiles, sm_count());
+    if (args.max_ctas > 0)
+    {
+        grid = std::min(grid, args.max_ctas);
+    }
     const bool timed = gemm_timing_enabled();
     if (timed)
     {

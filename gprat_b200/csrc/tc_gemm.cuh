@@ -49,6 +49,7 @@ struct TcGemmArgs
     double *rowsq;
     int64_t rowsq_half;  // >= M when rowsq is set
     DeviceStatus *status;  // receives the timeout flag if a bounded wait gives up
+    int max_ctas;          // persistent grid limit (0 = one CTA per SM); leaves SMs to concurrent streams
 };
 
 void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cudaStream_t s);

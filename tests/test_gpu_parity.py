@@ -116,7 +116,8 @@ def test_gradient_matches_central_differences(capi):
         assert abs(fd - g[q]) <= 1e-6 * max(1.0, abs(g[q]))
 
 
-@pytest.mark.parametrize("n,m,T,d", [(1000, 300, 100, 8), (2048, 512, 256, 8), (384, 100, 96, 3)])
+@pytest.mark.parametrize("n,m,T,d", [(1000, 300, 100, 8), (2048, 512, 256, 8), (384, 100, 96, 3),
+                                     (1000, 300, 100, 16), (1536, 257, 128, 40), (700, 130, 70, 100)])
 def test_against_numpy_oracle(capi, n, m, T, d):
     x, y, xt = O.synthetic(n, m, d)
     h = (1.3, 0.8, 0.05)
