@@ -36,17 +36,25 @@ namespace
 {
 
 constexpr int TM = 128;
-constexpr int TN = 128;
-constexpr int TILE_BYTES = 128 * 128;  // one 128-row x 128-byte operand tile
-constexpr int STAGE_BYTES = 2 * TILE_BYTES;
-constexpr int STAGES = 6;
+constexpr int TN = 128;                // N of the narrow tile (row sums of squares need N <= TN)
+constexpr int TILE_BYTES = 128 * 128;  // one 128-row x 128-byte operand tile (one TMA box)
 constexpr int NUM_THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
-constexpr int EPI_COLS = 64;     // columns per epilogue warp
 constexpr int EPI_WARPS = 8;
 constexpr int EPI_BUF_BYTES = 32 * 128;  // one 32 x 32 FP32 sub-tile (TMA box, 128-byte swizzle)
-constexpr int TMEM_COLS = 2 * TN;
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // bounded waits: 2 s
-constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + EPI_WARPS * EPI_BUF_BYTES + 256;
+
+// Tile shape: 128 x TNV (TNV = 128 or 256).  The wide tile halves the A
+// traffic per flop and lowers the shared-memory bandwidth the MMA and the
+// TMA fills need (operand reads + fills per flop: 3/4 of the narrow tile's).
+template <int TNV>
+struct TileCfg
+{
+    static constexpr int STAGE_BYTES = TILE_BYTES + (TNV / 128) * TILE_BYTES;  // A + B
+    static constexpr int STAGES = (TNV == 128) ? 6 : 4;
+    static constexpr int TMEM_COLS = 2 * TNV;  // two accumulators
+    static constexpr int EPI_COLS = TNV / 2;   // columns per epilogue warp
+    static constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + EPI_WARPS * EPI_BUF_BYTES + 256;
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -160,10 +168,10 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr)
 }
 
 // Instruction descriptor: D = F32, A/B format (1 = BF16, 2 = TF32), both
-// K-major, N = 128, M = 128.
-__host__ __device__ constexpr uint32_t make_idesc(uint32_t fmt)
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t make_idesc(uint32_t fmt, int n)
 {
-    return (1u << 4) | (fmt << 7) | (fmt << 10) | (static_cast<uint32_t>(TN >> 3) << 17) |
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
            (static_cast<uint32_t>(TM >> 4) << 24);
 }
 
@@ -214,10 +222,20 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v)
 
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// Tile t -> (m0, n0).  Lower mode (M == N): row tile i holds the column
+// tiles that reach the diagonal or below, (i * TM) / TNV + 1 of them.
+template <int TNV>
 __device__ __forceinline__ void tile_of(int t, bool lower, int tiles_n, int &m0, int &n0)
 {
-    if (lower)
+    if (!lower)
     {
+        m0 = (t / tiles_n) * TM;
+        n0 = (t % tiles_n) * TNV;
+        return;
+    }
+    if (TNV == TM)
+    {
+        // prefix(i) = i (i + 1) / 2
         int i = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
         while ((i + 1) * (i + 2) / 2 <= t)
         {
@@ -228,20 +246,41 @@ __device__ __forceinline__ void tile_of(int t, bool lower, int tiles_n, int &m0,
             --i;
         }
         m0 = i * TM;
-        n0 = (t - i * (i + 1) / 2) * TN;
+        n0 = (t - i * (i + 1) / 2) * TNV;
     }
     else
     {
-        m0 = (t / tiles_n) * TM;
-        n0 = (t % tiles_n) * TN;
+        // TNV = 2 TM: row tile i holds i / 2 + 1 column tiles;
+        // prefix(2a) = a (a + 1), prefix(2a + 1) = (a + 1)^2
+        auto prefix = [](int i)
+        {
+            const int a = i >> 1;
+            return (i & 1) ? (a + 1) * (a + 1) : a * (a + 1);
+        };
+        int i = static_cast<int>(2.0 * sqrt(static_cast<double>(t))) - 2;
+        i = i < 0 ? 0 : i;
+        while (prefix(i + 1) <= t)
+        {
+            ++i;
+        }
+        while (i > 0 && prefix(i) > t)
+        {
+            --i;
+        }
+        m0 = i * TM;
+        n0 = (t - prefix(i)) * TNV;
     }
 }
 
-template <int KIND>
+template <int KIND, int TNV>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const __grid_constant__ CUtensorMap tmC, TcGemmArgs p, int tiles_n, int ntiles)
 {
+    using Cfg = TileCfg<TNV>;
+    constexpr int STAGES = Cfg::STAGES;
+    constexpr int STAGE_BYTES = Cfg::STAGE_BYTES;
+    constexpr int EPI_COLS = Cfg::EPI_COLS;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t *tiles = smem;
@@ -257,7 +296,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     constexpr int KSTAGE = (KIND == static_cast<int>(TcKind::TF32)) ? 32 : 64;  // elements per 128 bytes
-    constexpr uint32_t IDESC = make_idesc(KIND == static_cast<int>(TcKind::TF32) ? 2u : 1u);
+    constexpr uint32_t IDESC = make_idesc(KIND == static_cast<int>(TcKind::TF32) ? 2u : 1u, TNV);
     const int kiters = p.K / KSTAGE;
 
     if (threadIdx.x == 0)
@@ -279,7 +318,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     if (warp == 0)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(TMEM_COLS));
+                     "r"(Cfg::TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     tc_fence_before();
@@ -300,7 +339,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             for (int t = blockIdx.x; ok && t < ntiles; t += gridDim.x)
             {
                 int m0, n0;
-                tile_of(t, p.lower, tiles_n, m0, n0);
+                tile_of<TNV>(t, p.lower, tiles_n, m0, n0);
                 for (int k = 0; k < kiters; ++k)
                 {
                     if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag))
@@ -311,7 +350,12 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     mbar_expect_tx(&full[s], STAGE_BYTES);
                     uint8_t *st = tiles + s * STAGE_BYTES;
                     tma_load_2d(st, &tmA, &full[s], p.a_col0 + k * KSTAGE, p.a_row0 + m0);
-                    tma_load_2d(st + TILE_BYTES, &tmB, &full[s], p.b_col0 + k * KSTAGE, p.b_row0 + n0);
+#pragma unroll
+                    for (int bh = 0; bh < TNV / 128; ++bh)
+                    {
+                        tma_load_2d(st + TILE_BYTES * (1 + bh), &tmB, &full[s], p.b_col0 + k * KSTAGE,
+                                    p.b_row0 + n0 + 128 * bh);
+                    }
                     if (++s == STAGES)
                     {
                         s = 0;
@@ -347,7 +391,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     break;
                 }
                 tc_fence_after();
-                const uint32_t d = tmem_base + static_cast<uint32_t>(b * TN);
+                const uint32_t d = tmem_base + static_cast<uint32_t>(b * TNV);
                 for (int k = 0; k < kiters; ++k)
                 {
                     if (!mbar_wait(&full[s], ph, abort_flag))
@@ -387,7 +431,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     else
     {
         // ---------------- epilogue (warps 2..9) ----------------
-        // two warps per TMEM lane quarter, each owning 64 of the 128 columns
+        // two warps per TMEM lane quarter, each owning half of the TNV columns,
+        // read from TMEM and written out 32 columns at a time
         const int ew = warp - 2;
         const int q = warp & 3;  // TMEM lane quarter this warp may access
         const int h = ew >> 2;   // column half
@@ -400,33 +445,31 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         {
             const int b = it & 1;
             int m0, n0;
-            tile_of(t, p.lower, tiles_n, m0, n0);
+            tile_of<TNV>(t, p.lower, tiles_n, m0, n0);
             if (!mbar_wait(&tfull[b], (acc_bits >> b) & 1u, abort_flag))
             {
                 break;
             }
             tc_fence_after();
-            float v[EPI_COLS];
             const uint32_t taddr = tmem_base + (static_cast<uint32_t>(q * 32) << 16) +
-                                   static_cast<uint32_t>(b * TN + h * EPI_COLS);
-#pragma unroll
-            for (int c = 0; c < EPI_COLS / 32; ++c)
-            {
-                tmem_ld32(taddr + c * 32, v + c * 32);
-            }
-            tmem_ld_wait();
-            tc_fence_before();
-            mbar_arrive(&tempty[b]);
-            acc_bits ^= 1u << b;
-
+                                   static_cast<uint32_t>(b * TNV + h * EPI_COLS);
             const int row = m0 + r_in;
             const int row0 = m0 + q * 32;  // first row of this warp's sub-tiles
-            const bool diag = p.lower && m0 == n0;
+            const bool diag = p.lower && n0 + TNV > m0;  // tile reaches above the diagonal
             double sq = 0.0;
-#pragma unroll
+#pragma unroll 1
             for (int c = 0; c < EPI_COLS / 32; ++c)
             {
                 const int col0 = n0 + h * EPI_COLS + c * 32;
+                float v[32];
+                tmem_ld32(taddr + c * 32, v);
+                tmem_ld_wait();
+                if (c == EPI_COLS / 32 - 1)
+                {
+                    // the whole accumulator has been read: release it to the MMA warp
+                    tc_fence_before();
+                    mbar_arrive(&tempty[b]);
+                }
                 // warp-uniform: sub-tile outside C, or entirely above the diagonal
                 if (col0 >= p.N || (diag && col0 >= row0 + 32))
                 {
@@ -436,7 +479,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 #pragma unroll
                 for (int j = 0; j < 32; ++j)
                 {
-                    float val = p.alpha * v[c * 32 + j];
+                    float val = p.alpha * v[j];
                     if (diag && col0 + j > row)
                     {
                         val = 0.0f;
@@ -476,6 +519,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     bulk_commit();
                 }
             }
+            acc_bits ^= 1u << b;
             if (p.rowsq != nullptr && row < p.M)
             {
                 p.rowsq[h * p.rowsq_half + row] += sq;  // single writer per word and launch
@@ -494,7 +538,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     {
         __syncwarp();
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(Cfg::TMEM_COLS));
     }
     if (threadIdx.x == 0 && *abort_flag && p.status != nullptr)
     {
@@ -659,9 +703,26 @@ void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cud
             throw Error(4, "cuTensorMapEncodeTiled (C) failed with code " + std::to_string(static_cast<int>(r)));
         }
     }
+    // wide tiles for wide updates; the narrow tile for N < 512 (a 256-wide tile
+    // would waste up to half its columns there) and for row sums of squares
+    const bool wide = args.N >= 512 && args.rowsq == nullptr;
+    const int tnv = wide ? 256 : 128;
     const int tiles_m = ceil_div(args.M, TM);
-    const int tiles_n = ceil_div(args.N, TN);
-    const int ntiles = args.lower ? tiles_m * (tiles_m + 1) / 2 : tiles_m * tiles_n;
+    const int tiles_n = ceil_div(args.N, tnv);
+    int ntiles;
+    if (!args.lower)
+    {
+        ntiles = tiles_m * tiles_n;
+    }
+    else if (!wide)
+    {
+        ntiles = tiles_m * (tiles_m + 1) / 2;
+    }
+    else
+    {
+        const int a = tiles_m >> 1;
+        ntiles = (tiles_m & 1) ? (a + 1) * (a + 1) : a * (a + 1);
+    }
     int grid = std::min(ntiles, sm_count());
     if (args.max_ctas > 0)
     {
@@ -672,15 +733,32 @@ void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cud
     {
         gemm_timing_begin(s);
     }
+    auto run = [&](auto kernel, int smem)
+    {
+        ensure_smem_attr(reinterpret_cast<const void *>(kernel), smem);
+        kernel<<<grid, NUM_THREADS, smem, s>>>(A.map, B.map, tmC, args, tiles_n, ntiles);
+    };
     if (A.kind == TcKind::TF32)
     {
-        ensure_smem_attr(reinterpret_cast<const void *>(tc_gemm_kernel<0>), SMEM_BYTES);
-        tc_gemm_kernel<0><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(A.map, B.map, tmC, args, tiles_n, ntiles);
+        if (wide)
+        {
+            run(tc_gemm_kernel<0, 256>, TileCfg<256>::SMEM_BYTES);
+        }
+        else
+        {
+            run(tc_gemm_kernel<0, 128>, TileCfg<128>::SMEM_BYTES);
+        }
     }
     else
     {
-        ensure_smem_attr(reinterpret_cast<const void *>(tc_gemm_kernel<1>), SMEM_BYTES);
-        tc_gemm_kernel<1><<<grid, NUM_THREADS, SMEM_BYTES, s>>>(A.map, B.map, tmC, args, tiles_n, ntiles);
+        if (wide)
+        {
+            run(tc_gemm_kernel<1, 256>, TileCfg<256>::SMEM_BYTES);
+        }
+        else
+        {
+            run(tc_gemm_kernel<1, 128>, TileCfg<128>::SMEM_BYTES);
+        }
     }
     GPRAT_LAUNCH_CHECK();
     if (timed)

@@ -11,6 +11,11 @@ has the reference tree and the compiled reference, oracle/_ref):
    oracle/_ref) on seeded synthetic inputs: a 1024-point case with 64-wide
    tiles, a ragged test set, a 64-regressor case, and 5 Adam steps with the
    gradient at every step.
+3. c3_optimize.npz (`--c3`, several minutes): the hyper-parameter
+   optimisation configuration, n_train = 8192, d = 8, 16 x 16 tiles of 512,
+   initial (lengthscale, vertical_lengthscale, noise) = (0.5, 2.0, 0.5),
+   50 Adam steps at lr = 0.1: the reference's loss and parameters after every
+   step and its gradient at steps 0, 10, 20, 30, 40.
 """
 from __future__ import annotations
 
@@ -86,8 +91,29 @@ def case_optimize(store):
     })
 
 
+def case_c3():
+    n, d, T, steps = 8192, 8, 512, 50
+    adam = (0.1, 0.9, 0.999, 1e-8)
+    x, y, _ = O.synthetic(n, 16, d)
+    gp = ref.RefGP(x, y, n // T, T, d, (0.5, 2.0, 0.5))
+    checkpoints = [0, 10, 20, 30, 40]
+    losses, params, grads = [], [], []
+    for it in range(steps):
+        if it in checkpoints:
+            grads.append(gp.gradient(*adam))
+        losses.append(gp.optimize_step(it, *adam))
+        params.append(gp.get_params())
+        print(f"c3 step {it}: loss {losses[-1]:.12f}", flush=True)
+    np.savez_compressed(os.path.join(HERE, "c3_optimize.npz"), cfg=np.array([n, d, T, steps], dtype=np.int64),
+                        adam=np.array(adam), checkpoints=np.array(checkpoints, dtype=np.int64),
+                        losses=np.array(losses), params=np.array(params), grads=np.array(grads))
+
+
 def main():
     ref.start()
+    if "--c3" in sys.argv:
+        case_c3()
+        return
     known_answer()
     store = {}
     case_predict("c0", 1024, 1024, 8, 64, (1.0, 1.0, 0.1), store)

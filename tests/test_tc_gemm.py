@@ -79,3 +79,11 @@ def test_reduce_add_ragged_edges(capi, kind):
 @pytest.mark.parametrize("kind", [0, 1])
 def test_lower_triangle_ragged(capi, kind):
     run_case(capi, kind, 300, 300, 128, -1.0, 1.0, lower=True, seed=7)
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_wide_tiles(capi, kind):
+    # N >= 512 runs the 128 x 256 tile: ragged edges, lower mode, both betas
+    run_case(capi, kind, 700, 600, 128, 1.0, 0.0, seed=8)
+    run_case(capi, kind, 1000, 1000, 192, -1.0, 1.0, lower=True, seed=9)
+    run_case(capi, kind, 1536, 1536, 256, -1.0, 1.0, lower=True, seed=10)
