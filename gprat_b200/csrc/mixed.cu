@@ -324,8 +324,13 @@ void precondition(gprat_cu_gp *gp, const double *r, double *z, cudaStream_t s)
 namespace
 {
 
-constexpr int SIDE_SMS = 16;         // SMs kept free for the look-ahead stream next to a large update
-constexpr int LARGE_UPDATE = 16384;  // trailing-update size above which the look-ahead stream is limited
+// Share of the SMs the main stream's trailing update may hold while the
+// look-ahead stream works next to it (persistent CTAs never yield their SM,
+// so the side stream, which carries the critical path, needs SMs left free).
+#ifndef GPRAT_LOOKAHEAD_MAIN_PERCENT
+#define GPRAT_LOOKAHEAD_MAIN_PERCENT 70
+#endif
+constexpr int MAIN_PERCENT = GPRAT_LOOKAHEAD_MAIN_PERCENT;
 
 void ensure_lookahead(gprat_cu_gp *gp, int nevents)
 {
@@ -357,8 +362,8 @@ TcGemmArgs limited(TcGemmArgs a, int max_ctas)
 //     panel solves and the in-panel updates on tcgen05), then apply panel k
 //     to the columns of panel k+1 and factor panel k+1;
 //   main stream: the trailing update of everything right of panel k+1 with
-//     panel k (the bulk of the flops), on all but SIDE_SMS SMs while the side
-//     stream works next to it.
+//     panel k (the bulk of the flops), on MAIN_PERCENT % of the SMs while the
+//     side stream works next to it (the panel chain is the critical path).
 // Events order the two streams: panel k+1's columns are written by the
 // update of panel k-1 (main) before the side stream touches them, and the
 // update of panel k waits for panel k's factorisation.
@@ -449,7 +454,6 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
         const int next_end = std::min(pend + NBO, n);  // end of panel k+1
         const int rest = n - next_end;
         const bool ahead = k + 1 < nout;
-        const bool large = rest >= LARGE_UPDATE;
         // main: everything right of panel k+1, with panel k
         GPRAT_CUDA_CHECK(cudaStreamWaitEvent(s, evF(k), 0));
         if (rest > 0)
@@ -457,7 +461,7 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
             tc_gemm(ops.trail(), ops.trail(),
                     limited(tc_args(rest, rest, bo, next_end, K0, next_end, K0, at(next_end, next_end), ld32, -1.0f,
                                     1.0f, true, nullptr, gp->status.ptr),
-                            ahead ? sms - SIDE_SMS : 0),
+                            ahead ? std::max(1, sms * MAIN_PERCENT / 100) : 0),
                     s);
         }
         GPRAT_CUDA_CHECK(cudaEventRecord(evR(k), s));
@@ -466,7 +470,7 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
             break;
         }
         // side: panel k applied to panel k+1's columns, then panel k+1 factored
-        const int side_ctas = large ? SIDE_SMS : 0;
+        const int side_ctas = 0;  // the critical path takes every SM it can get
         if (k >= 1)
         {
             GPRAT_CUDA_CHECK(cudaStreamWaitEvent(side, evR(k - 1), 0));

@@ -457,19 +457,21 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             const int row0 = m0 + q * 32;  // first row of this warp's sub-tiles
             const bool diag = p.lower && n0 + TNV > m0;  // tile reaches above the diagonal
             double sq = 0.0;
-#pragma unroll 1
+            // the whole accumulator slice into registers first, then release it
+            // to the MMA warp before any shared-memory or TMA work
+            float v[EPI_COLS];
+#pragma unroll
+            for (int c = 0; c < EPI_COLS / 32; ++c)
+            {
+                tmem_ld32(taddr + c * 32, v + c * 32);
+            }
+            tmem_ld_wait();
+            tc_fence_before();
+            mbar_arrive(&tempty[b]);
+#pragma unroll
             for (int c = 0; c < EPI_COLS / 32; ++c)
             {
                 const int col0 = n0 + h * EPI_COLS + c * 32;
-                float v[32];
-                tmem_ld32(taddr + c * 32, v);
-                tmem_ld_wait();
-                if (c == EPI_COLS / 32 - 1)
-                {
-                    // the whole accumulator has been read: release it to the MMA warp
-                    tc_fence_before();
-                    mbar_arrive(&tempty[b]);
-                }
                 // warp-uniform: sub-tile outside C, or entirely above the diagonal
                 if (col0 >= p.N || (diag && col0 >= row0 + 32))
                 {
@@ -479,7 +481,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 #pragma unroll
                 for (int j = 0; j < 32; ++j)
                 {
-                    float val = p.alpha * v[j];
+                    float val = p.alpha * v[c * 32 + j];
                     if (diag && col0 + j > row)
                     {
                         val = 0.0f;
