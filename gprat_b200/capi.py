@@ -74,7 +74,8 @@ def _load() -> ctypes.CDLL:
     lib.gprat_cu_stats_read.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _dp, _dp]
     _fp = ctypes.POINTER(ctypes.c_float)
     lib.gprat_cu_test_tc_gemm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _fp, _i64, _fp,
-                                          _i64, _fp, _i64, ctypes.c_float, ctypes.c_float, ctypes.c_int, _dp]
+                                          _i64, _fp, _i64, ctypes.c_float, ctypes.c_float, ctypes.c_int, _dp,
+                                          ctypes.c_int]
     _vp, _i64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)
     lib.gprat_cu_server_create.argtypes = [ctypes.c_int, _i64, ctypes.c_int, ctypes.POINTER(_vp)]
     lib.gprat_cu_server_destroy.argtypes = [_vp]
@@ -130,9 +131,10 @@ def stats_read() -> dict:
 
 
 def test_tc_gemm(kind: int, A: np.ndarray, B: np.ndarray, C: np.ndarray, alpha: float, beta: float,
-                 lower: bool = False, rowsq: Optional[np.ndarray] = None) -> None:
+                 lower: bool = False, rowsq: Optional[np.ndarray] = None, tile_mode: int = 0) -> None:
     """Runs the tcgen05 GEMM C = beta*C + alpha*A B^T in place on float32 arrays
-    (kind 0 = TF32, 1 = BF16)."""
+    (kind 0 = TF32, 1 = BF16; tile_mode 0 = automatic, 1 = 128x128, 2 = 128x256,
+    3 = 256x256 on a CTA pair)."""
     _fp = ctypes.POINTER(ctypes.c_float)
     for a in (A, B, C):
         if a.dtype != np.float32 or not a.flags.c_contiguous:
@@ -142,7 +144,7 @@ def test_tc_gemm(kind: int, A: np.ndarray, B: np.ndarray, C: np.ndarray, alpha: 
     rp = rowsq.ctypes.data_as(_dp) if rowsq is not None else None
     check(lib.gprat_cu_test_tc_gemm(int(kind), M, N, K, A.ctypes.data_as(_fp), K, B.ctypes.data_as(_fp), K,
                                     C.ctypes.data_as(_fp), C.shape[1], float(alpha), float(beta), int(bool(lower)),
-                                    rp))
+                                    rp, int(tile_mode)))
 
 
 def _arr(a) -> np.ndarray:

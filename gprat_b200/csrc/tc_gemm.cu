@@ -548,6 +548,385 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     }
 }
 
+// ---------------------------------------------------------------------------
+// CTA-pair variant: a cluster of two CTAs computes one 256 x 256 tile with
+// tcgen05.mma.cta_group::2 (M = 256 across the pair, N = 256).  Each CTA loads
+// its own 128 rows of A and its own 128 rows of B (plain TMA loads, no
+// multicast; the transaction bytes of both CTAs complete the leader's stage
+// barrier); the leader's single MMA thread reads A from each CTA's shared
+// memory for that CTA's rows and B from both, and accumulates each CTA's 128 x
+// 256 half in that CTA's TMEM.  Per SM this moves 32 KB of operands per
+// 128 x 256 x 32 step instead of 48 KB for the single-CTA 128 x 256 tile.
+//   leader (rank 0): TMA warp (its halves + expect_tx for both), MMA warp,
+//                    8 epilogue warps for rows m0 .. m0+127
+//   peer   (rank 1): TMA warp (its halves), 8 epilogue warps for rows m0+128 ..
+// Stage barriers: full[s] (leader; both CTAs' TMA bytes), empty[s] (both;
+// the leader's commit arrives on both), tfull[b] (both; multicast commit),
+// tempty[b] (leader; one arrival per epilogue warp of either CTA).
+constexpr int PAIR_STAGE_BYTES = 2 * TILE_BYTES;  // per CTA: A half + B half
+constexpr int PAIR_STAGES = 6;
+constexpr int PAIR_TN = 256;
+constexpr int PAIR_TMEM_COLS = 2 * PAIR_TN;
+constexpr int PAIR_SMEM_BYTES = 1024 + PAIR_STAGES * PAIR_STAGE_BYTES + EPI_WARPS * EPI_BUF_BYTES + 256;
+
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// shared::cluster address of the same shared variable in CTA `rank`
+__device__ __forceinline__ uint32_t map_to_rank(const void *p, uint32_t rank)
+{
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(smem_u32(p)), "r"(rank));
+    return out;
+}
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d_pair(void *dst, const CUtensorMap *map, uint32_t leader_bar, int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(leader_bar), "r"(x), "r"(y)
+        : "memory");
+}
+
+template <int KIND>
+__device__ __forceinline__ void mma_issue_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                               uint32_t accumulate)
+{
+    if (KIND == static_cast<int>(TcKind::TF32))
+    {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+    }
+    else
+    {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+    }
+}
+
+// arrives on the barrier at the same offset in both CTAs of the pair
+__device__ __forceinline__ void mma_commit_pair_both(uint64_t *bar)
+{
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"(static_cast<uint16_t>(3))
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit_pair_local(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// pair tile t -> (m0, n0) in units of 256 (lower: square tiles at or below the diagonal)
+__device__ __forceinline__ void pair_tile_of(int t, bool lower, int tiles_n, int &m0, int &n0)
+{
+    if (!lower)
+    {
+        m0 = (t / tiles_n) * 256;
+        n0 = (t % tiles_n) * 256;
+        return;
+    }
+    int i = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while ((i + 1) * (i + 2) / 2 <= t)
+    {
+        ++i;
+    }
+    while (i > 0 && i * (i + 1) / 2 > t)
+    {
+        --i;
+    }
+    m0 = i * 256;
+    n0 = (t - i * (i + 1) / 2) * 256;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+    tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                        const __grid_constant__ CUtensorMap tmC, TcGemmArgs p, int tiles_n, int ntiles)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t *tiles = smem;
+    uint8_t *epi_smem = smem + PAIR_STAGES * PAIR_STAGE_BYTES;
+    uint64_t *full = reinterpret_cast<uint64_t *>(epi_smem + EPI_WARPS * EPI_BUF_BYTES);
+    uint64_t *empty = full + PAIR_STAGES;
+    uint64_t *tfull = empty + PAIR_STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint64_t *drain = tempty + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const int pair = blockIdx.x >> 1;
+    const int npairs = gridDim.x >> 1;
+    constexpr int KSTAGE = (KIND == static_cast<int>(TcKind::TF32)) ? 32 : 64;
+    constexpr uint32_t IDESC = (1u << 4) | ((KIND == static_cast<int>(TcKind::TF32) ? 2u : 1u) << 7) |
+                               ((KIND == static_cast<int>(TcKind::TF32) ? 2u : 1u) << 10) |
+                               (static_cast<uint32_t>(PAIR_TN >> 3) << 17) | (static_cast<uint32_t>(256 >> 4) << 24);
+    const int kiters = p.K / KSTAGE;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < PAIR_STAGES; ++s)
+        {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b)
+        {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 2 * EPI_WARPS);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(PAIR_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::);
+    }
+    tc_fence_before();
+    cluster_sync_all();  // barriers of both CTAs initialised, TMEM allocated
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            // ---------------- TMA producer (both CTAs) ----------------
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+            int s = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            for (int t = pair; ok && t < ntiles; t += npairs)
+            {
+                int m0, n0;
+                pair_tile_of(t, p.lower, tiles_n, m0, n0);
+                const int arow = p.a_row0 + m0 + 128 * static_cast<int>(rank);
+                const int brow = p.b_row0 + n0 + 128 * static_cast<int>(rank);
+                for (int k = 0; k < kiters; ++k)
+                {
+                    if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    if (leader)
+                    {
+                        mbar_expect_tx(&full[s], 2 * PAIR_STAGE_BYTES);  // both CTAs' bytes
+                    }
+                    const uint32_t bar = map_to_rank(&full[s], 0);
+                    uint8_t *st = tiles + s * PAIR_STAGE_BYTES;
+                    tma_load_2d_pair(st, &tmA, bar, p.a_col0 + k * KSTAGE, arow);
+                    tma_load_2d_pair(st + TILE_BYTES, &tmB, bar, p.b_col0 + k * KSTAGE, brow);
+                    if (++s == PAIR_STAGES)
+                    {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+            if (*abort_flag)
+            {
+                const unsigned long long t0 = global_ns();
+                while (global_ns() - t0 < 200000ull)
+                {
+                }
+            }
+        }
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0 && leader)
+        {
+            // ---------------- MMA issuer (leader only) ----------------
+            int s = 0;
+            uint32_t ph = 0;
+            uint32_t acc_bits = 0u;
+            bool ok = true;
+            int it = 0;
+            for (int t = pair; ok && t < ntiles; t += npairs, ++it)
+            {
+                const int b = it & 1;
+                if (!mbar_wait(&tempty[b], ((acc_bits >> b) & 1u) ^ 1u, abort_flag))
+                {
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem_base + static_cast<uint32_t>(b * PAIR_TN);
+                for (int k = 0; k < kiters; ++k)
+                {
+                    if (!mbar_wait(&full[s], ph, abort_flag))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_addr = smem_u32(tiles + s * PAIR_STAGE_BYTES);
+                    const uint64_t adesc = sw128_desc(a_addr);
+                    const uint64_t bdesc = sw128_desc(a_addr + TILE_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk)
+                    {
+                        mma_issue_pair<KIND>(d, adesc + 2 * kk, bdesc + 2 * kk, IDESC, (k | kk) != 0 ? 1u : 0u);
+                    }
+                    mma_commit_pair_both(&empty[s]);
+                    if (++s == PAIR_STAGES)
+                    {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (!ok)
+                {
+                    break;
+                }
+                mma_commit_pair_both(&tfull[b]);
+                acc_bits ^= 1u << b;
+            }
+            mma_commit_pair_local(drain);
+            mbar_wait(drain, 0u, abort_flag);
+        }
+    }
+    else
+    {
+        // ---------------- epilogue (warps 2..9 of both CTAs) ----------------
+        constexpr int EPI_COLS = PAIR_TN / 2;
+        const int ew = warp - 2;
+        const int q = warp & 3;
+        const int h = ew >> 2;
+        uint8_t *buf = epi_smem + ew * EPI_BUF_BYTES;
+        const uint32_t buf_row = smem_u32(buf) + static_cast<uint32_t>(lane) * 128u;
+        uint32_t acc_bits = 0u;
+        int it = 0;
+        for (int t = pair; t < ntiles; t += npairs, ++it)
+        {
+            const int b = it & 1;
+            int mp, n0;
+            pair_tile_of(t, p.lower, tiles_n, mp, n0);
+            const int m0 = mp + 128 * static_cast<int>(rank);  // this CTA's rows
+            if (!mbar_wait(&tfull[b], (acc_bits >> b) & 1u, abort_flag))
+            {
+                break;
+            }
+            tc_fence_after();
+            const uint32_t taddr = tmem_base + (static_cast<uint32_t>(q * 32) << 16) +
+                                   static_cast<uint32_t>(b * PAIR_TN + h * EPI_COLS);
+            float v[EPI_COLS];
+#pragma unroll
+            for (int c = 0; c < EPI_COLS / 32; ++c)
+            {
+                tmem_ld32(taddr + c * 32, v + c * 32);
+            }
+            tmem_ld_wait();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0)
+            {
+                mbar_arrive_cluster(map_to_rank(&tempty[b], 0));
+            }
+            acc_bits ^= 1u << b;
+            const int row = m0 + q * 32 + lane;
+            const int row0 = m0 + q * 32;
+            const bool diag = p.lower && n0 + PAIR_TN > m0;
+#pragma unroll
+            for (int c = 0; c < EPI_COLS / 32; ++c)
+            {
+                const int col0 = n0 + h * EPI_COLS + c * 32;
+                if (col0 >= p.N || row0 >= p.M || (diag && col0 >= row0 + 32))
+                {
+                    continue;
+                }
+                float w[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                {
+                    float val = p.alpha * v[c * 32 + j];
+                    if (diag && col0 + j > row)
+                    {
+                        val = 0.0f;
+                    }
+                    w[j] = val;
+                }
+                if (lane == 0)
+                {
+                    bulk_wait_read_all();
+                }
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                {
+                    const uint32_t addr = buf_row + (static_cast<uint32_t>(j ^ (lane & 7)) << 4);
+                    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(w[4 * j]),
+                                 "f"(w[4 * j + 1]), "f"(w[4 * j + 2]), "f"(w[4 * j + 3])
+                                 : "memory");
+                }
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0)
+                {
+                    if (p.beta != 0.0f)
+                    {
+                        tma_reduce_add_2d(&tmC, buf, col0, row0);
+                    }
+                    else
+                    {
+                        tma_store_2d(&tmC, buf, col0, row0);
+                    }
+                    bulk_commit();
+                }
+            }
+        }
+        if (lane == 0)
+        {
+            bulk_wait_all();
+        }
+        __syncwarp();
+    }
+
+    tc_fence_before();
+    cluster_sync_all();  // no CTA leaves while its peer may still signal or read it
+    if (warp == 0)
+    {
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(PAIR_TMEM_COLS));
+    }
+    if (threadIdx.x == 0 && *abort_flag && p.status != nullptr)
+    {
+        atomicExch(&p.status->timeout, 1);
+    }
+}
+
 template <typename T>
 __global__ void convert_kernel(const T *__restrict__ src, int64_t lds, void *__restrict__ dst, int64_t ldd, int rows,
                                int cols, int mode)
@@ -705,61 +1084,112 @@ void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cud
             throw Error(4, "cuTensorMapEncodeTiled (C) failed with code " + std::to_string(static_cast<int>(r)));
         }
     }
-    // wide tiles for wide updates; the narrow tile for N < 512 (a 256-wide tile
-    // would waste up to half its columns there) and for row sums of squares
-    const bool wide = args.N >= 512 && args.rowsq == nullptr;
-    const int tnv = wide ? 256 : 128;
-    const int tiles_m = ceil_div(args.M, TM);
-    const int tiles_n = ceil_div(args.N, tnv);
-    int ntiles;
-    if (!args.lower)
+    // Tile choice: a CTA pair (256 x 256) for large updates, 128 x 256 for wide
+    // ones, 128 x 128 for N < 512 (a 256-wide tile would waste up to half its
+    // columns there) and for row sums of squares.
+    int mode = args.tile_mode;
+    if (mode == 0)
     {
-        ntiles = tiles_m * tiles_n;
+        mode = (args.rowsq != nullptr || args.N < 512) ? 1 : (args.M >= 1024 ? 3 : 2);
     }
-    else if (!wide)
+    if (mode != 1 && args.rowsq != nullptr)
     {
-        ntiles = tiles_m * (tiles_m + 1) / 2;
+        throw Error(1, "tc_gemm: row sums of squares need the 128 x 128 tile");
     }
-    else
-    {
-        const int a = tiles_m >> 1;
-        ntiles = (tiles_m & 1) ? (a + 1) * (a + 1) : a * (a + 1);
-    }
-    int grid = std::min(ntiles, sm_count());
-    if (args.max_ctas > 0)
-    {
-        grid = std::min(grid, args.max_ctas);
-    }
+    const int sms = sm_count();
     const bool timed = gemm_timing_enabled();
-    if (timed)
+    if (mode == 3)
     {
-        gemm_timing_begin(s);
-    }
-    auto run = [&](auto kernel, int smem)
-    {
-        ensure_smem_attr(reinterpret_cast<const void *>(kernel), smem);
-        kernel<<<grid, NUM_THREADS, smem, s>>>(A.map, B.map, tmC, args, tiles_n, ntiles);
-    };
-    if (A.kind == TcKind::TF32)
-    {
-        if (wide)
+        const int tiles_m = ceil_div(args.M, 256);
+        const int tiles_n = ceil_div(args.N, 256);
+        const int ntiles = args.lower ? tiles_m * (tiles_m + 1) / 2 : tiles_m * tiles_n;
+        int npairs = std::min(ntiles, sms / 2);
+        if (args.max_ctas > 0)
         {
-            run(tc_gemm_kernel<0, 256>, TileCfg<256>::SMEM_BYTES);
+            npairs = std::min(npairs, std::max(1, args.max_ctas / 2));
+        }
+        if (timed)
+        {
+            gemm_timing_begin(s);
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2 * npairs);
+        cfg.blockDim = dim3(NUM_THREADS);
+        cfg.dynamicSmemBytes = PAIR_SMEM_BYTES;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        if (A.kind == TcKind::TF32)
+        {
+            ensure_smem_attr(reinterpret_cast<const void *>(tc_gemm_pair_kernel<0>), PAIR_SMEM_BYTES);
+            GPRAT_CUDA_CHECK(cudaLaunchKernelEx(&cfg, tc_gemm_pair_kernel<0>, A.map, B.map, tmC, args, tiles_n, ntiles));
         }
         else
         {
-            run(tc_gemm_kernel<0, 128>, TileCfg<128>::SMEM_BYTES);
+            ensure_smem_attr(reinterpret_cast<const void *>(tc_gemm_pair_kernel<1>), PAIR_SMEM_BYTES);
+            GPRAT_CUDA_CHECK(cudaLaunchKernelEx(&cfg, tc_gemm_pair_kernel<1>, A.map, B.map, tmC, args, tiles_n, ntiles));
         }
     }
     else
     {
-        if (wide)
+        const bool wide = mode == 2;
+        const int tnv = wide ? 256 : 128;
+        const int tiles_m = ceil_div(args.M, TM);
+        const int tiles_n = ceil_div(args.N, tnv);
+        int ntiles;
+        if (!args.lower)
         {
-            run(tc_gemm_kernel<1, 256>, TileCfg<256>::SMEM_BYTES);
+            ntiles = tiles_m * tiles_n;
+        }
+        else if (!wide)
+        {
+            ntiles = tiles_m * (tiles_m + 1) / 2;
         }
         else
         {
-            run(tc_gemm_kernel<1, 128>, TileCfg<128>::SMEM_BYTES);
+            const int a = tiles_m >> 1;
+            ntiles = (tiles_m & 1) ? (a + 1) * (a + 1) : a * (a + 1);
+        }
+        int grid = std::min(ntiles, sms);
+        if (args.max_ctas > 0)
+        {
+            grid = std::min(grid, args.max_ctas);
+        }
+        if (timed)
+        {
+            gemm_timing_begin(s);
+        }
+        auto run = [&](auto kernel, int smem)
+        {
+            ensure_smem_attr(reinterpret_cast<const void *>(kernel), smem);
+            kernel<<<grid, NUM_THREADS, smem, s>>>(A.map, B.map, tmC, args, tiles_n, ntiles);
+        };
+        if (A.kind == TcKind::TF32)
+        {
+            if (wide)
+            {
+                run(tc_gemm_kernel<0, 256>, TileCfg<256>::SMEM_BYTES);
+            }
+            else
+            {
+                run(tc_gemm_kernel<0, 128>, TileCfg<128>::SMEM_BYTES);
+            }
+        }
+        else
+        {
+            if (wide)
+            {
+                run(tc_gemm_kernel<1, 256>, TileCfg<256>::SMEM_BYTES);
+            }
+            else
+            {
+                run(tc_gemm_kernel<1, 128>, TileCfg<128>::SMEM_BYTES);
+            }
         }
     }
     GPRAT_LAUNCH_CHECK();

@@ -50,6 +50,7 @@ struct TcGemmArgs
     int64_t rowsq_half;  // >= M when rowsq is set
     DeviceStatus *status;  // receives the timeout flag if a bounded wait gives up
     int max_ctas;          // persistent grid limit (0 = one CTA per SM); leaves SMs to concurrent streams
+    int tile_mode;         // 0 = automatic; 1 = 128 x 128, 2 = 128 x 256, 3 = 256 x 256 on a CTA pair (tests)
 };
 
 void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cudaStream_t s);

@@ -38,12 +38,12 @@ struct Buf
 
 extern "C" int gprat_cu_test_tc_gemm(int kind, int M, int N, int K, const float *A, int64_t lda, const float *B,
                                      int64_t ldb, float *C, int64_t ldc, float alpha, float beta, int lower,
-                                     double *rowsq)
+                                     double *rowsq, int tile_mode)
 {
     try
     {
         if (A == nullptr || B == nullptr || C == nullptr || M <= 0 || N <= 0 || K <= 0 || lda < K || ldb < K ||
-            ldc < N || (kind != 0 && kind != 1))
+            ldc < N || (kind != 0 && kind != 1) || tile_mode < 0 || tile_mode > 3)
         {
             throw Error(GPRAT_CU_ERR_INVALID_ARG, "gprat_cu_test_tc_gemm: invalid arguments");
         }
@@ -88,6 +88,7 @@ extern "C" int gprat_cu_test_tc_gemm(int kind, int M, int N, int K, const float 
         g.lower = lower != 0;
         g.rowsq = rowsq != nullptr ? static_cast<double *>(dRow.p) : nullptr;
         g.rowsq_half = M;
+        g.tile_mode = tile_mode;
         g.status = static_cast<DeviceStatus *>(dStatus.p);
         tc_gemm(oa, ob, g, s);
         GPRAT_CUDA_CHECK(cudaStreamSynchronize(s));

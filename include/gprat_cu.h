@@ -244,7 +244,9 @@ int gprat_cu_stats_read(int64_t *launches, int64_t *gemm_launches, double *gemm_
  * B (N x K, ldb), C (M x N, ldc; read when beta = 1, written back).
  * kind 0 = TF32 operands, 1 = BF16 operands (rounded from the FP32 input).
  * lower != 0: M == N and only C[i][j], i >= j, is written.  rowsq (optional,
- * N <= 128): rowsq[i] += sum_j C_new[i][j]^2.  K must be a multiple of 64.
+ * N <= 128, beta = 0): rowsq[i] += sum_j C_new[i][j]^2.  K must be a multiple
+ * of 64.  tile_mode: 0 = the library's choice, 1 = 128 x 128 tiles,
+ * 2 = 128 x 256 tiles, 3 = 256 x 256 tiles on a pair of CTAs.
  */
 int gprat_cu_test_tc_gemm(int kind,
                           int M,
@@ -259,7 +261,8 @@ int gprat_cu_test_tc_gemm(int kind,
                           float alpha,
                           float beta,
                           int lower,
-                          double *rowsq);
+                          double *rowsq,
+                          int tile_mode);
 
 /*
  * Serving (no counterpart in the reference, whose every predict call

@@ -18,14 +18,14 @@ def capi():
     return c
 
 
-def run_case(capi, kind, M, N, K, alpha, beta, lower=False, seed=0, with_rowsq=False):
+def run_case(capi, kind, M, N, K, alpha, beta, lower=False, seed=0, with_rowsq=False, tile_mode=0):
     rng = np.random.default_rng(seed)
     A = rng.standard_normal((M, K)).astype(np.float32)
     B = A.copy() if lower else rng.standard_normal((N, K)).astype(np.float32)
     C0 = rng.standard_normal((M, N)).astype(np.float32)
     C = C0.copy()
     rowsq = np.zeros(M) if with_rowsq else None
-    capi.test_tc_gemm(kind, A, B, C, alpha, beta, lower, rowsq)
+    capi.test_tc_gemm(kind, A, B, C, alpha, beta, lower, rowsq, tile_mode)
     prod = A.astype(np.float64) @ B.astype(np.float64).T
     want = beta * C0.astype(np.float64) + alpha * prod
     scale = np.abs(A).astype(np.float64) @ np.abs(B).astype(np.float64).T + np.abs(C0) * beta + 1e-30
@@ -87,3 +87,13 @@ def test_wide_tiles(capi, kind):
     run_case(capi, kind, 700, 600, 128, 1.0, 0.0, seed=8)
     run_case(capi, kind, 1000, 1000, 192, -1.0, 1.0, lower=True, seed=9)
     run_case(capi, kind, 1536, 1536, 256, -1.0, 1.0, lower=True, seed=10)
+
+
+@pytest.mark.parametrize("mode", [1, 2, 3])
+@pytest.mark.parametrize("kind", [0, 1])
+def test_every_tile_shape(capi, kind, mode):
+    # the same cases through each tile shape: 128x128, 128x256, 256x256 on a CTA pair
+    run_case(capi, kind, 640, 768, 128, 1.0, 0.0, seed=11, tile_mode=mode)
+    run_case(capi, kind, 1000, 1000, 192, -1.0, 1.0, lower=True, seed=12, tile_mode=mode)
+    run_case(capi, kind, 300, 520, 64, -1.0, 1.0, seed=13, tile_mode=mode)
+    run_case(capi, kind, 2304, 2304, 256, -1.0, 1.0, lower=True, seed=14, tile_mode=mode)
