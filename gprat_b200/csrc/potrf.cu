@@ -38,6 +38,19 @@ constexpr int PTHREADS = 256;
 constexpr int NWARPS = PTHREADS / 32;
 constexpr size_t SMEM_DOUBLES = PB * PS + 4 * SB * XS + PB + SB * TS + SB;
 
+template <typename T>
+struct PairOf;
+template <>
+struct PairOf<double>
+{
+    using type = double2;
+};
+template <>
+struct PairOf<float>
+{
+    using type = float2;
+};
+
 __device__ __forceinline__ void dmma(double (&c)[4], const double (&a)[4], const double (&b)[2])
 {
     asm volatile(
@@ -69,22 +82,24 @@ __device__ __forceinline__ void frag_b(double (&b)[2], const double *M, int ld, 
 }
 
 // Warp 0: factor the 32 x 32 sub-block at (c0, c0), write L back to smem,
-// and store X = L^-1 (zero above the diagonal) in xinv and the pivot
-// reciprocals 1/L_jj in dinv[0..31].
+// and store the pivot reciprocals 1/L_jj in dinv[0..31].
 //
-// Both loops are rolled and branch-free.  Each lane keeps a window of its row
-// in registers that shifts left by one column per step, so the current column
-// is always r[0] and every register index is a compile-time constant.  The
+// Branch-free, in rolled chunks of 8 pivots.  Each lane keeps a window of its
+// row in registers that shifts left by 8 columns per chunk, so every register
+// index is a compile-time constant and the code stays small (a fully unrolled
+// triangular loop outgrows the instruction cache).  The
 // updates are unconditional: a lane's entries above the diagonal (and window
 // slots past column 31) receive values that are never read, which keeps the
 // warp converged (per-lane conditional updates compile to divergent branches
 // that cost more than the arithmetic).  colbuf (32 doubles) broadcasts the
 // new column of L.
-__device__ __forceinline__ void diag_factor_invert(double *a, int c0, int bs, int row0, int *bad, double *xinv,
-                                                   double *dinv, double *colbuf)
+constexpr int CHUNK = 8;  // pivots per unrolled chunk of the diagonal factorisation
+
+__device__ __forceinline__ void diag_factor_invert(double *a, int c0, int bs, int row0, int *bad, double *dinv,
+                                                   double *colbuf)
 {
     const int lane = threadIdx.x & 31;
-    double r[SB];  // r[c] = A[lane][j + c] during step j
+    double r[SB];  // r[c] = A[lane][j0 + c] during chunk j0
     {
         const double *arow = a + (c0 + lane) * PS + c0;
 #pragma unroll
@@ -95,62 +110,85 @@ __device__ __forceinline__ void diag_factor_invert(double *a, int c0, int bs, in
     }
     int first_bad = 0;
 #pragma unroll 1
-    for (int j = 0; j < SB; ++j)
+    for (int j0 = 0; j0 < SB; j0 += CHUNK)
     {
-        const double ajj = __shfl_sync(0xffffffffu, r[0], j);
-        first_bad = (first_bad == 0 && !(ajj > 0.0) && c0 + j < bs) ? row0 + c0 + j + 1 : first_bad;
-        const double inv = rsqrt(ajj);
-        const double l = (lane == j) ? ajj * inv : r[0] * inv;  // L[lane][j] for lane >= j
-        colbuf[lane] = l;
-        a[(c0 + lane) * PS + c0 + j] = l;  // above the diagonal: a value nobody reads
-        if (lane == 0)
-        {
-            dinv[j] = inv;
-        }
-        __syncwarp();
 #pragma unroll
-        for (int c = 1; c < SB; ++c)
+        for (int jj = 0; jj < CHUNK; ++jj)
         {
-            r[c] -= l * colbuf[(j + c) & (SB - 1)];
-        }
-        __syncwarp();
+            const int j = j0 + jj;
+            const double ajj = __shfl_sync(0xffffffffu, r[jj], j);
+            first_bad = (first_bad == 0 && !(ajj > 0.0) && c0 + j < bs) ? row0 + c0 + j + 1 : first_bad;
+            const double inv = rsqrt(ajj);
+            const double l = (lane == j) ? ajj * inv : r[jj] * inv;  // L[lane][j] for lane >= j
+            colbuf[lane] = l;
+            a[(c0 + lane) * PS + c0 + j] = l;  // above the diagonal: a value nobody reads
+            if (lane == 0)
+            {
+                dinv[j] = inv;
+            }
+            __syncwarp();
+            // window slot c is column j0 + c; slots past column 31 are never read
 #pragma unroll
-        for (int c = 0; c < SB - 1; ++c)
-        {
-            r[c] = r[c + 1];
+            for (int c = jj + 1; c < SB; ++c)
+            {
+                r[c] -= l * colbuf[(j0 + c) & (SB - 1)];
+            }
+            __syncwarp();
         }
-        r[SB - 1] = 0.0;
+#pragma unroll
+        for (int c = 0; c < SB - CHUNK; ++c)
+        {
+            r[c] = r[c + CHUNK];
+        }
+#pragma unroll
+        for (int c = SB - CHUNK; c < SB; ++c)
+        {
+            r[c] = 0.0;
+        }
     }
     if (lane == 0 && first_bad != 0 && *bad == 0)
     {
         *bad = first_bad;
     }
-    __syncwarp();
-    // X column `lane`: x = e_lane; step k: x_k *= 1/L_kk, x_i -= L_ik x_k (i > k).
-    // x[c] holds x_{k + c} during step k.
-    double x[SB];
+}
+
+// All 8 warps: X = L^-1 of the factored 32 x 32 sub-block at (c0, c0), zero
+// above the diagonal, into xinv.  Warp w solves columns 4w .. 4w+3; lane i owns
+// row i (its row of L in registers) and the four columns' x_i.  Step k
+// broadcasts x_k (final once scaled by 1/L_kk) and every lane below updates.
+// Fully unrolled (32 short steps) and branch-free.
+__device__ __forceinline__ void diag_inverse_all_warps(const double *a, int c0, const double *dinv, double *xinv)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double lrow[SB];
+    const double *arow = a + (c0 + lane) * PS + c0;
 #pragma unroll
     for (int c = 0; c < SB; ++c)
     {
-        x[c] = (c == lane) ? 1.0 : 0.0;
+        lrow[c] = arow[c];  // above the diagonal: never used (lane > k selects)
     }
-#pragma unroll 1
+    double x[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+    {
+        x[q] = (lane == 4 * warp + q) ? 1.0 : 0.0;
+    }
+#pragma unroll
     for (int k = 0; k < SB; ++k)
     {
-        const double xk = x[0] * dinv[k];
-        xinv[k * XS + lane] = xk;
-        const double *col = a + c0 * PS + c0 + k;  // column k of L: L[i][k] at col[i * PS]
+        const double dk = dinv[k];
 #pragma unroll
-        for (int c = 1; c < SB; ++c)
+        for (int q = 0; q < 4; ++q)
         {
-            x[c] -= col[min(k + c, SB - 1) * PS] * xk;  // rows past 31: unused window slots
+            const double xk = __shfl_sync(0xffffffffu, x[q], k) * dk;
+            const double upd = x[q] - lrow[k] * xk;
+            x[q] = (lane == k) ? xk : ((lane > k) ? upd : x[q]);
         }
+    }
 #pragma unroll
-        for (int c = 0; c < SB - 1; ++c)
-        {
-            x[c] = x[c + 1];
-        }
-        x[SB - 1] = 0.0;
+    for (int q = 0; q < 4; ++q)
+    {
+        xinv[lane * XS + 4 * warp + q] = x[q];
     }
 }
 
@@ -176,18 +214,39 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
     {
         bad = 0;
     }
-    // load the lower triangle; pad with the identity beyond bs
-#pragma unroll 16
-    for (int q = 0; q < PB * PB / PTHREADS; ++q)
+    // load the lower triangle in pairs of columns (one 8- or 16-byte load each,
+    // all issued before the first store); pad with the identity beyond bs
     {
-        const int idx = q * PTHREADS + tid;
-        const int i = idx >> 7, c = idx & (PB - 1);
-        double v = (i == c) ? 1.0 : 0.0;
-        if (i < bs && c <= i)
+        using Pair = typename PairOf<T>::type;
+        double v0[PB * PB / 2 / PTHREADS], v1[PB * PB / 2 / PTHREADS];
+#pragma unroll
+        for (int q = 0; q < PB * PB / 2 / PTHREADS; ++q)
         {
-            v = static_cast<double>(A[static_cast<int64_t>(i) * lda + c]);
+            const int idx = q * PTHREADS + tid;
+            const int i = idx >> 6, c = 2 * (idx & 63);
+            const T *src = A + static_cast<int64_t>(i) * lda + c;
+            double a0 = (i == c) ? 1.0 : 0.0, a1 = (i == c + 1) ? 1.0 : 0.0;
+            if (i < bs && c + 1 <= i)
+            {
+                const Pair w = *reinterpret_cast<const Pair *>(src);
+                a0 = static_cast<double>(w.x);
+                a1 = static_cast<double>(w.y);
+            }
+            else if (i < bs && c == i)
+            {
+                a0 = static_cast<double>(src[0]);
+                a1 = 0.0;
+            }
+            v0[q] = a0;
+            v1[q] = a1;
         }
-        sa[i * PS + c] = v;
+#pragma unroll
+        for (int q = 0; q < PB * PB / 2 / PTHREADS; ++q)
+        {
+            const int idx = q * PTHREADS + tid;
+            const int i = idx >> 6, c = 2 * (idx & 63);
+            *reinterpret_cast<double2 *>(sa + i * PS + c) = make_double2(v0[q], v1[q]);
+        }
     }
     __syncthreads();
 
@@ -198,8 +257,10 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
         double *xs = xall + s * SB * XS;
         if (warp == 0)
         {
-            diag_factor_invert(sa, c0, bs, row0, &bad, xs, dinv + c0, colbuf);
+            diag_factor_invert(sa, c0, bs, row0, &bad, dinv + c0, colbuf);
         }
+        __syncthreads();
+        diag_inverse_all_warps(sa, c0, dinv + c0, xs);
         __syncthreads();
         if (s == 3)
         {
@@ -288,15 +349,27 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
     {
         atomicCAS(&status->not_spd_row, 0, bad);
     }
-    // write L (lower triangle incl. diagonal) back
-#pragma unroll 16
-    for (int q = 0; q < PB * PB / PTHREADS; ++q)
+    // write L (lower triangle incl. diagonal) back, in pairs of columns
     {
-        const int idx = q * PTHREADS + tid;
-        const int i = idx >> 7, c = idx & (PB - 1);
-        if (i < bs && c <= i)
+        using Pair = typename PairOf<T>::type;
+#pragma unroll 8
+        for (int q = 0; q < PB * PB / 2 / PTHREADS; ++q)
         {
-            A[static_cast<int64_t>(i) * lda + c] = static_cast<T>(sa[i * PS + c]);
+            const int idx = q * PTHREADS + tid;
+            const int i = idx >> 6, c = 2 * (idx & 63);
+            T *dst = A + static_cast<int64_t>(i) * lda + c;
+            const double2 v = *reinterpret_cast<const double2 *>(sa + i * PS + c);
+            if (i < bs && c + 1 <= i)
+            {
+                Pair w;
+                w.x = static_cast<T>(v.x);
+                w.y = static_cast<T>(v.y);
+                *reinterpret_cast<Pair *>(dst) = w;
+            }
+            else if (i < bs && c == i)
+            {
+                dst[0] = static_cast<T>(v.x);
+            }
         }
     }
     if (diag_out != nullptr && tid < bs)
@@ -369,18 +442,35 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
         }
         __syncthreads();
     }
-#pragma unroll 16
-    for (int q = 0; q < PB * PB / PTHREADS; ++q)
+    // store Linv (zero above the diagonal) in pairs of columns
+#pragma unroll 8
+    for (int q = 0; q < PB * PB / 2 / PTHREADS; ++q)
     {
         const int idx = q * PTHREADS + tid;
-        const int i = idx >> 7, c = idx & (PB - 1);
-        if (i < bs && c < bs)
+        const int i = idx >> 6, c = 2 * (idx & 63);
+        if (i >= bs || c >= bs)
         {
-            const double v = (c <= i) ? sa[i * PS + c] : 0.0;
-            Linv[static_cast<int64_t>(i) * ldi + c] = v;
-            if (Linv32 != nullptr)
+            continue;
+        }
+        const double2 raw = *reinterpret_cast<const double2 *>(sa + i * PS + c);
+        const double v0 = (c <= i) ? raw.x : 0.0;
+        const double v1 = (c + 1 <= i) ? raw.y : 0.0;
+        double *drow = Linv + static_cast<int64_t>(i) * ldi + c;
+        float *frow = (Linv32 != nullptr) ? Linv32 + static_cast<int64_t>(i) * ldi32 + c : nullptr;
+        if (c + 1 < bs)
+        {
+            *reinterpret_cast<double2 *>(drow) = make_double2(v0, v1);
+            if (frow != nullptr)
             {
-                Linv32[static_cast<int64_t>(i) * ldi32 + c] = static_cast<float>(v);
+                *reinterpret_cast<float2 *>(frow) = make_float2(static_cast<float>(v0), static_cast<float>(v1));
+            }
+        }
+        else
+        {
+            drow[0] = v0;
+            if (frow != nullptr)
+            {
+                frow[0] = static_cast<float>(v0);
             }
         }
     }
