@@ -173,16 +173,17 @@ void trsv_forward(const double *L, int64_t ldl, const double *Linv, int nb, int 
 void trsv_backward(const double *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, double *tmp,
                    cudaStream_t s);
 // Single-launch solves (trsv_fused.cu): one kernel per solve, row blocks
-// claimed by ticket, a progress counter between blocks.  flags: 2 ints of
-// scratch (zeroed by the call).  L in FP64 or FP32; x is FP64, in place.
+// claimed by ticket, every element of x written once and awaited by value.
+// flags: 1 int of scratch; scratch: n doubles (the right-hand side is copied
+// there).  L in FP64 or FP32; x is FP64, in place (b in, solution out).
 void trsv_fused_forward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                        DeviceStatus *st, cudaStream_t s);
+                        double *scratch, DeviceStatus *st, cudaStream_t s);
 void trsv_fused_backward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                         DeviceStatus *st, cudaStream_t s);
+                         double *scratch, DeviceStatus *st, cudaStream_t s);
 void trsv_fused_forward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                            DeviceStatus *st, cudaStream_t s);
+                            double *scratch, DeviceStatus *st, cudaStream_t s);
 void trsv_fused_backward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                             DeviceStatus *st, cudaStream_t s);
+                             double *scratch, DeviceStatus *st, cudaStream_t s);
 // Same with an FP32 factor (mixed precision); FP64 right-hand side and arithmetic.
 void trsv_forward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s);
 void trsv_backward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s);

@@ -200,9 +200,12 @@ void solve_alpha_fp64(gprat_cu_gp *gp, cudaStream_t s)
 {
     GPRAT_CUDA_CHECK(
         cudaMemcpyAsync(gp->alpha.ptr, gp->y.ptr, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    gp->flags.ensure(gp->nblk + 1);
-    trsv_fused_forward(gp->K.ptr, gp->ld, gp->Linv.ptr, gp->n, gp->alpha.ptr, gp->flags.ptr, gp->status.ptr, s);
-    trsv_fused_backward(gp->K.ptr, gp->ld, gp->Linv.ptr, gp->n, gp->alpha.ptr, gp->flags.ptr, gp->status.ptr, s);
+    gp->flags.ensure(2);
+    gp->trsv_b.ensure(gp->n);
+    trsv_fused_forward(gp->K.ptr, gp->ld, gp->Linv.ptr, gp->n, gp->alpha.ptr, gp->flags.ptr, gp->trsv_b.ptr,
+                       gp->status.ptr, s);
+    trsv_fused_backward(gp->K.ptr, gp->ld, gp->Linv.ptr, gp->n, gp->alpha.ptr, gp->flags.ptr, gp->trsv_b.ptr,
+                        gp->status.ptr, s);
 }
 
 bool mixed(const gprat_cu_gp *gp) { return gp->precision != GPRAT_CU_PREC_FP64; }

@@ -87,7 +87,8 @@ struct gprat_cu_gp
     gprat_cu::DevBuf<double> pcg_r, pcg_z, pcg_p, pcg_q, symv_part;
     gprat_cu::DevBuf<gprat_cu::PcgScalars> pcg_s;
     int pcg_last_iters = 0;
-    gprat_cu::DevBuf<int> flags;  // ticket + ready flags of the single-launch solves
+    gprat_cu::DevBuf<int> flags;         // ticket counter of the single-launch solves
+    gprat_cu::DevBuf<double> trsv_b;     // right-hand side copy of the single-launch solves
 
     ~gprat_cu_gp()
     {
@@ -103,7 +104,7 @@ struct gprat_cu_gp
             cudaStreamSynchronize(side);
         }
         for (gprat_cu::DevBuf<double> *b : { &x, &y, &K, &Linv, &alpha, &U, &partials, &xt, &W, &vacc, &mean_part,
-                                             &mean, &var, &losses, &D64, &pcg_r, &pcg_z, &pcg_p, &pcg_q, &symv_part })
+                                             &mean, &var, &losses, &D64, &pcg_r, &pcg_z, &pcg_p, &pcg_q, &symv_part, &trsv_b })
         {
             b->release();
         }

@@ -314,9 +314,12 @@ void symv(gprat_cu_gp *gp, const double *p, double *q, cudaStream_t s)
 void precondition(gprat_cu_gp *gp, const double *r, double *z, cudaStream_t s)
 {
     GPRAT_CUDA_CHECK(cudaMemcpyAsync(z, r, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    gp->flags.ensure(gp->nblk + 1);
-    trsv_fused_forward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, gp->n, z, gp->flags.ptr, gp->status.ptr, s);
-    trsv_fused_backward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, gp->n, z, gp->flags.ptr, gp->status.ptr, s);
+    gp->flags.ensure(2);
+    gp->trsv_b.ensure(gp->n);
+    trsv_fused_forward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, gp->n, z, gp->flags.ptr, gp->trsv_b.ptr,
+                           gp->status.ptr, s);
+    trsv_fused_backward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, gp->n, z, gp->flags.ptr, gp->trsv_b.ptr,
+                            gp->status.ptr, s);
 }
 
 }  // namespace

@@ -6,16 +6,20 @@
 // walk the block columns one after another.  Launching one kernel per block
 // makes the solve launch-latency bound (two launches per 128 rows).  Here one
 // kernel does the whole solve:
+//   * the right-hand side is copied aside and x is filled with a sentinel bit
+//     pattern (all ones, a NaN no arithmetic produces); every element of x is
+//     then written exactly once, by the CTA that solves its block;
 //   * every CTA takes a row block by atomic ticket (tickets follow launch
-//     order, so a CTA only ever waits for CTAs that are already running);
+//     order, so a CTA only waits for CTAs that are already running);
 //   * before it waits for anything it starts the asynchronous copy of its
-//     diagonal inverse into shared memory (lower triangle, packed);
-//   * it accumulates L_ij x_j over the blocks j it depends on; the loads of
-//     each tile of L are issued before the wait for x_j, so the DRAM latency
-//     overlaps the wait;
-//   * x_i = Linv_ii (b_i - sum_j L_ij x_j) from shared memory, then x_i is
-//     published by a release (threadfence) and the progress counter (number of
-//     finished blocks; blocks finish in solve order) is advanced.
+//     diagonal inverse into shared memory (lower triangle, packed) and issues
+//     the loads of the first tile of L;
+//   * it accumulates L_ij x_j over the blocks j it depends on, reading x_j
+//     straight from L2 and re-reading an element until it is no longer the
+//     sentinel -- the value is the flag, so no fence, counter or extra round
+//     trip sits on the chain between two blocks;
+//   * x_i = Linv_ii (b_i - sum_j L_ij x_j) from shared memory, eight threads
+//     per row.
 // L is read exactly once per solve.  Waits are bounded; a wait that runs out
 // sets the status word's timeout flag (the caller reports an error).
 #include "common.cuh"
@@ -27,7 +31,8 @@ namespace
 
 constexpr int FT = 256;  // threads per CTA (8 warps)
 constexpr int FB = 128;  // block size
-constexpr long long SPIN_LIMIT = 1ll << 24;  // with 64 ns sleeps: about 1-2 s
+constexpr long long SPIN_LIMIT = 1ll << 24;  // with 32 ns sleeps: about 0.5-1 s
+constexpr long long SENTINEL = -1ll;          // 0xFFFF...FF
 
 // Packed lower triangle of a 128 x 128 FP64 block: row r holds columns
 // 0..r padded to an even count, so every row starts on a 16-byte boundary.
@@ -60,27 +65,77 @@ __device__ __forceinline__ void load_diag_inverse(double *dst, const double *Li)
     }
 }
 
-// Thread 0 waits until *progress >= target; returns the value it saw (or
-// target after a timeout, with the status flag set).
-__device__ __forceinline__ int wait_progress(const volatile int *progress, int target, DeviceStatus *st)
+__device__ __forceinline__ double load_relaxed(const double *p)
+{
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Reads N elements of x (one per call site), waiting (bounded) until their
+// solvers have written them.  Every lane of the warp calls this together.
+// urgent: the block is the one this CTA's own block waits on (its result is
+// on the critical path), so every lane re-polls at once; otherwise (the whole
+// frontier of waiting CTAs would be polling the same kilobyte of L2) one lane
+// polls with a longer sleep and the warp re-reads when it sees data.
+template <int N>
+__device__ __forceinline__ void await_x(const double *const (&p)[N], double (&v)[N], bool urgent, DeviceStatus *st)
 {
     long long spins = 0;
-    int v = *progress;
-    while (v < target)
+    for (;;)
     {
+        bool missing = false;
+#pragma unroll
+        for (int q = 0; q < N; ++q)
+        {
+            v[q] = load_relaxed(p[q]);
+            missing |= __double_as_longlong(v[q]) == SENTINEL;
+        }
+        if (!__any_sync(0xffffffffu, missing))
+        {
+            return;
+        }
         if (++spins > SPIN_LIMIT)
         {
             if (st != nullptr)
             {
                 atomicExch(&st->timeout, 1);
             }
-            return target;
+#pragma unroll
+            for (int q = 0; q < N; ++q)
+            {
+                v[q] = 0.0;
+            }
+            return;
         }
-        __nanosleep(64);
-        v = *progress;
+        if (urgent)
+        {
+            __nanosleep(20);
+        }
+        else
+        {
+            // one lane waits on one missing element before the warp re-reads
+            const unsigned who = __ballot_sync(0xffffffffu, missing);
+            if ((threadIdx.x & 31) == __ffs(who) - 1)
+            {
+                bool waited = false;
+#pragma unroll
+                for (int t = 0; t < N; ++t)
+                {
+                    if (!waited && __double_as_longlong(v[t]) == SENTINEL)
+                    {
+                        long long inner = 0;
+                        while (__double_as_longlong(load_relaxed(p[t])) == SENTINEL && ++inner < SPIN_LIMIT)
+                        {
+                            __nanosleep(256);
+                        }
+                        waited = true;
+                    }
+                }
+            }
+            __syncwarp();
+        }
     }
-    __threadfence();
-    return v;
 }
 
 template <typename T>
@@ -89,11 +144,12 @@ __device__ __forceinline__ double to_d(T v)
     return static_cast<double>(v);
 }
 
-// flags[0] = ticket counter, flags[1] = progress (finished blocks).
+// flags[0] = ticket counter; b = right-hand side (copy); x = solution (sentinel-filled).
 template <typename T>
 __global__ void __launch_bounds__(FT, 1) trsv_fwd_fused_kernel(const T *__restrict__ L, int64_t ld,
-                                                               const double *__restrict__ Linv, int n, double *x,
-                                                               int *flags, DeviceStatus *st)
+                                                               const double *__restrict__ Linv, int n,
+                                                               const double *__restrict__ b, double *x, int *flags,
+                                                               DeviceStatus *st)
 {
     extern __shared__ __align__(16) double sm[];
     double *linv_s = sm;              // packed lower triangle of Linv_ii
@@ -111,7 +167,7 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_fused_kernel(const T *__restri
     load_diag_inverse(linv_s, Linv + static_cast<int64_t>(i) * FB * FB);
     if (tid < FB)
     {
-        rhs[tid] = (tid < bs) ? x[r0 + tid] : 0.0;
+        rhs[tid] = (tid < bs) ? b[r0 + tid] : 0.0;
     }
     __syncthreads();  // rhs rows are updated below by other threads
 
@@ -123,7 +179,6 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_fused_kernel(const T *__restri
     {
         part[q] = 0.0;
     }
-    int seen = 0;  // progress observed so far
     for (int j = 0; j < i; ++j)
     {
         const int c0 = j * FB;
@@ -142,21 +197,10 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_fused_kernel(const T *__restri
                     v[q][c] = lr[32 * c];
                 }
             }
-            if (qb == 0 && j >= seen)
-            {
-                if (tid == 0)
-                {
-                    shared_int[1] = wait_progress(flags + 1, j + 1, st);
-                }
-                __syncthreads();
-                seen = shared_int[1];
-                __syncthreads();
-            }
             double xv[4];
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
             {
-                xv[c] = __ldcg(x + c0 + lane + 32 * c);
+                const double *xp[4] = { x + c0 + lane, x + c0 + lane + 32, x + c0 + lane + 64, x + c0 + lane + 96 };
+                await_x<4>(xp, xv, j == i - 1, st);
             }
 #pragma unroll
             for (int q = 0; q < QB; ++q)
@@ -193,34 +237,35 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_fused_kernel(const T *__restri
     }
     cp_async_wait_all();
     __syncthreads();
-    // x_i[r] = sum_{c <= r} Linv[r][c] rhs[c]; two threads per row, 64 columns each
+    // x_i[r] = sum_{c <= r} Linv[r][c] rhs[c]: eight threads per row, columns
+    // p, p+8, ... (consecutive threads read consecutive words), 32 rows per pass
+#pragma unroll
+    for (int pass = 0; pass < FB / 32; ++pass)
     {
-        const int r = tid >> 1, h = tid & 1;
+        const int r = pass * 32 + (tid >> 3), p = tid & 7;
         const double *lr = linv_s + packed_off(r);
         double s = 0.0;
-        const int cend = min(r, 64 * h + 63);
-        for (int c = 64 * h; c <= cend; ++c)
+#pragma unroll
+        for (int k = 0; k < FB / 8; ++k)
         {
-            s += lr[c] * rhs[c];
+            const int c = p + 8 * k;
+            s += (c <= r) ? lr[c] * rhs[c] : 0.0;
         }
         s += __shfl_xor_sync(0xffffffffu, s, 1);
-        if (h == 0 && r < bs)
+        s += __shfl_xor_sync(0xffffffffu, s, 2);
+        s += __shfl_xor_sync(0xffffffffu, s, 4);
+        if (p == 0 && r < bs)
         {
             x[r0 + r] = s;
         }
-    }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0)
-    {
-        atomicMax(flags + 1, i + 1);
     }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(FT, 1) trsv_bwd_fused_kernel(const T *__restrict__ L, int64_t ld,
                                                                const double *__restrict__ Linv, int n, int nblk,
-                                                               double *x, int *flags, DeviceStatus *st)
+                                                               const double *__restrict__ b, double *x, int *flags,
+                                                               DeviceStatus *st)
 {
     extern __shared__ __align__(16) double sm[];
     double *linv_s = sm;
@@ -239,17 +284,15 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_fused_kernel(const T *__restri
     load_diag_inverse(linv_s, Linv + static_cast<int64_t>(i) * FB * FB);
     if (tid < FB)
     {
-        rhs[tid] = (tid < bs) ? x[c0 + tid] : 0.0;
+        rhs[tid] = (tid < bs) ? b[c0 + tid] : 0.0;
     }
     // lanes own columns lane + 32c of block i; warps own rows warp + 8q of each block j
     constexpr int QB = sizeof(T) == 4 ? 16 : 8;
     double part[4] = { 0.0, 0.0, 0.0, 0.0 };
-    int seen = 0;
     for (int j = nblk - 1; j > i; --j)
     {
         const int r0 = j * FB;
         const int rs = min(FB, n - r0);
-        const int need = nblk - j;  // blocks nblk-1 .. j finished
 #pragma unroll
         for (int qb = 0; qb < 16; qb += QB)
         {
@@ -265,25 +308,25 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_fused_kernel(const T *__restri
                     v[q][c] = (lane + 32 * c < bs) ? lr[32 * c] : T(0);
                 }
             }
-            if (qb == 0 && need > seen)
+            double xv[QB];
             {
-                if (tid == 0)
+                const double *xp[QB];
+#pragma unroll
+                for (int q = 0; q < QB; ++q)
                 {
-                    shared_int[1] = wait_progress(flags + 1, need, st);
+                    xp[q] = x + r0 + min(warp + 8 * (qb + q), rs - 1);
                 }
-                __syncthreads();
-                seen = shared_int[1];
-                __syncthreads();
+                await_x<QB>(xp, xv, j == i + 1, st);
             }
 #pragma unroll
             for (int q = 0; q < QB; ++q)
             {
                 const int r = warp + 8 * (qb + q);
-                const double xv = (r < rs) ? __ldcg(x + r0 + r) : 0.0;
+                const double xr = (r < rs) ? xv[q] : 0.0;
 #pragma unroll
                 for (int c = 0; c < 4; ++c)
                 {
-                    part[c] += to_d(v[q][c]) * xv;
+                    part[c] += to_d(v[q][c]) * xr;
                 }
             }
         }
@@ -306,74 +349,83 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_fused_kernel(const T *__restri
     }
     cp_async_wait_all();
     __syncthreads();
-    // x_i[c] = sum_{p >= c} Linv[p][c] rhs[p]; two threads per column, 64 rows each
+    // x_i[c] = sum_{p >= c} Linv[p][c] rhs[p]: eight threads per column, rows
+    // q, q+8, ..., 32 columns per pass
+#pragma unroll
+    for (int pass = 0; pass < FB / 32; ++pass)
     {
-        const int c = tid >> 1, h = tid & 1;
+        const int c = pass * 32 + (tid >> 3), q = tid & 7;
         double s = 0.0;
-        const int pbeg = max(c, 64 * h);
-        const int pend = min(bs - 1, 64 * h + 63);
-        for (int p = pbeg; p <= pend; ++p)
+#pragma unroll
+        for (int k = 0; k < FB / 8; ++k)
         {
-            s += linv_s[packed_off(p) + c] * rhs[p];
+            const int p = q + 8 * k;
+            s += (p >= c && p < bs) ? linv_s[packed_off(p) + min(c, p)] * rhs[p] : 0.0;
         }
         s += __shfl_xor_sync(0xffffffffu, s, 1);
-        if (h == 0 && c < bs)
+        s += __shfl_xor_sync(0xffffffffu, s, 2);
+        s += __shfl_xor_sync(0xffffffffu, s, 4);
+        if (q == 0 && c < bs)
         {
             x[c0 + c] = s;
         }
     }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0)
-    {
-        atomicMax(flags + 1, nblk - i);
-    }
+}
+
+// x: in = b, out = solution.  scratch: n doubles (receives b).
+void prepare(double *x, double *scratch, int n, int *flags, cudaStream_t s)
+{
+    GPRAT_CUDA_CHECK(cudaMemcpyAsync(scratch, x, static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    GPRAT_CUDA_CHECK(cudaMemsetAsync(x, 0xFF, static_cast<size_t>(n) * sizeof(double), s));
+    GPRAT_CUDA_CHECK(cudaMemsetAsync(flags, 0, sizeof(int), s));
 }
 
 template <typename T>
-void fwd(const T *L, int64_t ld, const double *Linv, int n, double *x, int *flags, DeviceStatus *st, cudaStream_t s)
+void fwd(const T *L, int64_t ld, const double *Linv, int n, double *x, int *flags, double *scratch, DeviceStatus *st,
+         cudaStream_t s)
 {
     const int nblk = ceil_div(n, FB);
     ensure_smem_attr(reinterpret_cast<const void *>(trsv_fwd_fused_kernel<T>), static_cast<int>(SMEM_BYTES));
-    GPRAT_CUDA_CHECK(cudaMemsetAsync(flags, 0, 2 * sizeof(int), s));
-    trsv_fwd_fused_kernel<T><<<nblk, FT, SMEM_BYTES, s>>>(L, ld, Linv, n, x, flags, st);
+    prepare(x, scratch, n, flags, s);
+    trsv_fwd_fused_kernel<T><<<nblk, FT, SMEM_BYTES, s>>>(L, ld, Linv, n, scratch, x, flags, st);
     GPRAT_LAUNCH_CHECK();
 }
 
 template <typename T>
-void bwd(const T *L, int64_t ld, const double *Linv, int n, double *x, int *flags, DeviceStatus *st, cudaStream_t s)
+void bwd(const T *L, int64_t ld, const double *Linv, int n, double *x, int *flags, double *scratch, DeviceStatus *st,
+         cudaStream_t s)
 {
     const int nblk = ceil_div(n, FB);
     ensure_smem_attr(reinterpret_cast<const void *>(trsv_bwd_fused_kernel<T>), static_cast<int>(SMEM_BYTES));
-    GPRAT_CUDA_CHECK(cudaMemsetAsync(flags, 0, 2 * sizeof(int), s));
-    trsv_bwd_fused_kernel<T><<<nblk, FT, SMEM_BYTES, s>>>(L, ld, Linv, n, nblk, x, flags, st);
+    prepare(x, scratch, n, flags, s);
+    trsv_bwd_fused_kernel<T><<<nblk, FT, SMEM_BYTES, s>>>(L, ld, Linv, n, nblk, scratch, x, flags, st);
     GPRAT_LAUNCH_CHECK();
 }
 
 }  // namespace
 
 void trsv_fused_forward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                        DeviceStatus *st, cudaStream_t s)
+                        double *scratch, DeviceStatus *st, cudaStream_t s)
 {
-    fwd(L, ld, Linv, n, x, flags, st, s);
+    fwd(L, ld, Linv, n, x, flags, scratch, st, s);
 }
 
 void trsv_fused_backward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                         DeviceStatus *st, cudaStream_t s)
+                         double *scratch, DeviceStatus *st, cudaStream_t s)
 {
-    bwd(L, ld, Linv, n, x, flags, st, s);
+    bwd(L, ld, Linv, n, x, flags, scratch, st, s);
 }
 
 void trsv_fused_forward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                            DeviceStatus *st, cudaStream_t s)
+                            double *scratch, DeviceStatus *st, cudaStream_t s)
 {
-    fwd(L, ld, Linv, n, x, flags, st, s);
+    fwd(L, ld, Linv, n, x, flags, scratch, st, s);
 }
 
 void trsv_fused_backward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                             DeviceStatus *st, cudaStream_t s)
+                             double *scratch, DeviceStatus *st, cudaStream_t s)
 {
-    bwd(L, ld, Linv, n, x, flags, st, s);
+    bwd(L, ld, Linv, n, x, flags, scratch, st, s);
 }
 
 }  // namespace gprat_cu
