@@ -114,6 +114,23 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(value: float, dist, device) -> float:
+    """The step time of a multi-GPU run: the maximum over all ranks (every rank
+    calls this, in the same order, like every collective)."""
+    import torch
+
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_seconds(ms_per_step: float, world: int) -> float:
+    """Whole-job seconds per fit+predict job: N replicas finish N jobs per step."""
+    return ms_per_step / 1e3 / world
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -219,6 +236,27 @@ def config_of(wl):
 
 PRECISIONS = {"fp64": 0, "mixed-tf32": 1, "mixed-bf16": 2}
 
+# DRAM traffic of one representative launch of the dominant kernel, from an
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum); the live
+# roofline above aggregates every GEMM launch of the step, so the per-launch
+# traffic is quoted from the capture instead of being measured in this run.
+TRAFFIC_SAMPLE = {
+    "mixed-tf32": {
+        "launch": "tc_gemm_pair_kernel<TF32>, trailing update after panel 0 at n_train=16384: "
+                  "lower 15360 x 15360, K=512, 51 CTA pairs",
+        "dram_bytes": 520.9e6 + 416.5e6,
+        "algorithmic_bytes": 2 * 15360 * 15361 / 2 * 4 + 15360 * 512 * 4,
+        "source": "profiles/tc_gemm_trailing_update_c1.md",
+    },
+    "fp64": {
+        "launch": "dgemm_kernel<2,0,1>, trailing update after the first outer panel at n_train=16384: "
+                  "lower 15872 x 15872, K=512",
+        "dram_bytes": 2.524e9 + 0.986e9,
+        "algorithmic_bytes": 2 * 15872 * 15873 / 2 * 8 + 15872 * 512 * 8,
+        "source": "profiles/dgemm_trailing_update_c1.md",
+    },
+}
+
 # Serving stream (resident models n in SERVE_MODELS, d=8, Poisson arrivals):
 # 90 % predict_with_uncertainty with m log-uniform in [1, 8192] on a uniformly
 # chosen model, 10 % fits with n log-uniform in [1024, 16384] (rounded to 128).
@@ -309,6 +347,16 @@ def serving_bench(precision: int, seed: int = 7):
             t_done.append(ts + lat / 1e3)
         wall = max(t_done) - t_start
         st = sv.stats()
+        # capacity: the same kind of stream submitted all at once
+        burst = []
+        for _ in range(SERVE_REQUESTS):
+            m = int(np.exp(rng.uniform(0.0, np.log(8192))))
+            burst.append((mids[int(rng.integers(0, len(SERVE_MODELS)))], rng.standard_normal(m + d - 1), m))
+        t0 = time.perf_counter()
+        bids = [sv.submit_predict(mid, series, m) for mid, series, m in burst]
+        for rid in bids:
+            sv.wait(rid)
+        burst_wall = time.perf_counter() - t0
     points = sum(sz for sz, k in zip(sizes, kinds) if k == "predict")
     return {
         "requests": SERVE_REQUESTS, "rate_per_s": SERVE_RATE,
@@ -317,6 +365,8 @@ def serving_bench(precision: int, seed: int = 7):
         "fit_p99_ms": float(np.percentile(lat_f, 99)) if lat_f else None,
         "predictions_per_s": points / wall, "predict_requests": len(lat_p), "fit_requests": len(lat_f),
         "batches": st.batches, "model_setup_s": setup_s,
+        "saturated_predictions_per_s": sum(b[2] for b in burst) / burst_wall,
+        "saturated_requests": len(burst),
     }
 
 
@@ -351,10 +401,7 @@ def run_ours(args, wl):
 
     elapsed_ms, stats, clk = time_device_steps(torch, gp, hyper, dxt, m, dmean, dvar, stream, args.steps,
                                                args.warmup, barrier, local)
-    t = torch.tensor([elapsed_ms], dtype=torch.float64, device=device)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_per_step = float(t.item()) / args.steps
+    ms_per_step = max_over_ranks(elapsed_ms, dist if world > 1 else None, device) / args.steps
 
     mean_h, var_h = dmean.cpu().numpy(), dvar.cpu().numpy()
     sane = bool(np.all(np.isfinite(mean_h)) and np.all(var_h > 0) and np.all(var_h <= hyper[1] + 1e-12))
@@ -385,14 +432,11 @@ def run_ours(args, wl):
         v64 = torch.empty_like(dvar)
         el64, st64, clk64 = time_device_steps(torch, gp, hyper, dxt, m, m64, v64, stream, args.steps, args.warmup,
                                               barrier, local)
-        t64 = torch.tensor([el64], dtype=torch.float64, device=device)
-        if world > 1:
-            dist.all_reduce(t64, op=dist.ReduceOp.MAX)
-        ms64 = float(t64.item()) / args.steps
+        ms64 = max_over_ranks(el64, dist if world > 1 else None, device) / args.steps
         mean64, var64 = m64.cpu().numpy(), v64.cpu().numpy()
         loss64 = gp.compute_loss(hyper)
         fp64 = {
-            "value": ms64 / 1e3 / world, "ms_per_step": ms64,
+            "value": aggregate_seconds(ms64, world), "ms_per_step": ms64,
             "gemm_tflops": st64["gemm_flops"] / (st64["gemm_ms"] / 1e3) / 1e12 if st64["gemm_ms"] > 0 else None,
             "clocks": clk64,
             "speedup_of_mixed": ms64 / ms_per_step,
@@ -440,7 +484,7 @@ def run_ours(args, wl):
             serve["fp64"] = serving_bench(capi.PREC_FP64)
     line = {
         "metric": METRIC,
-        "value": ms_per_step / 1e3 / world,
+        "value": aggregate_seconds(ms_per_step, world),
         "unit": "s",
         "n_gpus": world,
         "steps": args.steps,
@@ -462,6 +506,7 @@ def run_ours(args, wl):
             "unit": "TFLOP/s",
             "frac": (gemm_tflops / peak) if gemm_tflops else None,
             "traffic": None,
+            "traffic_sample": TRAFFIC_SAMPLE.get(args.precision),
             "gemm_share_of_step": (stats["gemm_ms"] / args.steps) / ms_per_step,
             "gemm_launches_per_step": stats["gemm_launches"] / args.steps,
         },

@@ -22,8 +22,11 @@ namespace gprat_cu
 namespace gemm
 {
 
-constexpr int BK = 16;
-constexpr int PAD_K = 4;  // stride BK+4 = 20 doubles
+#ifndef GPRAT_DGEMM_BK
+#define GPRAT_DGEMM_BK 16
+#endif
+constexpr int BK = GPRAT_DGEMM_BK;  // K per pipeline stage
+constexpr int PAD_K = 4;  // stride BK+4 doubles (conflict-free fragment loads)
 constexpr int PAD_T = 8;  // stride ROWS+8 doubles
 
 template <int WN>
@@ -33,7 +36,7 @@ struct Cfg
     static constexpr int THREADS = 32 * WM * WN;
     static constexpr int BM = 64 * WM;  // 128
     static constexpr int BN = 32 * WN;  // 128 or 64
-    static constexpr int STAGES = (WN == 4) ? 4 : 3;
+    static constexpr int STAGES = (WN == 4) ? (BK == 16 ? 4 : 3) : (BK == 16 ? 3 : 2);
     static constexpr int MIN_BLOCKS = (WN == 4) ? 1 : 2;
 };
 
@@ -91,7 +94,7 @@ __device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4]
 }
 
 // Copies one operand tile (ROWS rows of the operand starting at r0, K range
-// [k0, k0+16)) into shared memory with zero fill outside [rows) x [K).
+// [k0, k0+BK)) into shared memory with zero fill outside [rows) x [K).
 // KMAJOR: element (row, k) at P[row*ld + k]; otherwise at P[k*ld + row].
 template <bool KMAJOR, int ROWS, int THREADS>
 __device__ __forceinline__ void load_tile(double *s, const double *P, int64_t ld, int rows, int K, int r0, int k0,
@@ -104,8 +107,8 @@ __device__ __forceinline__ void load_tile(double *s, const double *P, int64_t ld
         for (int i = 0; i < CHUNKS / THREADS; ++i)
         {
             int c = tid + i * THREADS;
-            int row = c >> 3;
-            int kc = (c & 7) * 2;
+            int row = c / (BK / 2);
+            int kc = (c % (BK / 2)) * 2;
             int gr = r0 + row, gk = k0 + kc;
             int nv = (gr < rows) ? min(max(K - gk, 0), 2) : 0;
             const double *src = nv ? P + static_cast<int64_t>(gr) * ld + gk : P;
