@@ -207,6 +207,107 @@ def cpu_reference_sample(wl, reps: int):
     return statistics.median(times), scale, desc, threads
 
 
+def cpu_reference_calls(wl, reps: int = 3):
+    """Wall time of the reference's CPU API calls (compiled from source,
+    oracle/_ref, all host cores) at the bounded sample size n_train=8192 with
+    the workload's d and hyper-parameters: cholesky, predict_with_uncertainty,
+    calculate_loss (median of reps) and one optimize_step."""
+    from oracle import ref
+
+    n, d, T = CPU_SAMPLE_N, wl["d"], 512
+    m = wl["m"] * n // wl["n"]
+    ref.start(os.cpu_count() or 1)
+    x, y, xt = synthetic(n, m, d)
+    gp = ref.RefGP(x, y, n // T, T, d, wl["hyper"])
+
+    def med(f, r):
+        ts = []
+        for _ in range(r):
+            t0 = time.perf_counter()
+            f()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts)
+
+    return {
+        "n_train": n, "n_test": m, "n_regressors": d, "tile": T,
+        "cholesky_s": med(gp.cholesky, reps),
+        "predict_with_uncertainty_s": med(lambda: gp.predict_with_uncertainty(xt, m // T, T), reps),
+        "calculate_loss_s": med(gp.calculate_loss, reps),
+        "optimize_step_s": med(lambda: gp.optimize_step(0, 0.1, 0.9, 0.999, 1e-8), 1),
+    }
+
+
+def gpu_calls(wl, precision: int, reps: int = 3):
+    """The same calls through this library's C ABI (host buffers, synchronous),
+    at the same sample size as cpu_reference_calls."""
+    from gprat_b200 import capi
+
+    n, d, T = CPU_SAMPLE_N, wl["d"], 512
+    m = wl["m"] * n // wl["n"]
+    x, y, xt = synthetic(n, m, d)
+    gp = capi.CudaGP(x, y, n // T, T, d)
+    gp.set_precision(precision)
+    h = wl["hyper"]
+    params = np.array(list(h) + [0.0] * 6)
+
+    def med(f, r):
+        f()
+        ts = []
+        for _ in range(r):
+            t0 = time.perf_counter()
+            f()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts)
+
+    out = {
+        "predict_with_uncertainty_s": med(lambda: gp.predict_with_uncertainty(h, xt, m // T, T), reps),
+        "calculate_loss_s": med(lambda: gp.compute_loss(h), reps),
+    }
+    if precision == capi.PREC_FP64:
+        out["cholesky_s"] = med(lambda: gp.cholesky(h), reps)
+        out["optimize_step_s"] = med(lambda: gp.optimize_step(params.copy(), [0.1, 0.9, 0.999, 1e-8], [1, 1, 1], 0),
+                                     reps)
+    gp.close()
+    return out
+
+
+def cusolver_fp64_comparator(torch, device, wl):
+    """FP64 library comparator: the same fit+predict_with_uncertainty written
+    with torch's FP64 linear algebra on the GPU (cdist, cuSOLVER Cholesky,
+    triangular solves), device-timed with CUDA events (best of 2)."""
+    n, m, d, hyper = wl["n"], wl["m"], wl["d"], wl["hyper"]
+    x, y, xt = synthetic(n, m, d)
+    X = torch.tensor(x, dtype=torch.float64, device=device).unfold(0, d, 1)[:n]
+    Xt = torch.tensor(xt, dtype=torch.float64, device=device).unfold(0, d, 1)[:m]
+    yy = torch.tensor(y[:n], dtype=torch.float64, device=device)
+    l, v, noise = hyper
+
+    def step():
+        K = v * torch.exp(-0.5 / l ** 2 * torch.cdist(X, X).square_())
+        K.diagonal().add_(noise)
+        L = torch.linalg.cholesky(K)
+        del K
+        alpha = torch.cholesky_solve(yy.unsqueeze(1), L)
+        Ks = v * torch.exp(-0.5 / l ** 2 * torch.cdist(Xt, X).square_())
+        mean = Ks @ alpha
+        V = torch.linalg.solve_triangular(L, Ks.T, upper=False)
+        var = v - V.square().sum(0)
+        return mean, var
+
+    best = float("inf")
+    for _ in range(2):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        step()
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    torch.cuda.empty_cache()
+    return {"value": best / 1e3, "unit": "s",
+            "what": "torch FP64 on the GPU: cdist + exp assembly, torch.linalg.cholesky (cuSOLVER), cholesky_solve, "
+                    "solve_triangular for the variance; same inputs; best of 2"}
+
+
 def run_reference(args, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -420,6 +521,13 @@ def run_ours(args, wl):
         gp.predict_with_uncertainty(hyper, xt_pinned, 1, m)
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = float(np.mean(e2e_times))
+    # per-phase device time of one more call (step timers; not part of the timed region)
+    capi.steps_reset()
+    capi.steps_enable(True)
+    gp.predict_with_uncertainty(hyper, xt_pinned, 1, m)
+    phases = {k: round(v[1], 3) for k, v in capi.steps().items()}
+    capi.steps_enable(False)
+    capi.steps_reset()
     loss = gp.compute_loss(hyper)
     pcg_iters = gp.pcg_iterations()
 
@@ -474,9 +582,15 @@ def run_ours(args, wl):
     step_flops = algorithmic_flops(n, m)
     if world == 1 and not args.skip_cpu_baseline:
         sample_s, scale, desc, threads = cpu_reference_sample(wl, 3)
-        cpu = {"value": sample_s * scale, "unit": "s", "cores": threads, "kind": "reference", "sample": desc}
+        cpu = {"value": sample_s * scale, "unit": "s", "cores": threads, "kind": "reference", "sample": desc,
+               "calls_at_sample": cpu_reference_calls(wl),
+               "gpu_calls_at_sample": {"fp64": gpu_calls(wl, capi.PREC_FP64),
+                                       args.precision: gpu_calls(wl, PRECISIONS[args.precision])}}
     else:
         cpu = None
+    comparator = None
+    if world == 1 and not args.skip_fp64:
+        comparator = cusolver_fp64_comparator(torch, device, wl)
     serve = None
     if world == 1 and not args.skip_serving:
         serve = {args.precision: serving_bench(PRECISIONS[args.precision])}
@@ -514,8 +628,10 @@ def run_ours(args, wl):
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int((m + d - 1) * 8),
                 "d2h_bytes_per_step": int(2 * m * 8)},
         "gpu_launches": int(stats["launches"]),
+        "phases_ms": phases,
         "clocks": clk,
         "fp64": fp64,
+        "fp64_library_comparator": comparator,
         "serving": serve,
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
         "pcg_iterations": pcg_iters,

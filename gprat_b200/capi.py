@@ -77,6 +77,8 @@ def _load() -> ctypes.CDLL:
                                           _i64, _fp, _i64, ctypes.c_float, ctypes.c_float, ctypes.c_int, _dp,
                                           ctypes.c_int]
     _vp, _i64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)
+    lib.gprat_cu_steps_enable.argtypes = [ctypes.c_int]
+    lib.gprat_cu_steps_csv.argtypes = [ctypes.c_char_p, _i64, _i64p]
     lib.gprat_cu_server_create.argtypes = [ctypes.c_int, _i64, ctypes.c_int, ctypes.POINTER(_vp)]
     lib.gprat_cu_server_destroy.argtypes = [_vp]
     lib.gprat_cu_server_add_model.argtypes = [_vp, _dp, _i64, _dp, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -128,6 +130,32 @@ def stats_read() -> dict:
     c, d = ctypes.c_double(), ctypes.c_double()
     check(lib.gprat_cu_stats_read(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)))
     return {"launches": a.value, "gemm_launches": b.value, "gemm_ms": c.value, "gemm_flops": d.value}
+
+
+def steps_enable(enable: bool) -> None:
+    check(lib.gprat_cu_steps_enable(int(bool(enable))))
+
+
+def steps_reset() -> None:
+    check(lib.gprat_cu_steps_reset())
+
+
+def steps_csv() -> str:
+    """Per-phase step timers as CSV text: label,calls,total_ms,mean_ms."""
+    need = ctypes.c_int64()
+    check(lib.gprat_cu_steps_csv(None, 0, ctypes.byref(need)))
+    buf = ctypes.create_string_buffer(int(need.value) + 64)
+    check(lib.gprat_cu_steps_csv(buf, len(buf), ctypes.byref(need)))
+    return buf.value.decode()
+
+
+def steps() -> dict:
+    """{label: (calls, total_ms)} from steps_csv()."""
+    out = {}
+    for line in steps_csv().strip().splitlines()[1:]:
+        label, calls, total, _ = line.rsplit(",", 3)
+        out[label] = (int(calls), float(total))
+    return out
 
 
 def test_tc_gemm(kind: int, A: np.ndarray, B: np.ndarray, C: np.ndarray, alpha: float, beta: float,

@@ -65,6 +65,29 @@ void note_launch();
         GPRAT_CUDA_CHECK(cudaGetLastError());   \
     } while (0)
 
+// Step timers (stats.cu): a StepScope brackets one phase of a pipeline with
+// CUDA events on its stream when gprat_cu_steps_enable(1) is in effect; the
+// label is the calling entry point's prefix (StepPrefix, e.g. "predict_step")
+// plus the phase ("cholesky").
+bool steps_enabled();
+struct StepPrefix
+{
+    explicit StepPrefix(const char *prefix);
+    ~StepPrefix();
+    StepPrefix(const StepPrefix &) = delete;
+    StepPrefix &operator=(const StepPrefix &) = delete;
+    std::string saved;
+};
+struct StepScope
+{
+    StepScope(const char *phase, cudaStream_t s);
+    ~StepScope();
+    StepScope(const StepScope &) = delete;
+    StepScope &operator=(const StepScope &) = delete;
+    int slot;
+    cudaStream_t stream;
+};
+
 // GEMM timing hooks (stats.cu): returns true when timing is on, in which
 // case the caller brackets the launch with gemm_timing_begin/end.
 bool gemm_timing_enabled();

@@ -192,7 +192,11 @@ void cholesky_blocked(gprat_cu_gp *gp, cudaStream_t s)
 // FP64 factorisation (always used by cholesky() and the optimiser).
 void factor_fp64(gprat_cu_gp *gp, cudaStream_t s)
 {
-    assemble_covariance(gp->x.ptr, gp->n, gp->d, gp->T, gp->params.ptr, gp->K.ptr, gp->ld, s);
+    {
+        StepScope step("assembly", s);
+        assemble_covariance(gp->x.ptr, gp->n, gp->d, gp->T, gp->params.ptr, gp->K.ptr, gp->ld, s);
+    }
+    StepScope step("cholesky", s);
     cholesky_blocked(gp, s);
 }
 
@@ -202,8 +206,12 @@ void solve_alpha_fp64(gprat_cu_gp *gp, cudaStream_t s)
         cudaMemcpyAsync(gp->alpha.ptr, gp->y.ptr, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     gp->flags.ensure(2);
     gp->trsv_b.ensure(gp->n);
-    trsv_fused_forward(gp->K.ptr, gp->ld, gp->Linv.ptr, gp->n, gp->alpha.ptr, gp->flags.ptr, gp->trsv_b.ptr,
-                       gp->status.ptr, s);
+    {
+        StepScope step("forward", s);
+        trsv_fused_forward(gp->K.ptr, gp->ld, gp->Linv.ptr, gp->n, gp->alpha.ptr, gp->flags.ptr, gp->trsv_b.ptr,
+                           gp->status.ptr, s);
+    }
+    StepScope step("backward", s);
     trsv_fused_backward(gp->K.ptr, gp->ld, gp->Linv.ptr, gp->n, gp->alpha.ptr, gp->flags.ptr, gp->trsv_b.ptr,
                         gp->status.ptr, s);
 }
@@ -216,6 +224,7 @@ void fit(gprat_cu_gp *gp, cudaStream_t s)
     if (mixed(gp))
     {
         factor_mixed(gp, s);
+        StepScope step("alpha refinement", s);
         alpha_mixed(gp, s);
     }
     else
@@ -227,6 +236,7 @@ void fit(gprat_cu_gp *gp, cudaStream_t s)
 
 void loss_after_fit(gprat_cu_gp *gp, cudaStream_t s)
 {
+    StepScope step("loss", s);
     if (mixed(gp))
     {
         loss_mixed(gp, s);
@@ -293,6 +303,7 @@ void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     gp->mean_part.ensure(static_cast<int64_t>(m) * parts);
     if (d_var == nullptr)
     {
+        StepScope step("prediction", s);
         assemble_cross(d_xt, m, gp->x.ptr, gp->n, gp->d, gp->params.ptr, nullptr, 0, gp->alpha.ptr,
                        gp->mean_part.ptr, parts, s, row_offsets);
         reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
@@ -300,11 +311,18 @@ void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     }
     gp->W.ensure(static_cast<int64_t>(m) * gp->ld);
     gp->vacc.ensure(m);
-    assemble_cross(d_xt, m, gp->x.ptr, gp->n, gp->d, gp->params.ptr, gp->W.ptr, gp->ld, gp->alpha.ptr,
-                   gp->mean_part.ptr, parts, s, row_offsets);
-    reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
-    GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->vacc.ptr, 0, m * sizeof(double), s));
-    solve_right_lt(gp, gp->W.ptr, gp->ld, m, gp->vacc.ptr, [m](int) { return m; }, s);
+    {
+        StepScope step("prediction", s);
+        assemble_cross(d_xt, m, gp->x.ptr, gp->n, gp->d, gp->params.ptr, gp->W.ptr, gp->ld, gp->alpha.ptr,
+                       gp->mean_part.ptr, parts, s, row_offsets);
+        reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
+    }
+    {
+        StepScope step("forward KcK", s);
+        GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->vacc.ptr, 0, m * sizeof(double), s));
+        solve_right_lt(gp, gp->W.ptr, gp->ld, m, gp->vacc.ptr, [m](int) { return m; }, s);
+    }
+    StepScope step("prediction uncertainty", s);
     finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, s);
 }
 
@@ -566,6 +584,7 @@ int gprat_cu_cholesky(gprat_cu_gp *gp, const double hyper[3], double *tiles_out)
             check_gp(gp);
             require(tiles_out != nullptr, "output must not be NULL");
             DeviceGuard guard(gp->device);
+            StepPrefix prefix("cholesky_step");
             upload_hyper(gp, hyper, gp->stream);
             factor_fp64(gp, gp->stream);
             std::vector<double> full(static_cast<size_t>(gp->n) * gp->ld);
@@ -605,6 +624,7 @@ int gprat_cu_predict(gprat_cu_gp *gp, const double hyper[3], const double *test_
             const int m = m_tiles * m_tile_size;
             require(mean != nullptr || m == 0, "mean output must not be NULL");
             DeviceGuard guard(gp->device);
+            StepPrefix prefix("predict_step");
             upload_hyper(gp, hyper, gp->stream);
             upload_test(gp, test_in, n_test_in, m);
             gp->mean.ensure(std::max(m, 1));
@@ -616,7 +636,7 @@ int gprat_cu_predict(gprat_cu_gp *gp, const double hyper[3], const double *test_
 }
 
 static int predict_var_common(gprat_cu_gp *gp, const double hyper[3], const double *test_in, int64_t n_test_in,
-                              int m_tiles, int m_tile_size, double *mean, double *var)
+                              int m_tiles, int m_tile_size, double *mean, double *var, const char *step_prefix)
 {
     return guarded(
         [&]
@@ -626,6 +646,7 @@ static int predict_var_common(gprat_cu_gp *gp, const double hyper[3], const doub
             const int m = m_tiles * m_tile_size;
             require((mean != nullptr && var != nullptr) || m == 0, "outputs must not be NULL");
             DeviceGuard guard(gp->device);
+            StepPrefix prefix(step_prefix);
             upload_hyper(gp, hyper, gp->stream);
             upload_test(gp, test_in, n_test_in, m);
             gp->mean.ensure(std::max(m, 1));
@@ -641,13 +662,13 @@ static int predict_var_common(gprat_cu_gp *gp, const double hyper[3], const doub
 int gprat_cu_predict_with_uncertainty(gprat_cu_gp *gp, const double hyper[3], const double *test_in,
                                       int64_t n_test_in, int m_tiles, int m_tile_size, double *mean, double *var)
 {
-    return predict_var_common(gp, hyper, test_in, n_test_in, m_tiles, m_tile_size, mean, var);
+    return predict_var_common(gp, hyper, test_in, n_test_in, m_tiles, m_tile_size, mean, var, "predict_uncer_step");
 }
 
 int gprat_cu_predict_with_full_cov(gprat_cu_gp *gp, const double hyper[3], const double *test_in, int64_t n_test_in,
                                    int m_tiles, int m_tile_size, double *mean, double *var)
 {
-    return predict_var_common(gp, hyper, test_in, n_test_in, m_tiles, m_tile_size, mean, var);
+    return predict_var_common(gp, hyper, test_in, n_test_in, m_tiles, m_tile_size, mean, var, "predict_full_cov_step");
 }
 
 int gprat_cu_predict_full_covariance(gprat_cu_gp *gp, const double hyper[3], const double *test_in,

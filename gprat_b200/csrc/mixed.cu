@@ -395,7 +395,11 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
     auto evR = [&](int k) { return gp->events[1 + nout + k]; };
     const int sms = device_sm_count();
 
-    assemble_covariance(gp->x.ptr, n, gp->d, gp->T, gp->params.ptr, gp->K.ptr, gp->ld, s, gp->K32.ptr, ld32);
+    {
+        StepScope step("assembly", s);
+        assemble_covariance(gp->x.ptr, n, gp->d, gp->T, gp->params.ptr, gp->K.ptr, gp->ld, s, gp->K32.ptr, ld32);
+    }
+    StepScope step("cholesky", s);
     GPRAT_CUDA_CHECK(cudaEventRecord(gp->events[0], s));
     GPRAT_CUDA_CHECK(cudaStreamWaitEvent(side, gp->events[0], 0));
     const MixedOps ops = make_ops(gp);
@@ -566,13 +570,17 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
         gp->Wb.ensure(static_cast<int64_t>(m) * ld32);
     }
     float *W = gp->W32.ptr;
-    assemble_cross_f32(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, W, ld32, gp->alpha.ptr, gp->mean_part.ptr,
-                       parts, s, row_offsets);
-    reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
+    {
+        StepScope step("prediction", s);
+        assemble_cross_f32(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, W, ld32, gp->alpha.ptr, gp->mean_part.ptr,
+                           parts, s, row_offsets);
+        reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
+    }
     if (d_var == nullptr)
     {
         return;
     }
+    StepScope step("forward KcK", s);
     GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->vacc.ptr, 0, 2 * m * sizeof(double), s));
     const MixedOps ops = make_ops(gp);
     TcOperand opW, opWb;

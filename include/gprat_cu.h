@@ -238,6 +238,21 @@ int gprat_cu_stats_enable_timing(int enable);
 int gprat_cu_stats_read(int64_t *launches, int64_t *gemm_launches, double *gemm_ms, double *gemm_flops);
 
 /*
+ * Per-phase step timers, the counterpart of the reference's APEX step timers
+ * (GPRAT_START_STEP / GPRAT_END_STEP, core/include/apex_utils.hpp:19-54) with
+ * the same labels ("predict_uncer_step cholesky", "cholesky_step assembly",
+ * ..., core/src/cpu/gp_functions.cpp:29-678) plus "... alpha refinement" for
+ * the mixed-precision alpha and "... loss".  When enabled, every phase of
+ * every call is bracketed by CUDA events on the stream that runs it (device
+ * time; the look-ahead's side stream is included in "cholesky").
+ * gprat_cu_steps_csv writes "label,calls,total_ms,mean_ms" rows (NUL
+ * terminated, truncated to cap) and the size it needs into *needed.
+ */
+int gprat_cu_steps_enable(int enable);
+int gprat_cu_steps_reset(void);
+int gprat_cu_steps_csv(char *buf, int64_t cap, int64_t *needed);
+
+/*
  * Kernel-level test entry (no counterpart in the reference): runs the
  * tcgen05 tensor-core GEMM of the mixed-precision path on the current
  * device, C = beta*C + alpha * A B^T with host buffers A (M x K, lda),
