@@ -61,18 +61,62 @@ def synthetic(n, m, d):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+    """SM clocks and clock-event reasons of the bench's GPU, sampled DURING the
+    timed region. NVML is read from a thread every 10 ms (read-only queries; the
+    device is found by its UUID, so CUDA_VISIBLE_DEVICES remapping cannot point
+    the sampler at another GPU). Without NVML the fallback is `nvidia-smi -lms 200`,
+    started early enough that its first sample exists before timing begins."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.device)
+        try:
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(props.uuid))
+        except Exception:
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def _poll(self, nv, h):
+        bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(mx), [self.NAMES[i] for i, b in enumerate(bits) if r & b]))
+            except Exception:
+                pass
+            self.stop.wait(0.01)
 
     def __enter__(self):
+        import threading
+
+        try:
+            nv, h = self._nvml_handle()
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.thread.start()
+            self.source = "nvml 10 ms"
+            return self
+        except Exception:
+            self.thread = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -80,11 +124,18 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(self.device)], stdout=self.out,
                                          stderr=subprocess.DEVNULL)
+            self.source = "nvidia-smi 200 ms"
+            t0 = time.time()
+            while time.time() - t0 < 10 and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
 
     def __exit__(self, *exc):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -95,23 +146,25 @@ class ClockSampler:
             self.out.close()
 
     def summary(self):
-        if self.proc is None or self.path is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        rows = []
-        with open(self.path) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        if self.thread is None:
+            if self.proc is None or self.path is None:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+            with open(self.path) as f:
+                for line in f:
+                    p = [x.strip() for x in line.split(",")]
+                    if len(p) >= 9 and p[1].replace(".", "").isdigit():
+                        mx = float(p[2]) if p[2].replace(".", "").isdigit() else None
+                        self.rows.append((float(p[1]), mx,
+                                          [self.NAMES[i] for i in range(4) if p[5 + i].lower() == "active"]))
+            os.unlink(self.path)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0,
+                    "source": self.source}
+        sm = [r[0] for r in self.rows]
+        mx = [r[1] for r in self.rows if r[1] is not None]
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted({n for r in self.rows for n in r[2]}), "samples": len(self.rows),
+                "source": self.source}
 
 
 def max_over_ranks(value: float, dist, device) -> float:

@@ -651,8 +651,15 @@ static int predict_var_common(gprat_cu_gp *gp, const double hyper[3], const doub
             upload_test(gp, test_in, n_test_in, m);
             gp->mean.ensure(std::max(m, 1));
             gp->var.ensure(std::max(m, 1));
-            fit(gp, gp->stream);
-            predict_device(gp, gp->xt.ptr, m, gp->mean.ptr, gp->var.ptr, gp->stream);
+            if (mixed(gp))
+            {
+                fit_predict_mixed(gp, gp->xt.ptr, m, gp->mean.ptr, gp->var.ptr, gp->stream);
+            }
+            else
+            {
+                fit(gp, gp->stream);
+                predict_device(gp, gp->xt.ptr, m, gp->mean.ptr, gp->var.ptr, gp->stream);
+            }
             download(gp, mean, gp->mean.ptr, m);
             download(gp, var, gp->var.ptr, m);
             finish_and_check(gp);

@@ -151,7 +151,8 @@ namespace gprat_cu
 void factor_mixed(gprat_cu_gp *gp, cudaStream_t s);
 void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s);
 void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s,
-                    const int64_t *row_offsets = nullptr);
+                    const int64_t *row_offsets = nullptr, int max_ctas = 0);
+void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s);
 
 // gp.cu: internal entry points for the serving layer (serve.cu)
 void gp_fit(gprat_cu_gp *gp, const double hyper[3], cudaStream_t s);

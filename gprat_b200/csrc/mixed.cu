@@ -21,6 +21,7 @@
 #include "gp_state.cuh"
 
 #include <cmath>
+#include <cstdlib>
 #include <string>
 
 namespace gprat_cu
@@ -333,7 +334,23 @@ namespace
 #ifndef GPRAT_LOOKAHEAD_MAIN_PERCENT
 #define GPRAT_LOOKAHEAD_MAIN_PERCENT 70
 #endif
-constexpr int MAIN_PERCENT = GPRAT_LOOKAHEAD_MAIN_PERCENT;
+
+// A share of the SMs in percent: the environment variable `name` if it holds
+// an integer in [10, 100], else the compiled default (a tuning knob).
+int sm_percent(const char *name, int dflt)
+{
+    const char *v = std::getenv(name);
+    if (v != nullptr)
+    {
+        char *end = nullptr;
+        const long p = std::strtol(v, &end, 10);
+        if (end != v && *end == '\0' && p >= 10 && p <= 100)
+        {
+            return static_cast<int>(p);
+        }
+    }
+    return dflt;
+}
 
 void ensure_lookahead(gprat_cu_gp *gp, int nevents)
 {
@@ -365,7 +382,7 @@ TcGemmArgs limited(TcGemmArgs a, int max_ctas)
 //     panel solves and the in-panel updates on tcgen05), then apply panel k
 //     to the columns of panel k+1 and factor panel k+1;
 //   main stream: the trailing update of everything right of panel k+1 with
-//     panel k (the bulk of the flops), on MAIN_PERCENT % of the SMs while the
+//     panel k (the bulk of the flops), on GPRAT_LOOKAHEAD_MAIN_PERCENT % of the SMs while the
 //     side stream works next to it (the panel chain is the critical path).
 // Events order the two streams: panel k+1's columns are written by the
 // update of panel k-1 (main) before the side stream touches them, and the
@@ -394,6 +411,7 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
     auto evF = [&](int k) { return gp->events[1 + k]; };
     auto evR = [&](int k) { return gp->events[1 + nout + k]; };
     const int sms = device_sm_count();
+    const int main_percent = sm_percent("GPRAT_CU_LOOKAHEAD_MAIN_PERCENT", GPRAT_LOOKAHEAD_MAIN_PERCENT);
 
     {
         StepScope step("assembly", s);
@@ -468,7 +486,7 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
             tc_gemm(ops.trail(), ops.trail(),
                     limited(tc_args(rest, rest, bo, next_end, K0, next_end, K0, at(next_end, next_end), ld32, -1.0f,
                                     1.0f, true, nullptr, gp->status.ptr),
-                            ahead ? std::max(1, sms * MAIN_PERCENT / 100) : 0),
+                            ahead ? std::max(1, sms * main_percent / 100) : 0),
                     s);
         }
         GPRAT_CUDA_CHECK(cudaEventRecord(evR(k), s));
@@ -555,8 +573,64 @@ void loss_mixed(gprat_cu_gp *gp, cudaStream_t s)
     loss_kernel(gp->y.ptr, gp->alpha.ptr, gp->D64.ptr + NB * NB, 0, gp->n, gp->params.ptr, s);
 }
 
+namespace
+{
+
+// Operands and buffers of one variance solve W L^T = K* (in place in W).
+struct VarianceSolve
+{
+    gprat_cu_gp *gp;
+    MixedOps ops;
+    TcOperand opW;   // W (TF32 view)
+    TcOperand opWb;  // BF16 copy of the solved columns of W (MIXED_BF16)
+    float *W;
+    int64_t ld32;
+    int m;
+    int max_ctas;
+    cudaStream_t s;
+
+    const TcOperand &wt() const { return ops.bf16 ? opWb : opW; }
+
+    // W[:, c0:c1) := W[:, c0:c1) L[c0:c1, c0:c1)^-T, for columns that already
+    // hold every update from the columns left of c0.  Recursive halving: the
+    // update between the halves is one GEMM of depth (mid - c0), so each
+    // level of the recursion reads and writes W once (the K = 512 outer
+    // panels of the factorisation would read and write it n / 512 times).
+    void solve(int c0, int c1) const
+    {
+        if (c1 - c0 <= NB)
+        {
+            const int k = c0 / NB;
+            tc_gemm(opW, ops.Linv,
+                    limited(tc_args(m, NB, NB, 0, c0, k * NB, 0, W + c0, ld32, 1.0f, 0.0f, false, gp->vacc.ptr,
+                                    gp->status.ptr),
+                            max_ctas),
+                    s);
+            if (ops.bf16)
+            {
+                convert_f32_to_bf16(W + c0, ld32, gp->Wb.ptr + c0, ld32, m, NB, s);
+            }
+            return;
+        }
+        const int mid = c0 + ((c1 - c0) / NB / 2) * NB;
+        solve(c0, mid);
+        tc_gemm(wt(), ops.trail(),
+                limited(tc_args(m, c1 - mid, mid - c0, 0, c0, mid, c0, W + mid, ld32, -1.0f, 1.0f, false, nullptr,
+                                gp->status.ptr),
+                        max_ctas),
+                s);
+        solve(mid, c1);
+    }
+};
+
+}  // namespace
+
+// Mean (when d_mean != nullptr, from the refined alpha) and variance (when
+// d_var != nullptr) for m test points.  max_ctas bounds the grid of the
+// variance solve's GEMMs (0: every SM), so that another stream can run next
+// to it.
 void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s,
-                    const int64_t *row_offsets)
+                    const int64_t *row_offsets, int max_ctas)
 {
     const int n = gp->n;
     const int64_t ld32 = gp->ld32;
@@ -572,9 +646,13 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     float *W = gp->W32.ptr;
     {
         StepScope step("prediction", s);
-        assemble_cross_f32(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, W, ld32, gp->alpha.ptr, gp->mean_part.ptr,
-                           parts, s, row_offsets);
-        reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
+        assemble_cross_f32(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, W, ld32,
+                           d_mean != nullptr ? gp->alpha.ptr : nullptr,
+                           d_mean != nullptr ? gp->mean_part.ptr : nullptr, parts, s, row_offsets);
+        if (d_mean != nullptr)
+        {
+            reduce_mean(gp->mean_part.ptr, m, parts, d_mean, s);
+        }
     }
     if (d_var == nullptr)
     {
@@ -582,48 +660,58 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     }
     StepScope step("forward KcK", s);
     GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->vacc.ptr, 0, 2 * m * sizeof(double), s));
-    const MixedOps ops = make_ops(gp);
-    TcOperand opW, opWb;
-    tc_make_operand(opW, W, m, static_cast<int>(ld32), ld32, TcKind::TF32);
+    VarianceSolve v{ gp, make_ops(gp), {}, {}, W, ld32, m, max_ctas, s };
+    tc_make_operand(v.opW, W, m, static_cast<int>(ld32), ld32, TcKind::TF32);
     if (bf16)
     {
-        tc_make_operand(opWb, gp->Wb.ptr, m, static_cast<int>(ld32), ld32, TcKind::BF16);
+        tc_make_operand(v.opWb, gp->Wb.ptr, m, static_cast<int>(ld32), ld32, TcKind::BF16);
     }
-    const TcOperand &opWt = bf16 ? opWb : opW;
-    for (int K0 = 0; K0 < n; K0 += NBO)
-    {
-        const int bo = std::min(NBO, n - K0);
-        const int pend = K0 + bo;
-        for (int c0 = K0; c0 < pend; c0 += NB)
-        {
-            const int k = c0 / NB;
-            tc_gemm(opW, ops.Linv,
-                    tc_args(m, NB, NB, 0, c0, k * NB, 0, W + c0, ld32, 1.0f, 0.0f, false, gp->vacc.ptr,
-                            gp->status.ptr),
-                    s);
-            if (bf16)
-            {
-                convert_f32_to_bf16(W + c0, ld32, gp->Wb.ptr + c0, ld32, m, NB, s);
-            }
-            const int ncols = pend - (c0 + NB);
-            if (ncols > 0)
-            {
-                tc_gemm(opWt, ops.trail(),
-                        tc_args(m, ncols, NB, 0, c0, c0 + NB, c0, W + c0 + NB, ld32, -1.0f, 1.0f, false, nullptr,
-                                gp->status.ptr),
-                        s);
-            }
-        }
-        const int rest = n - pend;
-        if (rest > 0)
-        {
-            tc_gemm(opWt, ops.trail(),
-                    tc_args(m, rest, bo, 0, K0, pend, K0, W + pend, ld32, -1.0f, 1.0f, false, nullptr,
-                            gp->status.ptr),
-                    s);
-        }
-    }
+    v.solve(0, n);
     finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, s, gp->vacc.ptr + m);
+}
+
+// Share of the SMs the variance solve's GEMMs hold while alpha is refined
+// next to them (the refinement's solves are latency-bound and need few SMs).
+#ifndef GPRAT_VARIANCE_PERCENT
+#define GPRAT_VARIANCE_PERCENT 75
+#endif
+
+// Fit, mean and variance (predict_with_uncertainty).  After the
+// factorisation the two remaining halves are independent: the variance solve
+// needs only the factor, alpha's refinement needs only the factor and K.  So
+// the variance solve's GEMMs run on `s` with GPRAT_VARIANCE_PERCENT % of the
+// SMs while the high-priority side stream refines alpha (FP64 PCG) and forms
+// the mean from it.  The side stream joins `s` at the end.
+void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
+{
+    factor_mixed(gp, s);
+    const int nout = ceil_div(gp->n, NBO);
+    ensure_lookahead(gp, 2 * nout + 3);
+    cudaEvent_t factored = gp->events[2 * nout + 1], refined = gp->events[2 * nout + 2];
+    cudaStream_t side = gp->side;
+    const int parts = ceil_div(gp->n, 128);
+    gp->mean_part.ensure(static_cast<int64_t>(std::max(m, 1)) * parts);
+    GPRAT_CUDA_CHECK(cudaEventRecord(factored, s));
+    GPRAT_CUDA_CHECK(cudaStreamWaitEvent(side, factored, 0));
+    if (m > 0)
+    {
+        variance_mixed(gp, d_xt, m, nullptr, d_var, s, nullptr,
+                       std::max(1, device_sm_count() *
+                                       sm_percent("GPRAT_CU_VARIANCE_PERCENT", GPRAT_VARIANCE_PERCENT) / 100));
+    }
+    {
+        StepScope step("alpha refinement", side);
+        alpha_mixed(gp, side);
+    }
+    if (m > 0)
+    {
+        StepScope step("prediction", side);
+        assemble_cross(d_xt, m, gp->x.ptr, gp->n, gp->d, gp->params.ptr, nullptr, 0, gp->alpha.ptr,
+                       gp->mean_part.ptr, parts, side, nullptr);
+        reduce_mean(gp->mean_part.ptr, m, parts, d_mean, side);
+    }
+    GPRAT_CUDA_CHECK(cudaEventRecord(refined, side));
+    GPRAT_CUDA_CHECK(cudaStreamWaitEvent(s, refined, 0));
 }
 
 }  // namespace gprat_cu
