@@ -36,7 +36,7 @@ constexpr int XS = SB + 4;                // smem row stride of a sub-block inve
 constexpr int TS = 3 * SB + 4;            // smem row stride of the assembly temporary
 constexpr int PTHREADS = 256;
 constexpr int NWARPS = PTHREADS / 32;
-constexpr size_t SMEM_DOUBLES = PB * PS + 4 * SB * XS + PB + SB * TS + SB;
+constexpr size_t SMEM_DOUBLES = PB * PS + 4 * SB * XS + PB + SB * TS + 2 * SB;
 
 template <typename T>
 struct PairOf;
@@ -91,8 +91,11 @@ __device__ __forceinline__ void frag_b(double (&b)[2], const double *M, int ld, 
 // updates are unconditional: a lane's entries above the diagonal (and window
 // slots past column 31) receive values that are never read, which keeps the
 // warp converged (per-lane conditional updates compile to divergent branches
-// that cost more than the arithmetic).  colbuf (32 doubles) broadcasts the
-// new column of L.
+// that cost more than the arithmetic).  colbuf (2 x 32 doubles, alternating by
+// pivot, so one __syncwarp per pivot suffices) broadcasts the new column of L.
+// The next pivot's lane computes its updated diagonal a_j+1,j+1 - l^2 from its
+// own l before the broadcast, and the next pivot's shuffle and rsqrt are
+// issued before the column update, so their latency overlaps it.
 constexpr int CHUNK = 8;  // pivots per unrolled chunk of the diagonal factorisation
 
 __device__ __forceinline__ void diag_factor_invert(double *a, int c0, int bs, int row0, int *bad, double *dinv,
@@ -109,6 +112,8 @@ __device__ __forceinline__ void diag_factor_invert(double *a, int c0, int bs, in
         }
     }
     int first_bad = 0;
+    double ajj = __shfl_sync(0xffffffffu, r[0], 0);  // the current pivot's updated diagonal entry
+    double inv = rsqrt(ajj);
 #pragma unroll 1
     for (int j0 = 0; j0 < SB; j0 += CHUNK)
     {
@@ -116,24 +121,27 @@ __device__ __forceinline__ void diag_factor_invert(double *a, int c0, int bs, in
         for (int jj = 0; jj < CHUNK; ++jj)
         {
             const int j = j0 + jj;
-            const double ajj = __shfl_sync(0xffffffffu, r[jj], j);
+            double *cb = colbuf + (jj & 1) * SB;
             first_bad = (first_bad == 0 && !(ajj > 0.0) && c0 + j < bs) ? row0 + c0 + j + 1 : first_bad;
-            const double inv = rsqrt(ajj);
             const double l = (lane == j) ? ajj * inv : r[jj] * inv;  // L[lane][j] for lane >= j
-            colbuf[lane] = l;
+            const double dnext = r[jj + 1] - l * l;                  // lane j+1: the next pivot
+            cb[lane] = l;
             a[(c0 + lane) * PS + c0 + j] = l;  // above the diagonal: a value nobody reads
             if (lane == 0)
             {
                 dinv[j] = inv;
             }
             __syncwarp();
+            // the next pivot's shuffle and rsqrt are independent of the column
+            // update below and overlap it (after the last pivot they are unused)
+            ajj = __shfl_sync(0xffffffffu, dnext, (j + 1) & (SB - 1));
+            inv = rsqrt(ajj);
             // window slot c is column j0 + c; slots past column 31 are never read
 #pragma unroll
             for (int c = jj + 1; c < SB; ++c)
             {
-                r[c] -= l * colbuf[(j0 + c) & (SB - 1)];
+                r[c] -= l * cb[(j0 + c) & (SB - 1)];
             }
-            __syncwarp();
         }
 #pragma unroll
         for (int c = 0; c < SB - CHUNK; ++c)
@@ -154,35 +162,36 @@ __device__ __forceinline__ void diag_factor_invert(double *a, int c0, int bs, in
 
 // All 8 warps: X = L^-1 of the factored 32 x 32 sub-block at (c0, c0), zero
 // above the diagonal, into xinv.  Warp w solves columns 4w .. 4w+3; lane i owns
-// row i (its row of L in registers) and the four columns' x_i.  Step k
-// broadcasts x_k (final once scaled by 1/L_kk) and every lane below updates.
-// Fully unrolled (32 short steps) and branch-free.
+// row i and the four columns' x_i.  The system is scaled to a unit diagonal
+// first (row i of L and of the right-hand side times 1/L_ii), so step k is one
+// shuffle of the final x_k and one FMA on the lanes below (their strictly
+// lower entries; every other coefficient is zero).  Fully unrolled (32 short
+// steps) and branch-free.
 __device__ __forceinline__ void diag_inverse_all_warps(const double *a, int c0, const double *dinv, double *xinv)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double lrow[SB];
     const double *arow = a + (c0 + lane) * PS + c0;
+    const double di = dinv[lane];
 #pragma unroll
     for (int c = 0; c < SB; ++c)
     {
-        lrow[c] = arow[c];  // above the diagonal: never used (lane > k selects)
+        lrow[c] = (c < lane) ? arow[c] * di : 0.0;
     }
     double x[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
     {
-        x[q] = (lane == 4 * warp + q) ? 1.0 : 0.0;
+        x[q] = (lane == 4 * warp + q) ? di : 0.0;
     }
 #pragma unroll
     for (int k = 0; k < SB; ++k)
     {
-        const double dk = dinv[k];
 #pragma unroll
         for (int q = 0; q < 4; ++q)
         {
-            const double xk = __shfl_sync(0xffffffffu, x[q], k) * dk;
-            const double upd = x[q] - lrow[k] * xk;
-            x[q] = (lane == k) ? xk : ((lane > k) ? upd : x[q]);
+            const double xk = __shfl_sync(0xffffffffu, x[q], k);
+            x[q] -= lrow[k] * xk;
         }
     }
 #pragma unroll
@@ -190,6 +199,78 @@ __device__ __forceinline__ void diag_inverse_all_warps(const double *a, int c0, 
     {
         xinv[lane * XS + 4 * warp + q] = x[q];
     }
+}
+
+__device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, int bytes)
+{
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gmem), "r"(bytes) : "memory");
+}
+
+// Offset (in 16-byte chunks) of row i in the packed FP32 staging of a lower
+// triangle whose row r holds r / 4 + 1 chunks (columns 0 .. 4 (r / 4) + 3).
+__device__ __forceinline__ int staged_row_chunks(int i)
+{
+    const int q = i >> 2, r = i & 3;
+    return (q + 1) * (2 * q + r);
+}
+
+// Loads the lower triangle of the block (rows < bs) with 16-byte cp.async
+// copies, then pads: the strict upper triangle is zero and rows >= bs are
+// identity rows.  Needs A and lda * sizeof(T) 16-byte aligned.  Every copy
+// stops at column i of its row (the rest of the chunk is zero-filled), so
+// nothing right of the block's diagonal is read.
+//   FP64: rows go straight to their place in sa;
+//   FP32: rows are packed into `stage` (2112 chunks, 33 KB), then widened.
+template <typename T>
+__device__ __forceinline__ void load_lower_async(const T *__restrict__ A, int64_t lda, int bs, double *sa,
+                                                 double *stage)
+{
+    constexpr int CH = 16 / sizeof(T);  // elements per chunk
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float *st32 = reinterpret_cast<float *>(stage);
+    for (int i = warp; i < bs; i += NWARPS)
+    {
+        const int nchunks = i / CH + 1;
+        for (int k = lane; k < nchunks; k += 32)
+        {
+            const int c = k * CH;
+            const int bytes = min(CH, i + 1 - c) * static_cast<int>(sizeof(T));
+            void *dst = (sizeof(T) == 8) ? static_cast<void *>(sa + i * PS + c)
+                                         : static_cast<void *>(st32 + 4 * (staged_row_chunks(i) + k));
+            cp_async16_zfill(dst, A + static_cast<int64_t>(i) * lda + c, bytes);
+        }
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+    for (int q = threadIdx.x; q < PB * PB / 2; q += PTHREADS)
+    {
+        const int i = q >> 6, c = 2 * (q & 63);
+        double v0 = (i == c) ? 1.0 : 0.0, v1 = (i == c + 1) ? 1.0 : 0.0;
+        if (i < bs && c <= i)
+        {
+            if (sizeof(T) == 8)
+            {
+                const double2 w = *reinterpret_cast<const double2 *>(sa + i * PS + c);
+                v0 = w.x;
+                v1 = (c + 1 <= i) ? w.y : 0.0;
+            }
+            else
+            {
+                const float *row = st32 + 4 * staged_row_chunks(i);
+                v0 = static_cast<double>(row[c]);
+                v1 = (c + 1 <= i) ? static_cast<double>(row[c + 1]) : 0.0;
+            }
+        }
+        *reinterpret_cast<double2 *>(sa + i * PS + c) = make_double2(v0, v1);
+    }
+}
+
+// True when the block and its rows start on 16-byte boundaries.
+template <typename T>
+__device__ __forceinline__ bool aligned16(const T *A, int64_t lda)
+{
+    return ((reinterpret_cast<uintptr_t>(A) | static_cast<uintptr_t>(lda * sizeof(T))) & 15) == 0;
 }
 
 // T: element type of the block in global memory (FP64, or FP32 for the
@@ -205,7 +286,7 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
     double *xall = sa + PB * PS;    // 4 x [SB][XS] sub-block inverses
     double *dinv = xall + 4 * SB * XS;       // [PB] pivot reciprocals
     double *tbuf = dinv + PB;                // [SB][TS]
-    double *colbuf = tbuf + SB * TS;         // [SB] column broadcast of the diagonal factorisation
+    double *colbuf = tbuf + SB * TS;         // [2][SB] column broadcast of the diagonal factorisation
     __shared__ int bad;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -214,38 +295,18 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
     {
         bad = 0;
     }
-    // load the lower triangle in pairs of columns (one 8- or 16-byte load each,
-    // all issued before the first store); pad with the identity beyond bs
+    if (aligned16(A, lda))
     {
-        using Pair = typename PairOf<T>::type;
-        double v0[PB * PB / 2 / PTHREADS], v1[PB * PB / 2 / PTHREADS];
-#pragma unroll
-        for (int q = 0; q < PB * PB / 2 / PTHREADS; ++q)
+        load_lower_async(A, lda, bs, sa, xall);
+    }
+    else
+    {
+        // unaligned block: element loads of the lower triangle, identity padding
+        for (int q = tid; q < PB * PB; q += PTHREADS)
         {
-            const int idx = q * PTHREADS + tid;
-            const int i = idx >> 6, c = 2 * (idx & 63);
-            const T *src = A + static_cast<int64_t>(i) * lda + c;
-            double a0 = (i == c) ? 1.0 : 0.0, a1 = (i == c + 1) ? 1.0 : 0.0;
-            if (i < bs && c + 1 <= i)
-            {
-                const Pair w = *reinterpret_cast<const Pair *>(src);
-                a0 = static_cast<double>(w.x);
-                a1 = static_cast<double>(w.y);
-            }
-            else if (i < bs && c == i)
-            {
-                a0 = static_cast<double>(src[0]);
-                a1 = 0.0;
-            }
-            v0[q] = a0;
-            v1[q] = a1;
-        }
-#pragma unroll
-        for (int q = 0; q < PB * PB / 2 / PTHREADS; ++q)
-        {
-            const int idx = q * PTHREADS + tid;
-            const int i = idx >> 6, c = 2 * (idx & 63);
-            *reinterpret_cast<double2 *>(sa + i * PS + c) = make_double2(v0[q], v1[q]);
+            const int i = q >> 7, c = q & (PB - 1);
+            sa[i * PS + c] = (i < bs && c <= i) ? static_cast<double>(A[static_cast<int64_t>(i) * lda + c])
+                                                : ((i == c) ? 1.0 : 0.0);
         }
     }
     __syncthreads();
@@ -349,7 +410,9 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
     {
         atomicCAS(&status->not_spd_row, 0, bad);
     }
-    // write L (lower triangle incl. diagonal) back, in pairs of columns
+    // write L (lower triangle incl. diagonal) back: in pairs of columns when
+    // the block is 16-byte aligned, else element by element
+    if (aligned16(A, lda))
     {
         using Pair = typename PairOf<T>::type;
 #pragma unroll 8
@@ -369,6 +432,17 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
             else if (i < bs && c == i)
             {
                 dst[0] = static_cast<T>(v.x);
+            }
+        }
+    }
+    else
+    {
+        for (int q = tid; q < PB * PB; q += PTHREADS)
+        {
+            const int i = q >> 7, c = q & (PB - 1);
+            if (i < bs && c <= i)
+            {
+                A[static_cast<int64_t>(i) * lda + c] = static_cast<T>(sa[i * PS + c]);
             }
         }
     }
@@ -485,6 +559,10 @@ void potrf_diag(double *A, int64_t lda, int bs, int row0, double *Linv, int64_t 
     {
         throw Error(1, "potrf_diag: block size must be in [1, 128]");
     }
+    if ((ldi & 1) != 0 || (reinterpret_cast<uintptr_t>(Linv) & 15) != 0)
+    {
+        throw Error(1, "potrf_diag: Linv must be 16-byte aligned with an even leading dimension");
+    }
     constexpr size_t smem = SMEM_DOUBLES * sizeof(double);
     ensure_smem_attr(reinterpret_cast<const void *>(potrf_inv_kernel<double>), static_cast<int>(smem));
     potrf_inv_kernel<double><<<1, PTHREADS, smem, s>>>(A, lda, bs, row0, Linv, ldi, nullptr, 0, nullptr, status);
@@ -497,6 +575,11 @@ void potrf_diag_f32(float *A, int64_t lda, int bs, int row0, double *Linv, int64
     if (bs <= 0 || bs > PB)
     {
         throw Error(1, "potrf_diag_f32: block size must be in [1, 128]");
+    }
+    if ((ldi & 1) != 0 || (ldi32 & 1) != 0 || (reinterpret_cast<uintptr_t>(Linv) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(Linv32) & 7) != 0)
+    {
+        throw Error(1, "potrf_diag_f32: Linv / Linv32 must be aligned with even leading dimensions");
     }
     constexpr size_t smem = SMEM_DOUBLES * sizeof(double);
     ensure_smem_attr(reinterpret_cast<const void *>(potrf_inv_kernel<float>), static_cast<int>(smem));
