@@ -94,6 +94,24 @@ bool gemm_timing_enabled();
 void gemm_timing_begin(cudaStream_t s);
 void gemm_timing_end(cudaStream_t s, double flops);
 
+// Programmatic dependent launch.  A kernel launched with
+// programmatic_launch_attr() may start while the kernel before it in the
+// stream is still running: it does its set-up (barriers, TMEM, descriptor
+// prefetch), then pdl_wait() blocks until that kernel has completed and its
+// memory is visible.  Every such kernel calls pdl_wait() before its first
+// access to global memory; pdl_launch_dependents() lets the next kernel's
+// set-up start.  Dependencies on events or other streams are unaffected.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+inline cudaLaunchAttribute programmatic_launch_attr()
+{
+    cudaLaunchAttribute a = {};
+    a.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    a.val.programmaticStreamSerializationAllowed = 1;
+    return a;
+}
+
 // Raises the dynamic shared-memory limit of `func` on the current device to
 // at least `bytes` (remembers the largest limit set per kernel and device).
 inline void ensure_smem_attr(const void *func, int bytes)

@@ -448,23 +448,17 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
                 convert_f32_to_bf16(at(r0, r0), ld32, gp->Lb.ptr + static_cast<int64_t>(r0) * ld32 + r0, ld32,
                                     n - r0, NB, side);
             }
+            // the rest of the panel's columns, every row below the block, in one
+            // launch (the strict upper triangle of the working copy is scratch:
+            // nothing reads it, so its in-panel part is updated too)
             const int ncols = pend - (r0 + NB);
             if (ncols > 0)
             {
                 tc_gemm(ops.trail(), ops.trail(),
-                        limited(tc_args(ncols, ncols, NB, r0 + NB, r0, r0 + NB, r0, at(r0 + NB, r0 + NB), ld32, -1.0f,
-                                        1.0f, true, nullptr, gp->status.ptr),
+                        limited(tc_args(n - (r0 + NB), ncols, NB, r0 + NB, r0, r0 + NB, r0, at(r0 + NB, r0 + NB), ld32,
+                                        -1.0f, 1.0f, false, nullptr, gp->status.ptr),
                                 ctas),
                         side);
-                const int below = n - pend;
-                if (below > 0)
-                {
-                    tc_gemm(ops.trail(), ops.trail(),
-                            limited(tc_args(below, ncols, NB, pend, r0, r0 + NB, r0, at(pend, r0 + NB), ld32, -1.0f,
-                                            1.0f, false, nullptr, gp->status.ptr),
-                                    ctas),
-                            side);
-                }
             }
         }
     };
@@ -500,20 +494,14 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
         {
             GPRAT_CUDA_CHECK(cudaStreamWaitEvent(side, evR(k - 1), 0));
         }
+        // panel k+1's columns, every row from its diagonal down, in one launch
+        // (the upper triangle of its diagonal region is scratch)
         const int nb = next_end - pend;
         tc_gemm(ops.trail(), ops.trail(),
-                limited(tc_args(nb, nb, bo, pend, K0, pend, K0, at(pend, pend), ld32, -1.0f, 1.0f, true, nullptr,
-                                gp->status.ptr),
+                limited(tc_args(n - pend, nb, bo, pend, K0, pend, K0, at(pend, pend), ld32, -1.0f, 1.0f, false,
+                                nullptr, gp->status.ptr),
                         side_ctas),
                 side);
-        if (rest > 0)
-        {
-            tc_gemm(ops.trail(), ops.trail(),
-                    limited(tc_args(rest, nb, bo, next_end, K0, pend, K0, at(next_end, pend), ld32, -1.0f, 1.0f, false,
-                                    nullptr, gp->status.ptr),
-                            side_ctas),
-                    side);
-        }
         factor_panel(pend, next_end, side_ctas);
         GPRAT_CUDA_CHECK(cudaEventRecord(evF(k + 1), side));
     }

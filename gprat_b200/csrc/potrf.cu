@@ -84,25 +84,21 @@ __device__ __forceinline__ void frag_b(double (&b)[2], const double *M, int ld, 
 // Warp 0: factor the 32 x 32 sub-block at (c0, c0), write L back to smem,
 // and store the pivot reciprocals 1/L_jj in dinv[0..31].
 //
-// Branch-free, in rolled chunks of 8 pivots.  Each lane keeps a window of its
-// row in registers that shifts left by 8 columns per chunk, so every register
-// index is a compile-time constant and the code stays small (a fully unrolled
-// triangular loop outgrows the instruction cache).  The
-// updates are unconditional: a lane's entries above the diagonal (and window
-// slots past column 31) receive values that are never read, which keeps the
-// warp converged (per-lane conditional updates compile to divergent branches
-// that cost more than the arithmetic).  colbuf (2 x 32 doubles, alternating by
-// pivot, so one __syncwarp per pivot suffices) broadcasts the new column of L.
+// Lane i keeps row i in registers; fully unrolled, so every register index is
+// a compile-time constant and pivot j updates exactly the columns j+1..31.
+// Branch-free: a lane's entries above the diagonal receive values that are
+// never read, which keeps the warp converged (per-lane conditional updates
+// compile to divergent branches that cost more than the arithmetic).
+// colbuf (2 x 32 doubles, alternating by pivot, so one __syncwarp per pivot
+// suffices) broadcasts the new column of L; the update reads it in pairs.
 // The next pivot's lane computes its updated diagonal a_j+1,j+1 - l^2 from its
 // own l before the broadcast, and the next pivot's shuffle and rsqrt are
 // issued before the column update, so their latency overlaps it.
-constexpr int CHUNK = 8;  // pivots per unrolled chunk of the diagonal factorisation
-
 __device__ __forceinline__ void diag_factor_invert(double *a, int c0, int bs, int row0, int *bad, double *dinv,
                                                    double *colbuf)
 {
     const int lane = threadIdx.x & 31;
-    double r[SB];  // r[c] = A[lane][j0 + c] during chunk j0
+    double r[SB];  // r[c] = A[lane][c0 + c]
     {
         const double *arow = a + (c0 + lane) * PS + c0;
 #pragma unroll
@@ -114,44 +110,39 @@ __device__ __forceinline__ void diag_factor_invert(double *a, int c0, int bs, in
     int first_bad = 0;
     double ajj = __shfl_sync(0xffffffffu, r[0], 0);  // the current pivot's updated diagonal entry
     double inv = rsqrt(ajj);
-#pragma unroll 1
-    for (int j0 = 0; j0 < SB; j0 += CHUNK)
-    {
 #pragma unroll
-        for (int jj = 0; jj < CHUNK; ++jj)
+    for (int j = 0; j < SB; ++j)
+    {
+        double *cb = colbuf + (j & 1) * SB;
+        first_bad = (first_bad == 0 && !(ajj > 0.0) && c0 + j < bs) ? row0 + c0 + j + 1 : first_bad;
+        const double l = (lane == j) ? ajj * inv : r[j] * inv;  // L[lane][j] for lane >= j
+        cb[lane] = l;
+        a[(c0 + lane) * PS + c0 + j] = l;  // above the diagonal: a value nobody reads
+        if (lane == 0)
         {
-            const int j = j0 + jj;
-            double *cb = colbuf + (jj & 1) * SB;
-            first_bad = (first_bad == 0 && !(ajj > 0.0) && c0 + j < bs) ? row0 + c0 + j + 1 : first_bad;
-            const double l = (lane == j) ? ajj * inv : r[jj] * inv;  // L[lane][j] for lane >= j
-            const double dnext = r[jj + 1] - l * l;                  // lane j+1: the next pivot
-            cb[lane] = l;
-            a[(c0 + lane) * PS + c0 + j] = l;  // above the diagonal: a value nobody reads
-            if (lane == 0)
-            {
-                dinv[j] = inv;
-            }
+            dinv[j] = inv;
+        }
+        if (j + 1 < SB)
+        {
+            const double dnext = r[j + 1] - l * l;  // lane j+1: the next pivot
             __syncwarp();
             // the next pivot's shuffle and rsqrt are independent of the column
-            // update below and overlap it (after the last pivot they are unused)
-            ajj = __shfl_sync(0xffffffffu, dnext, (j + 1) & (SB - 1));
+            // update below and overlap it
+            ajj = __shfl_sync(0xffffffffu, dnext, j + 1);
             inv = rsqrt(ajj);
-            // window slot c is column j0 + c; slots past column 31 are never read
-#pragma unroll
-            for (int c = jj + 1; c < SB; ++c)
+            int c = j + 1;
+            if (c & 1)
             {
-                r[c] -= l * cb[(j0 + c) & (SB - 1)];
+                r[c] -= l * cb[c];
+                ++c;
             }
-        }
 #pragma unroll
-        for (int c = 0; c < SB - CHUNK; ++c)
-        {
-            r[c] = r[c + CHUNK];
-        }
-#pragma unroll
-        for (int c = SB - CHUNK; c < SB; ++c)
-        {
-            r[c] = 0.0;
+            for (; c < SB; c += 2)
+            {
+                const double2 v = *reinterpret_cast<const double2 *>(cb + c);
+                r[c] -= l * v.x;
+                r[c + 1] -= l * v.y;
+            }
         }
     }
     if (lane == 0 && first_bad != 0 && *bad == 0)
@@ -295,6 +286,8 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
     {
         bad = 0;
     }
+    pdl_wait();  // the previous kernel's results are visible from here on
+    pdl_launch_dependents();
     if (aligned16(A, lda))
     {
         load_lower_async(A, lda, bs, sa, xall);
@@ -565,7 +558,17 @@ void potrf_diag(double *A, int64_t lda, int bs, int row0, double *Linv, int64_t 
     }
     constexpr size_t smem = SMEM_DOUBLES * sizeof(double);
     ensure_smem_attr(reinterpret_cast<const void *>(potrf_inv_kernel<double>), static_cast<int>(smem));
-    potrf_inv_kernel<double><<<1, PTHREADS, smem, s>>>(A, lda, bs, row0, Linv, ldi, nullptr, 0, nullptr, status);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(PTHREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1] = { programmatic_launch_attr() };
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    GPRAT_CUDA_CHECK(cudaLaunchKernelEx(&cfg, potrf_inv_kernel<double>, A, lda, bs, row0, Linv, ldi,
+                                        static_cast<float *>(nullptr), int64_t{ 0 }, static_cast<double *>(nullptr),
+                                        status));
     GPRAT_LAUNCH_CHECK();
 }
 
@@ -583,7 +586,16 @@ void potrf_diag_f32(float *A, int64_t lda, int bs, int row0, double *Linv, int64
     }
     constexpr size_t smem = SMEM_DOUBLES * sizeof(double);
     ensure_smem_attr(reinterpret_cast<const void *>(potrf_inv_kernel<float>), static_cast<int>(smem));
-    potrf_inv_kernel<float><<<1, PTHREADS, smem, s>>>(A, lda, bs, row0, Linv, ldi, Linv32, ldi32, diag, status);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(PTHREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1] = { programmatic_launch_attr() };
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    GPRAT_CUDA_CHECK(
+        cudaLaunchKernelEx(&cfg, potrf_inv_kernel<float>, A, lda, bs, row0, Linv, ldi, Linv32, ldi32, diag, status));
     GPRAT_LAUNCH_CHECK();
 }
 

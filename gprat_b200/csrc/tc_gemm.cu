@@ -325,6 +325,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
+    pdl_wait();  // the previous kernel's results are visible from here on
+    pdl_launch_dependents();
 
     if (warp == 0)
     {
@@ -716,6 +718,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     cluster_sync_all();  // barriers of both CTAs initialised, TMEM allocated
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
+    pdl_wait();  // the previous kernel's results are visible from here on
+    pdl_launch_dependents();
 
     if (warp == 0)
     {
@@ -1117,13 +1121,14 @@ void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cud
         cfg.blockDim = dim3(NUM_THREADS);
         cfg.dynamicSmemBytes = PAIR_SMEM_BYTES;
         cfg.stream = s;
-        cudaLaunchAttribute attr[1];
+        cudaLaunchAttribute attr[2];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = 2;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
+        attr[1] = programmatic_launch_attr();
         cfg.attrs = attr;
-        cfg.numAttrs = 1;
+        cfg.numAttrs = 2;
         if (A.kind == TcKind::TF32)
         {
             ensure_smem_attr(reinterpret_cast<const void *>(tc_gemm_pair_kernel<0>), PAIR_SMEM_BYTES);
@@ -1167,7 +1172,15 @@ void tc_gemm(const TcOperand &A, const TcOperand &B, const TcGemmArgs &args, cud
         auto run = [&](auto kernel, int smem)
         {
             ensure_smem_attr(reinterpret_cast<const void *>(kernel), smem);
-            kernel<<<grid, NUM_THREADS, smem, s>>>(A.map, B.map, tmC, args, tiles_n, ntiles);
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(grid);
+            cfg.blockDim = dim3(NUM_THREADS);
+            cfg.dynamicSmemBytes = static_cast<size_t>(smem);
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1] = { programmatic_launch_attr() };
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            GPRAT_CUDA_CHECK(cudaLaunchKernelEx(&cfg, kernel, A.map, B.map, tmC, args, tiles_n, ntiles));
         };
         if (A.kind == TcKind::TF32)
         {
