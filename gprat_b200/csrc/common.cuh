@@ -217,14 +217,16 @@ void trsv_backward(const double *L, int64_t ldl, const double *Linv, int nb, int
 // claimed by ticket, every element of x written once and awaited by value.
 // flags: 1 int of scratch; scratch: n doubles (the right-hand side is copied
 // there).  L in FP64 or FP32; x is FP64, in place (b in, solution out).
+// max_ctas > 0 bounds the grid (each CTA then solves several row blocks), so
+// that the solve leaves SMs to work on another stream.
 void trsv_fused_forward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                        double *scratch, DeviceStatus *st, cudaStream_t s);
+                        double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
 void trsv_fused_backward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                         double *scratch, DeviceStatus *st, cudaStream_t s);
+                         double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
 void trsv_fused_forward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                            double *scratch, DeviceStatus *st, cudaStream_t s);
+                            double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
 void trsv_fused_backward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                             double *scratch, DeviceStatus *st, cudaStream_t s);
+                             double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
 // Same with an FP32 factor (mixed precision); FP64 right-hand side and arithmetic.
 void trsv_forward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s);
 void trsv_backward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s);

@@ -149,7 +149,7 @@ namespace gprat_cu
 
 // mixed.cu
 void factor_mixed(gprat_cu_gp *gp, cudaStream_t s);
-void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s);
+void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s, int solve_ctas = 0);
 void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s,
                     const int64_t *row_offsets = nullptr, int max_ctas = 0);
 void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s);

@@ -312,15 +312,17 @@ void symv(gprat_cu_gp *gp, const double *p, double *q, cudaStream_t s)
     GPRAT_LAUNCH_CHECK();
 }
 
-void precondition(gprat_cu_gp *gp, const double *r, double *z, cudaStream_t s)
+// z = (L L^T)^-1 r with the low-precision factor; solve_ctas > 0 bounds the
+// solves' grids.
+void precondition(gprat_cu_gp *gp, const double *r, double *z, cudaStream_t s, int solve_ctas)
 {
     GPRAT_CUDA_CHECK(cudaMemcpyAsync(z, r, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     gp->flags.ensure(2);
     gp->trsv_b.ensure(gp->n);
     trsv_fused_forward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, gp->n, z, gp->flags.ptr, gp->trsv_b.ptr,
-                           gp->status.ptr, s);
+                           gp->status.ptr, s, solve_ctas);
     trsv_fused_backward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, gp->n, z, gp->flags.ptr, gp->trsv_b.ptr,
-                            gp->status.ptr, s);
+                            gp->status.ptr, s, solve_ctas);
 }
 
 }  // namespace
@@ -335,22 +337,25 @@ namespace
 #define GPRAT_LOOKAHEAD_MAIN_PERCENT 70
 #endif
 
-// A share of the SMs in percent: the environment variable `name` if it holds
-// an integer in [10, 100], else the compiled default (a tuning knob).
-int sm_percent(const char *name, int dflt)
+// A tuning knob: the environment variable `name` if it holds an integer in
+// [lo, hi], else the compiled default.
+int knob(const char *name, int dflt, int lo, int hi)
 {
     const char *v = std::getenv(name);
     if (v != nullptr)
     {
         char *end = nullptr;
         const long p = std::strtol(v, &end, 10);
-        if (end != v && *end == '\0' && p >= 10 && p <= 100)
+        if (end != v && *end == '\0' && p >= lo && p <= hi)
         {
             return static_cast<int>(p);
         }
     }
     return dflt;
 }
+
+// A share of the SMs in percent (knob in [10, 100]).
+int sm_percent(const char *name, int dflt) { return knob(name, dflt, 10, 100); }
 
 void ensure_lookahead(gprat_cu_gp *gp, int nevents)
 {
@@ -507,7 +512,7 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
     }
 }
 
-void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s)
+void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s, int solve_ctas)
 {
     const int n = gp->n;
     for (DevBuf<double> *b : { &gp->pcg_r, &gp->pcg_z, &gp->pcg_p, &gp->pcg_q })
@@ -525,7 +530,7 @@ void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s)
     GPRAT_CUDA_CHECK(cudaMemcpyAsync(r, gp->y.ptr, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     dot(r, r, n, part, s);
     scalar(ps, part, 0, s);
-    precondition(gp, r, z, s);
+    precondition(gp, r, z, s, solve_ctas);
     dot(r, z, n, part, s);
     scalar(ps, part, 1, s);
     GPRAT_CUDA_CHECK(cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -546,7 +551,7 @@ void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s)
         {
             break;
         }
-        precondition(gp, r, z, s);
+        precondition(gp, r, z, s, solve_ctas);
         dot(r, z, n, part, s);
         scalar(ps, part, 4, s);
         pcg_direction_kernel<<<nb, 256, 0, s>>>(ps, p, z, n);
@@ -659,7 +664,11 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
 }
 
 // Share of the SMs the variance solve's GEMMs hold while alpha is refined
-// next to them (the refinement's solves are latency-bound and need few SMs).
+// next to them (the refinement's solves are latency-bound and need few SMs),
+// and the grid of those solves (0: one CTA per row block).
+#ifndef GPRAT_SOLVE_CTAS
+#define GPRAT_SOLVE_CTAS 64
+#endif
 #ifndef GPRAT_VARIANCE_PERCENT
 #define GPRAT_VARIANCE_PERCENT 75
 #endif
@@ -689,7 +698,7 @@ void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mea
     }
     {
         StepScope step("alpha refinement", side);
-        alpha_mixed(gp, side);
+        alpha_mixed(gp, side, knob("GPRAT_CU_SOLVE_CTAS", GPRAT_SOLVE_CTAS, 0, 100000));
     }
     if (m > 0)
     {

@@ -222,15 +222,37 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v)
 
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// Full (non-lower) tile index t -> (row tile, column tile) in groups of
+// GROUP_M row tiles: a group sweeps its columns together, so the tiles in
+// flight at one time (one per CTA or CTA pair) share a few row panels of A
+// and a few column panels of B.  For deep updates (K in the thousands) an
+// operand panel is tens of MB and the L2 cannot keep one panel per tile in
+// flight; the grouping then cuts the HBM re-reads of B by about GROUP_M.
+constexpr int GROUP_M = 8;
+
+__device__ __forceinline__ void grouped_tile(int t, int tiles_n, int ntiles, int &tm, int &tn)
+{
+    const int tiles_m = ntiles / tiles_n;
+    const int span = GROUP_M * tiles_n;
+    const int g = t / span;
+    const int first = g * GROUP_M;
+    const int gm = min(tiles_m - first, GROUP_M);
+    const int r = t - g * span;
+    tm = first + r % gm;
+    tn = r / gm;
+}
+
 // Tile t -> (m0, n0).  Lower mode (M == N): row tile i holds the column
 // tiles that reach the diagonal or below, (i * TM) / TNV + 1 of them.
 template <int TNV>
-__device__ __forceinline__ void tile_of(int t, bool lower, int tiles_n, int &m0, int &n0)
+__device__ __forceinline__ void tile_of(int t, bool lower, int tiles_n, int ntiles, int &m0, int &n0)
 {
     if (!lower)
     {
-        m0 = (t / tiles_n) * TM;
-        n0 = (t % tiles_n) * TNV;
+        int tm, tn;
+        grouped_tile(t, tiles_n, ntiles, tm, tn);
+        m0 = tm * TM;
+        n0 = tn * TNV;
         return;
     }
     if (TNV == TM)
@@ -341,7 +363,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             for (int t = blockIdx.x; ok && t < ntiles; t += gridDim.x)
             {
                 int m0, n0;
-                tile_of<TNV>(t, p.lower, tiles_n, m0, n0);
+                tile_of<TNV>(t, p.lower, tiles_n, ntiles, m0, n0);
                 for (int k = 0; k < kiters; ++k)
                 {
                     if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag))
@@ -447,7 +469,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         {
             const int b = it & 1;
             int m0, n0;
-            tile_of<TNV>(t, p.lower, tiles_n, m0, n0);
+            tile_of<TNV>(t, p.lower, tiles_n, ntiles, m0, n0);
             if (!mbar_wait(&tfull[b], (acc_bits >> b) & 1u, abort_flag))
             {
                 break;
@@ -642,12 +664,14 @@ __device__ __forceinline__ void mma_commit_pair_local(uint64_t *bar)
 }
 
 // pair tile t -> (m0, n0) in units of 256 (lower: square tiles at or below the diagonal)
-__device__ __forceinline__ void pair_tile_of(int t, bool lower, int tiles_n, int &m0, int &n0)
+__device__ __forceinline__ void pair_tile_of(int t, bool lower, int tiles_n, int ntiles, int &m0, int &n0)
 {
     if (!lower)
     {
-        m0 = (t / tiles_n) * 256;
-        n0 = (t % tiles_n) * 256;
+        int tm, tn;
+        grouped_tile(t, tiles_n, ntiles, tm, tn);
+        m0 = tm * 256;
+        n0 = tn * 256;
         return;
     }
     int i = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
@@ -734,7 +758,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             for (int t = pair; ok && t < ntiles; t += npairs)
             {
                 int m0, n0;
-                pair_tile_of(t, p.lower, tiles_n, m0, n0);
+                pair_tile_of(t, p.lower, tiles_n, ntiles, m0, n0);
                 const int arow = p.a_row0 + m0 + 128 * static_cast<int>(rank);
                 const int brow = p.b_row0 + n0 + 128 * static_cast<int>(rank);
                 for (int k = 0; k < kiters; ++k)
@@ -836,7 +860,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         {
             const int b = it & 1;
             int mp, n0;
-            pair_tile_of(t, p.lower, tiles_n, mp, n0);
+            pair_tile_of(t, p.lower, tiles_n, ntiles, mp, n0);
             const int m0 = mp + 128 * static_cast<int>(rank);  // this CTA's rows
             if (!mbar_wait(&tfull[b], (acc_bits >> b) & 1u, abort_flag))
             {

@@ -156,12 +156,20 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_fused_kernel(const T *__restri
     double *rhs = linv_s + PACKED;    // b_i, then b_i - sum_j L_ij x_j
     int *shared_int = reinterpret_cast<int *>(rhs + 2 * FB + (FT / 32) * FB);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nblk = (n + FB - 1) / FB;
+    for (;;)
+    {
     if (tid == 0)
     {
         shared_int[0] = atomicAdd(flags, 1);
     }
     __syncthreads();
     const int i = shared_int[0];
+    __syncthreads();  // every thread has its ticket before thread 0 draws the next
+    if (i >= nblk)
+    {
+        break;
+    }
     const int r0 = i * FB;
     const int bs = min(FB, n - r0);
     load_diag_inverse(linv_s, Linv + static_cast<int64_t>(i) * FB * FB);
@@ -259,6 +267,8 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_fused_kernel(const T *__restri
             x[r0 + r] = s;
         }
     }
+    __syncthreads();  // shared memory is refilled for the next block
+    }
 }
 
 template <typename T>
@@ -273,12 +283,19 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_fused_kernel(const T *__restri
     double *colpart = rhs + 2 * FB;  // [8][FB]
     int *shared_int = reinterpret_cast<int *>(colpart + (FT / 32) * FB);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (;;)
+    {
     if (tid == 0)
     {
         shared_int[0] = nblk - 1 - atomicAdd(flags, 1);
     }
     __syncthreads();
     const int i = shared_int[0];
+    __syncthreads();  // every thread has its ticket before thread 0 draws the next
+    if (i < 0)
+    {
+        break;
+    }
     const int c0 = i * FB;
     const int bs = min(FB, n - c0);
     load_diag_inverse(linv_s, Linv + static_cast<int64_t>(i) * FB * FB);
@@ -370,6 +387,8 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_fused_kernel(const T *__restri
             x[c0 + c] = s;
         }
     }
+    __syncthreads();  // shared memory is refilled for the next block
+    }
 }
 
 // x: in = b, out = solution.  scratch: n doubles (receives b).
@@ -380,52 +399,57 @@ void prepare(double *x, double *scratch, int n, int *flags, cudaStream_t s)
     GPRAT_CUDA_CHECK(cudaMemsetAsync(flags, 0, sizeof(int), s));
 }
 
+// grid: one CTA per row block, or max_ctas (> 0) CTAs that each take row
+// blocks by ticket until none is left (the solve then holds fewer SMs).
+int grid_for(int nblk, int max_ctas) { return max_ctas > 0 ? std::min(nblk, max_ctas) : nblk; }
+
 template <typename T>
 void fwd(const T *L, int64_t ld, const double *Linv, int n, double *x, int *flags, double *scratch, DeviceStatus *st,
-         cudaStream_t s)
+         cudaStream_t s, int max_ctas)
 {
     const int nblk = ceil_div(n, FB);
     ensure_smem_attr(reinterpret_cast<const void *>(trsv_fwd_fused_kernel<T>), static_cast<int>(SMEM_BYTES));
     prepare(x, scratch, n, flags, s);
-    trsv_fwd_fused_kernel<T><<<nblk, FT, SMEM_BYTES, s>>>(L, ld, Linv, n, scratch, x, flags, st);
+    trsv_fwd_fused_kernel<T><<<grid_for(nblk, max_ctas), FT, SMEM_BYTES, s>>>(L, ld, Linv, n, scratch, x, flags, st);
     GPRAT_LAUNCH_CHECK();
 }
 
 template <typename T>
 void bwd(const T *L, int64_t ld, const double *Linv, int n, double *x, int *flags, double *scratch, DeviceStatus *st,
-         cudaStream_t s)
+         cudaStream_t s, int max_ctas)
 {
     const int nblk = ceil_div(n, FB);
     ensure_smem_attr(reinterpret_cast<const void *>(trsv_bwd_fused_kernel<T>), static_cast<int>(SMEM_BYTES));
     prepare(x, scratch, n, flags, s);
-    trsv_bwd_fused_kernel<T><<<nblk, FT, SMEM_BYTES, s>>>(L, ld, Linv, n, nblk, scratch, x, flags, st);
+    trsv_bwd_fused_kernel<T><<<grid_for(nblk, max_ctas), FT, SMEM_BYTES, s>>>(L, ld, Linv, n, nblk, scratch, x,
+                                                                             flags, st);
     GPRAT_LAUNCH_CHECK();
 }
 
 }  // namespace
 
 void trsv_fused_forward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                        double *scratch, DeviceStatus *st, cudaStream_t s)
+                        double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas)
 {
-    fwd(L, ld, Linv, n, x, flags, scratch, st, s);
+    fwd(L, ld, Linv, n, x, flags, scratch, st, s, max_ctas);
 }
 
 void trsv_fused_backward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                         double *scratch, DeviceStatus *st, cudaStream_t s)
+                         double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas)
 {
-    bwd(L, ld, Linv, n, x, flags, scratch, st, s);
+    bwd(L, ld, Linv, n, x, flags, scratch, st, s, max_ctas);
 }
 
 void trsv_fused_forward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                            double *scratch, DeviceStatus *st, cudaStream_t s)
+                            double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas)
 {
-    fwd(L, ld, Linv, n, x, flags, scratch, st, s);
+    fwd(L, ld, Linv, n, x, flags, scratch, st, s, max_ctas);
 }
 
 void trsv_fused_backward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
-                             double *scratch, DeviceStatus *st, cudaStream_t s)
+                             double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas)
 {
-    bwd(L, ld, Linv, n, x, flags, scratch, st, s);
+    bwd(L, ld, Linv, n, x, flags, scratch, st, s, max_ctas);
 }
 
 }  // namespace gprat_cu
