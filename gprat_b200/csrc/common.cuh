@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <cstdlib>
 
 #include <mutex>
 #include <map>
@@ -99,16 +100,22 @@ void gemm_timing_end(cudaStream_t s, double flops);
 // stream is still running: it does its set-up (barriers, TMEM, descriptor
 // prefetch), then pdl_wait() blocks until that kernel has completed and its
 // memory is visible.  Every such kernel calls pdl_wait() before its first
-// access to global memory; pdl_launch_dependents() lets the next kernel's
-// set-up start.  Dependencies on events or other streams are unaffected.
+// access to global memory; pdl_launch_dependents() (first call per CTA
+// counts) lets the next kernel's set-up start once every CTA has called it
+// or exited.  The next kernel's CTAs then hold SMs while they wait, so the
+// kernels here signal only near their end: an early signal would let a chain
+// of kernels on one stream occupy every free SM and starve other streams.
+// Dependencies on events or other streams are unaffected.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 inline cudaLaunchAttribute programmatic_launch_attr()
 {
+    // GPRAT_CU_NO_PDL=1 launches every kernel with plain stream ordering
+    static const bool off = std::getenv("GPRAT_CU_NO_PDL") != nullptr;
     cudaLaunchAttribute a = {};
     a.id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    a.val.programmaticStreamSerializationAllowed = 1;
+    a.val.programmaticStreamSerializationAllowed = off ? 0 : 1;
     return a;
 }
 

@@ -569,6 +569,11 @@ void loss_mixed(gprat_cu_gp *gp, cudaStream_t s)
 namespace
 {
 
+// Below this many test rows the variance solve runs in 512-column panels
+// (short GEMMs over many CTAs), at or above it by recursive halving (deep
+// GEMMs; W is read and written once per level instead of once per panel).
+constexpr int RECURSIVE_MIN_ROWS = 2048;
+
 // Operands and buffers of one variance solve W L^T = K* (in place in W).
 struct VarianceSolve
 {
@@ -584,6 +589,57 @@ struct VarianceSolve
 
     const TcOperand &wt() const { return ops.bf16 ? opWb : opW; }
 
+    // W[:, c0:c0+128) := W[:, c0:c0+128) Linv_k^T (k = c0 / 128), row sums of
+    // squares into vacc.
+    void leaf(int c0) const
+    {
+        const int k = c0 / NB;
+        tc_gemm(opW, ops.Linv,
+                limited(tc_args(m, NB, NB, 0, c0, k * NB, 0, W + c0, ld32, 1.0f, 0.0f, false, gp->vacc.ptr,
+                                gp->status.ptr),
+                        max_ctas),
+                s);
+        if (ops.bf16)
+        {
+            convert_f32_to_bf16(W + c0, ld32, gp->Wb.ptr + c0, ld32, m, NB, s);
+        }
+    }
+
+    // W[:, cols) -= W[:, k0:k1) L[cols, k0:k1)^T
+    void update(int k0, int k1, int c0, int c1) const
+    {
+        tc_gemm(wt(), ops.trail(),
+                limited(tc_args(m, c1 - c0, k1 - k0, 0, k0, c0, k0, W + c0, ld32, -1.0f, 1.0f, false, nullptr,
+                                gp->status.ptr),
+                        max_ctas),
+                s);
+    }
+
+    // Right-looking in panels of 512 columns (inner blocks of 128): every
+    // update has depth 128 or 512, so each GEMM is short.  For few rows (a
+    // single row of tiles) this keeps many CTAs busy and no SM is held for
+    // long, where the recursive solve would run depth-16384 updates on a
+    // few CTAs.
+    void solve_panels(int n) const
+    {
+        for (int K0 = 0; K0 < n; K0 += NBO)
+        {
+            const int pend = std::min(K0 + NBO, n);
+            for (int c0 = K0; c0 < pend; c0 += NB)
+            {
+                leaf(c0);
+                if (c0 + NB < pend)
+                {
+                    update(c0, c0 + NB, c0 + NB, pend);
+                }
+            }
+            if (pend < n)
+            {
+                update(K0, pend, pend, n);
+            }
+        }
+    }
+
     // W[:, c0:c1) := W[:, c0:c1) L[c0:c1, c0:c1)^-T, for columns that already
     // hold every update from the columns left of c0.  Recursive halving: the
     // update between the halves is one GEMM of depth (mid - c0), so each
@@ -593,25 +649,12 @@ struct VarianceSolve
     {
         if (c1 - c0 <= NB)
         {
-            const int k = c0 / NB;
-            tc_gemm(opW, ops.Linv,
-                    limited(tc_args(m, NB, NB, 0, c0, k * NB, 0, W + c0, ld32, 1.0f, 0.0f, false, gp->vacc.ptr,
-                                    gp->status.ptr),
-                            max_ctas),
-                    s);
-            if (ops.bf16)
-            {
-                convert_f32_to_bf16(W + c0, ld32, gp->Wb.ptr + c0, ld32, m, NB, s);
-            }
+            leaf(c0);
             return;
         }
         const int mid = c0 + ((c1 - c0) / NB / 2) * NB;
         solve(c0, mid);
-        tc_gemm(wt(), ops.trail(),
-                limited(tc_args(m, c1 - mid, mid - c0, 0, c0, mid, c0, W + mid, ld32, -1.0f, 1.0f, false, nullptr,
-                                gp->status.ptr),
-                        max_ctas),
-                s);
+        update(c0, mid, mid, c1);
         solve(mid, c1);
     }
 };
@@ -659,7 +702,14 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     {
         tc_make_operand(v.opWb, gp->Wb.ptr, m, static_cast<int>(ld32), ld32, TcKind::BF16);
     }
-    v.solve(0, n);
+    if (m >= RECURSIVE_MIN_ROWS)
+    {
+        v.solve(0, n);
+    }
+    else
+    {
+        v.solve_panels(n);
+    }
     finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, s, gp->vacc.ptr + m);
 }
 
@@ -667,7 +717,7 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
 // next to them (the refinement's solves are latency-bound and need few SMs),
 // and the grid of those solves (0: one CTA per row block).
 #ifndef GPRAT_SOLVE_CTAS
-#define GPRAT_SOLVE_CTAS 64
+#define GPRAT_SOLVE_CTAS 0
 #endif
 #ifndef GPRAT_VARIANCE_PERCENT
 #define GPRAT_VARIANCE_PERCENT 75

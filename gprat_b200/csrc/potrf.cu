@@ -287,7 +287,6 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
         bad = 0;
     }
     pdl_wait();  // the previous kernel's results are visible from here on
-    pdl_launch_dependents();
     if (aligned16(A, lda))
     {
         load_lower_async(A, lda, bs, sa, xall);
@@ -509,6 +508,7 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
         }
         __syncthreads();
     }
+    pdl_launch_dependents();  // only the stores are left
     // store Linv (zero above the diagonal) in pairs of columns
 #pragma unroll 8
     for (int q = 0; q < PB * PB / 2 / PTHREADS; ++q)

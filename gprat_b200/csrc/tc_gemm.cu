@@ -348,7 +348,6 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     pdl_wait();  // the previous kernel's results are visible from here on
-    pdl_launch_dependents();
 
     if (warp == 0)
     {
@@ -551,6 +550,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 p.rowsq[h * p.rowsq_half + row] += sq;  // single writer per word and launch
             }
         }
+        // the CTA's last tile is in its stores: the next kernel in the stream
+        // may start its set-up (its CTAs then wait on free SMs, so the
+        // signal comes late enough not to hold SMs other streams could use)
+        pdl_launch_dependents();
         if (lane == 0)
         {
             bulk_wait_all();
@@ -743,7 +746,6 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     pdl_wait();  // the previous kernel's results are visible from here on
-    pdl_launch_dependents();
 
     if (warp == 0)
     {
@@ -934,6 +936,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 }
             }
         }
+        // the CTA's last tile is in its stores: the next kernel in the stream
+        // may start its set-up (its CTAs then wait on free SMs, so the
+        // signal comes late enough not to hold SMs other streams could use)
+        pdl_launch_dependents();
         if (lane == 0)
         {
             bulk_wait_all();

@@ -91,3 +91,22 @@ def test_mixed_device_resident(capi, problem):
     mean, var = gp.predict_with_uncertainty(p["h"], p["xt"], 1, p["m"])
     assert np.allclose(dm.cpu().numpy(), mean, rtol=0, atol=1e-12 * np.max(np.abs(mean)))
     assert np.allclose(dv.cpu().numpy(), var, rtol=1e-12)
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+def test_mixed_variance_recursive_solve(capi, problem, prec):
+    """2560 test rows take the recursive-halving variance solve (512 rows take
+    the 512-column panels); both meet the same stated tolerances, and the rows
+    they share agree to the low-precision factor's error."""
+    p = problem
+    m2 = 2560
+    _, _, xt2 = O.synthetic(p["n"], m2, p["d"])
+    o = O.OracleGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"], p["h"])
+    om2, ov2 = o.predict_with_uncertainty(xt2, 1, m2)
+    gp = capi.CudaGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"])
+    gp.set_precision(prec)
+    mean2, var2 = gp.predict_with_uncertainty(p["h"], xt2, 1, m2)
+    assert np.max(np.abs(mean2 - om2)) / np.max(np.abs(om2)) <= 1e-8
+    assert np.max(np.abs(var2 - ov2) / ov2) <= VAR_TOL[prec]
+    mean1, var1 = gp.predict_with_uncertainty(p["h"], xt2[: 512 + p["d"]], 1, 512)
+    assert np.max(np.abs(var1 - var2[:512]) / ov2[:512]) <= VAR_TOL[prec]
