@@ -31,6 +31,23 @@ namespace
 
 constexpr int PCG_MAX_ITERS = 60;
 constexpr double PCG_TOL = 1e-12;
+
+// The relative residual PCG stops at: GPRAT_CU_PCG_TOL if it holds a number
+// in [1e-15, 1e-6], else 1e-12 (a tuning knob).
+double pcg_tol()
+{
+    const char *v = std::getenv("GPRAT_CU_PCG_TOL");
+    if (v != nullptr)
+    {
+        char *end = nullptr;
+        const double t = std::strtod(v, &end);
+        if (end != v && *end == '\0' && t >= 1e-15 && t <= 1e-6)
+        {
+            return t;
+        }
+    }
+    return PCG_TOL;
+}
 constexpr int DOT_BLOCKS = 296;
 constexpr int DOT_THREADS = 256;
 
@@ -84,6 +101,11 @@ TcGemmArgs tc_args(int M, int N, int K, int ar, int ac, int br, int bc, float *C
 // block I and K_IJ^T p_I to the rows of block J.  Each (block, rows) pair of
 // the partial buffer part[B][i] has exactly one writer, and q_i sums
 // part[0..nblk)[i] in a fixed order, so the result is deterministic.
+// Warp w reads rows 16w .. 16w+15 of the tile; lane l reads columns
+// 4l .. 4l+3 of each row (two 16-byte loads, a warp reads a whole 1 KB row),
+// all loads of eight rows issued before their arithmetic.  Row sums stay in
+// registers (one per row) and are reduced across lanes once at the end,
+// through shared memory; column sums are reduced across warps likewise.
 constexpr int SV_THREADS = 256;
 
 __global__ void __launch_bounds__(SV_THREADS) symv_tile_kernel(const double *__restrict__ K, int64_t ld, int n,
@@ -91,7 +113,7 @@ __global__ void __launch_bounds__(SV_THREADS) symv_tile_kernel(const double *__r
 {
     __shared__ double pI[128], pJ[128];
     __shared__ double colsum[8][128];
-    __shared__ double rowsum[128];
+    __shared__ double rowred[8][16][33];  // [warp][row][lane], padded against bank conflicts
     const int q = blockIdx.x;
     int I = static_cast<int>((sqrt(8.0 * q + 1.0) - 1.0) * 0.5);
     while ((I + 1) * (I + 2) / 2 <= q)
@@ -111,70 +133,118 @@ __global__ void __launch_bounds__(SV_THREADS) symv_tile_kernel(const double *__r
         pJ[t] = (j0 + t < n) ? p[j0 + t] : 0.0;
     }
     __syncthreads();
-    double cs[4] = { 0.0, 0.0, 0.0, 0.0 };
-    for (int r = warp; r < 128; r += SV_THREADS / 32)
-    {
-        const int gi = i0 + r;
-        double rs = 0.0;
-        if (gi < n)
-        {
-            const double *kr = K + static_cast<int64_t>(gi) * ld + j0;
+    const int c0 = 4 * lane;  // this lane's first column in the tile
+    double pj[4];
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+    for (int c = 0; c < 4; ++c)
+    {
+        pj[c] = pJ[c0 + c];
+    }
+    const bool full = (I != J) && (i0 + 128 <= n) && (j0 + 128 <= n);
+    double rs[16];
+    double cs[4] = { 0.0, 0.0, 0.0, 0.0 };
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+    {
+        double2 v[8][2];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+        {
+            const int r = 16 * warp + 8 * h + k;
+            const int gi = min(i0 + r, n - 1);
+            const double2 *src = reinterpret_cast<const double2 *>(K + static_cast<int64_t>(gi) * ld + j0 + c0);
+            if (full || (i0 + r < n && j0 + c0 + 3 < n))
             {
-                const int lj = lane + 32 * c;
-                const int gj = j0 + lj;
-                if (gj < n && (I != J || lj <= r))
+                v[k][0] = src[0];
+                v[k][1] = src[1];
+            }
+            else
+            {
+                // ragged edge: element loads inside the matrix, zero outside
+                double e[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
                 {
-                    const double v = kr[lj];
-                    rs += v * pJ[lj];
-                    if (I != J || lj < r)
-                    {
-                        cs[c] += v * pI[r];
-                    }
+                    e[c] = (i0 + r < n && j0 + c0 + c < n) ? K[static_cast<int64_t>(gi) * ld + j0 + c0 + c] : 0.0;
                 }
+                v[k][0] = make_double2(e[0], e[1]);
+                v[k][1] = make_double2(e[2], e[3]);
             }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
+        for (int k = 0; k < 8; ++k)
         {
-            rs += __shfl_xor_sync(0xffffffffu, rs, o);
+            const int r = 16 * warp + 8 * h + k;
+            double e[4] = { v[k][0].x, v[k][0].y, v[k][1].x, v[k][1].y };
+            if (!full)
+            {
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                {
+                    // diagonal tile: the lower triangle only (the diagonal once)
+                    e[c] = (I == J && c0 + c > r) ? 0.0 : e[c];
+                }
+            }
+            double sr = 0.0;
+            const double pir = pI[r];
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                sr += e[c] * pj[c];
+                // transposed part: strictly below the diagonal on a diagonal tile
+                cs[c] += ((I == J && c0 + c == r) ? 0.0 : e[c]) * pir;
+            }
+            rs[8 * h + k] = sr;
         }
-        if (lane == 0)
-        {
-            rowsum[r] = rs;
-        }
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+    {
+        rowred[warp][k][lane] = rs[k];
     }
 #pragma unroll
     for (int c = 0; c < 4; ++c)
     {
-        colsum[warp][lane + 32 * c] = cs[c];
+        colsum[warp][c0 + c] = cs[c];
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < 128; t += SV_THREADS)
+    // row r of the tile: warp r / 16, row slot r % 16; two threads per row
+    // each sum 16 lanes, then combine
     {
-        double c = 0.0;
+        const int r = threadIdx.x >> 1, half = threadIdx.x & 1;
+        const double *src = &rowred[r >> 4][r & 15][16 * half];
+        double sr = 0.0;
 #pragma unroll
-        for (int w = 0; w < SV_THREADS / 32; ++w)
+        for (int l = 0; l < 16; ++l)
         {
-            c += colsum[w][t];
+            sr += src[l];
         }
-        if (I == J)
+        sr += __shfl_xor_sync(0xffffffffu, sr, 1);
+        if (half == 0)
         {
-            if (i0 + t < n)
+            double c = 0.0;
+#pragma unroll
+            for (int w = 0; w < SV_THREADS / 32; ++w)
             {
-                part[static_cast<int64_t>(I) * n + i0 + t] = rowsum[t] + c;
+                c += colsum[w][r];
             }
-        }
-        else
-        {
-            if (i0 + t < n)
+            if (I == J)
             {
-                part[static_cast<int64_t>(J) * n + i0 + t] = rowsum[t];
+                if (i0 + r < n)
+                {
+                    part[static_cast<int64_t>(I) * n + i0 + r] = sr + c;
+                }
             }
-            if (j0 + t < n)
+            else
             {
-                part[static_cast<int64_t>(I) * n + j0 + t] = c;
+                if (i0 + r < n)
+                {
+                    part[static_cast<int64_t>(J) * n + i0 + r] = sr;
+                }
+                if (j0 + r < n)
+                {
+                    part[static_cast<int64_t>(I) * n + j0 + r] = c;
+                }
             }
         }
     }
@@ -297,7 +367,7 @@ void dot(const double *a, const double *b, int n, double *part, cudaStream_t s)
 
 void scalar(PcgScalars *ps, const double *part, int which, cudaStream_t s)
 {
-    pcg_scalar_kernel<<<1, 32, 0, s>>>(ps, part, which, PCG_TOL);
+    pcg_scalar_kernel<<<1, 32, 0, s>>>(ps, part, which, pcg_tol());
     GPRAT_LAUNCH_CHECK();
 }
 
