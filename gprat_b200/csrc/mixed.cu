@@ -406,6 +406,15 @@ namespace
 #ifndef GPRAT_LOOKAHEAD_MAIN_PERCENT
 #define GPRAT_LOOKAHEAD_MAIN_PERCENT 70
 #endif
+#ifndef GPRAT_MIXED_PANEL_BLOCKS
+#define GPRAT_MIXED_PANEL_BLOCKS 8  // outer panels of 8 x 128 columns
+#endif
+#ifndef GPRAT_LOOKAHEAD_MAIN_PERCENT_LARGE
+#define GPRAT_LOOKAHEAD_MAIN_PERCENT_LARGE 70
+#endif
+#ifndef GPRAT_LOOKAHEAD_LARGE_ROWS
+#define GPRAT_LOOKAHEAD_LARGE_ROWS 16384
+#endif
 
 // A tuning knob: the environment variable `name` if it holds an integer in
 // [lo, hi], else the compiled default.
@@ -443,6 +452,10 @@ void ensure_lookahead(gprat_cu_gp *gp, int nevents)
     }
 }
 
+// Events of one factorisation (two per outer panel of at least one block,
+// one to start) and two for fit_predict_mixed, at the end.
+int lookahead_events(int n) { return 2 * ceil_div(n, NB) + 3; }
+
 TcGemmArgs limited(TcGemmArgs a, int max_ctas)
 {
     a.max_ctas = max_ctas;
@@ -451,7 +464,7 @@ TcGemmArgs limited(TcGemmArgs a, int max_ctas)
 
 }  // namespace
 
-// Right-looking Cholesky of the FP32 working copy in outer panels of NBO
+// Right-looking Cholesky of the FP32 working copy in outer panels of nbo
 // columns (inner blocks of NB), with a look-ahead of one panel:
 //   side stream (high priority): factor panel k (diagonal blocks in FP64,
 //     panel solves and the in-panel updates on tcgen05), then apply panel k
@@ -480,13 +493,19 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
         gp->Lb.ensure(static_cast<int64_t>(n) * ld32);
     }
     double *ldiag = gp->D64.ptr + NB * NB;
-    const int nout = ceil_div(n, NBO);
-    ensure_lookahead(gp, 2 * nout + 1);
+    // outer panel width (a multiple of the 128-wide diagonal blocks)
+    const int nbo = NB * knob("GPRAT_CU_MIXED_PANEL_BLOCKS", GPRAT_MIXED_PANEL_BLOCKS, 1, 16);
+    const int nout = ceil_div(n, nbo);
+    ensure_lookahead(gp, lookahead_events(n));
     cudaStream_t side = gp->side;
     auto evF = [&](int k) { return gp->events[1 + k]; };
     auto evR = [&](int k) { return gp->events[1 + nout + k]; };
     const int sms = device_sm_count();
+    // While the trailing matrix is large the update of panel k outlasts the
+    // panel chain by far, so it may take a larger share of the SMs.
     const int main_percent = sm_percent("GPRAT_CU_LOOKAHEAD_MAIN_PERCENT", GPRAT_LOOKAHEAD_MAIN_PERCENT);
+    const int main_percent_large = sm_percent("GPRAT_CU_LOOKAHEAD_MAIN_PERCENT_LARGE", GPRAT_LOOKAHEAD_MAIN_PERCENT_LARGE);
+    const int large_rows = knob("GPRAT_CU_LOOKAHEAD_LARGE_ROWS", GPRAT_LOOKAHEAD_LARGE_ROWS, 0, 1 << 30);
 
     {
         StepScope step("assembly", s);
@@ -499,12 +518,26 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
     float *K32 = gp->K32.ptr;
     auto at = [&](int r, int c) { return K32 + static_cast<int64_t>(r) * ld32 + c; };
 
-    // factor panel [K0, pend): diagonal blocks, panel solves, in-panel updates
+    // factor panel [K0, pend): diagonal blocks, panel solves, in-panel updates.
+    // Left-looking inside the panel (the default): before block column r0 is
+    // factored it receives the updates of every solved block column of the
+    // panel left of it in one GEMM of depth r0 - K0 (n - r0 rows, 128
+    // columns).  Right-looking: each solved block column updates all the
+    // panel's columns right of it at once; the same flops in twice the tiles.
+    const bool left = knob("GPRAT_CU_PANEL_LEFT_LOOKING", 1, 0, 1) != 0;
     auto factor_panel = [&](int K0, int pend, int ctas)
     {
         for (int r0 = K0; r0 < pend; r0 += NB)
         {
             const int k = r0 / NB;
+            if (left && r0 > K0)
+            {
+                tc_gemm(ops.trail(), ops.trail(),
+                        limited(tc_args(n - r0, NB, r0 - K0, r0, K0, r0, K0, at(r0, r0), ld32, -1.0f, 1.0f, false,
+                                        nullptr, gp->status.ptr),
+                                ctas),
+                        side);
+            }
             double *Lk = gp->Linv.ptr + static_cast<int64_t>(k) * NB * NB;
             potrf_diag_f32(at(r0, r0), ld32, NB, r0, Lk, NB, gp->Linv32.ptr + static_cast<int64_t>(k) * NB * NB, NB,
                            ldiag + r0, gp->status.ptr, side);
@@ -527,7 +560,7 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
             // launch (the strict upper triangle of the working copy is scratch:
             // nothing reads it, so its in-panel part is updated too)
             const int ncols = pend - (r0 + NB);
-            if (ncols > 0)
+            if (!left && ncols > 0)
             {
                 tc_gemm(ops.trail(), ops.trail(),
                         limited(tc_args(n - (r0 + NB), ncols, NB, r0 + NB, r0, r0 + NB, r0, at(r0 + NB, r0 + NB), ld32,
@@ -538,14 +571,14 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
         }
     };
 
-    factor_panel(0, std::min(NBO, n), 0);
+    factor_panel(0, std::min(nbo, n), 0);
     GPRAT_CUDA_CHECK(cudaEventRecord(evF(0), side));
     for (int k = 0; k < nout; ++k)
     {
-        const int K0 = k * NBO;
-        const int pend = std::min(K0 + NBO, n);
+        const int K0 = k * nbo;
+        const int pend = std::min(K0 + nbo, n);
         const int bo = pend - K0;
-        const int next_end = std::min(pend + NBO, n);  // end of panel k+1
+        const int next_end = std::min(pend + nbo, n);  // end of panel k+1
         const int rest = n - next_end;
         const bool ahead = k + 1 < nout;
         // main: everything right of panel k+1, with panel k
@@ -555,7 +588,8 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
             tc_gemm(ops.trail(), ops.trail(),
                     limited(tc_args(rest, rest, bo, next_end, K0, next_end, K0, at(next_end, next_end), ld32, -1.0f,
                                     1.0f, true, nullptr, gp->status.ptr),
-                            ahead ? std::max(1, sms * main_percent / 100) : 0),
+                            ahead ? std::max(1, sms * (rest >= large_rows ? main_percent_large : main_percent) / 100)
+                                  : 0),
                     s);
         }
         GPRAT_CUDA_CHECK(cudaEventRecord(evR(k), s));
@@ -802,9 +836,9 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
 void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
 {
     factor_mixed(gp, s);
-    const int nout = ceil_div(gp->n, NBO);
-    ensure_lookahead(gp, 2 * nout + 3);
-    cudaEvent_t factored = gp->events[2 * nout + 1], refined = gp->events[2 * nout + 2];
+    const int ne = lookahead_events(gp->n);
+    ensure_lookahead(gp, ne);
+    cudaEvent_t factored = gp->events[ne - 2], refined = gp->events[ne - 1];
     cudaStream_t side = gp->side;
     const int parts = ceil_div(gp->n, 128);
     gp->mean_part.ensure(static_cast<int64_t>(std::max(m, 1)) * parts);
