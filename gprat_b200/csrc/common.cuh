@@ -209,10 +209,10 @@ void assemble_prior(const double *xt, int m, int n_reg, const DeviceParams *p, d
 void potrf_diag(double *A, int64_t lda, int bs, int row0, double *Linv, int64_t ldi, DeviceStatus *status,
                 cudaStream_t s);
 // Same for an FP32 block (factored in FP64 in shared memory, L written back
-// in FP32); also writes Linv in FP32 (Linv32, ldi32) and the FP64 diagonal of
-// L (diag, bs values).
+// in FP32 unless write_l is false); also writes Linv in FP32 (Linv32, ldi32)
+// and the FP64 diagonal of L (diag, bs values).  Linv (FP64) may be null.
 void potrf_diag_f32(float *A, int64_t lda, int bs, int row0, double *Linv, int64_t ldi, float *Linv32, int64_t ldi32,
-                    double *diag, DeviceStatus *status, cudaStream_t s);
+                    double *diag, DeviceStatus *status, cudaStream_t s, bool write_l = true);
 
 // Triangular solves with the blocked factor (L in Lmat, diagonal-block
 // inverses in Linv, block size nb).
@@ -230,9 +230,9 @@ void trsv_fused_forward(const double *L, int64_t ld, const double *Linv, int n, 
                         double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
 void trsv_fused_backward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
                          double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
-void trsv_fused_forward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+void trsv_fused_forward_f32(const float *L, int64_t ld, const float *Linv, int n, double *x, int *flags,
                             double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
-void trsv_fused_backward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+void trsv_fused_backward_f32(const float *L, int64_t ld, const float *Linv, int n, double *x, int *flags,
                              double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
 // Same with an FP32 factor (mixed precision); FP64 right-hand side and arithmetic.
 void trsv_forward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s);

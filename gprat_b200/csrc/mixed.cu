@@ -389,9 +389,9 @@ void precondition(gprat_cu_gp *gp, const double *r, double *z, cudaStream_t s, i
     GPRAT_CUDA_CHECK(cudaMemcpyAsync(z, r, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     gp->flags.ensure(2);
     gp->trsv_b.ensure(gp->n);
-    trsv_fused_forward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, gp->n, z, gp->flags.ptr, gp->trsv_b.ptr,
+    trsv_fused_forward_f32(gp->K32.ptr, gp->ld32, gp->Linv32.ptr, gp->n, z, gp->flags.ptr, gp->trsv_b.ptr,
                            gp->status.ptr, s, solve_ctas);
-    trsv_fused_backward_f32(gp->K32.ptr, gp->ld32, gp->Linv.ptr, gp->n, z, gp->flags.ptr, gp->trsv_b.ptr,
+    trsv_fused_backward_f32(gp->K32.ptr, gp->ld32, gp->Linv32.ptr, gp->n, z, gp->flags.ptr, gp->trsv_b.ptr,
                             gp->status.ptr, s, solve_ctas);
 }
 
@@ -538,9 +538,11 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
                                 ctas),
                         side);
             }
-            double *Lk = gp->Linv.ptr + static_cast<int64_t>(k) * NB * NB;
-            potrf_diag_f32(at(r0, r0), ld32, NB, r0, Lk, NB, gp->Linv32.ptr + static_cast<int64_t>(k) * NB * NB, NB,
-                           ldiag + r0, gp->status.ptr, side);
+            // the diagonal block of L in the working copy and an FP64 inverse
+            // are not used downstream (solves use Linv32, the log-determinant
+            // the FP64 diagonal): neither is written
+            potrf_diag_f32(at(r0, r0), ld32, NB, r0, nullptr, 0, gp->Linv32.ptr + static_cast<int64_t>(k) * NB * NB,
+                           NB, ldiag + r0, gp->status.ptr, side, false);
             const int rows = n - r0 - NB;
             if (rows > 0)
             {

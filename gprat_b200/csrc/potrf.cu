@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
                                                                 double *__restrict__ Linv, int64_t ldi,
                                                                 float *__restrict__ Linv32, int64_t ldi32,
                                                                 double *__restrict__ diag_out,
-                                                                DeviceStatus *__restrict__ status)
+                                                                DeviceStatus *__restrict__ status, int write_l)
 {
     extern __shared__ double sa[];  // [PB][PS]
     double *xall = sa + PB * PS;    // 4 x [SB][XS] sub-block inverses
@@ -402,9 +402,10 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
     {
         atomicCAS(&status->not_spd_row, 0, bad);
     }
-    // write L (lower triangle incl. diagonal) back: in pairs of columns when
-    // the block is 16-byte aligned, else element by element
-    if (aligned16(A, lda))
+    // write L (lower triangle incl. diagonal) back, unless the caller has no
+    // use for it: in pairs of columns when the block is 16-byte aligned, else
+    // element by element
+    if (write_l && aligned16(A, lda))
     {
         using Pair = typename PairOf<T>::type;
 #pragma unroll 8
@@ -427,7 +428,7 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
             }
         }
     }
-    else
+    else if (write_l)
     {
         for (int q = tid; q < PB * PB; q += PTHREADS)
         {
@@ -522,11 +523,14 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
         const double2 raw = *reinterpret_cast<const double2 *>(sa + i * PS + c);
         const double v0 = (c <= i) ? raw.x : 0.0;
         const double v1 = (c + 1 <= i) ? raw.y : 0.0;
-        double *drow = Linv + static_cast<int64_t>(i) * ldi + c;
+        double *drow = (Linv != nullptr) ? Linv + static_cast<int64_t>(i) * ldi + c : nullptr;
         float *frow = (Linv32 != nullptr) ? Linv32 + static_cast<int64_t>(i) * ldi32 + c : nullptr;
         if (c + 1 < bs)
         {
-            *reinterpret_cast<double2 *>(drow) = make_double2(v0, v1);
+            if (drow != nullptr)
+            {
+                *reinterpret_cast<double2 *>(drow) = make_double2(v0, v1);
+            }
             if (frow != nullptr)
             {
                 *reinterpret_cast<float2 *>(frow) = make_float2(static_cast<float>(v0), static_cast<float>(v1));
@@ -534,7 +538,10 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
         }
         else
         {
-            drow[0] = v0;
+            if (drow != nullptr)
+            {
+                drow[0] = v0;
+            }
             if (frow != nullptr)
             {
                 frow[0] = static_cast<float>(v0);
@@ -568,18 +575,18 @@ void potrf_diag(double *A, int64_t lda, int bs, int row0, double *Linv, int64_t 
     cfg.numAttrs = 1;
     GPRAT_CUDA_CHECK(cudaLaunchKernelEx(&cfg, potrf_inv_kernel<double>, A, lda, bs, row0, Linv, ldi,
                                         static_cast<float *>(nullptr), int64_t{ 0 }, static_cast<double *>(nullptr),
-                                        status));
+                                        status, 1));
     GPRAT_LAUNCH_CHECK();
 }
 
 void potrf_diag_f32(float *A, int64_t lda, int bs, int row0, double *Linv, int64_t ldi, float *Linv32, int64_t ldi32,
-                    double *diag, DeviceStatus *status, cudaStream_t s)
+                    double *diag, DeviceStatus *status, cudaStream_t s, bool write_l)
 {
     if (bs <= 0 || bs > PB)
     {
         throw Error(1, "potrf_diag_f32: block size must be in [1, 128]");
     }
-    if ((ldi & 1) != 0 || (ldi32 & 1) != 0 || (reinterpret_cast<uintptr_t>(Linv) & 15) != 0 ||
+    if ((Linv != nullptr && ((ldi & 1) != 0 || (reinterpret_cast<uintptr_t>(Linv) & 15) != 0)) || (ldi32 & 1) != 0 ||
         (reinterpret_cast<uintptr_t>(Linv32) & 7) != 0)
     {
         throw Error(1, "potrf_diag_f32: Linv / Linv32 must be aligned with even leading dimensions");
@@ -595,7 +602,8 @@ void potrf_diag_f32(float *A, int64_t lda, int bs, int row0, double *Linv, int64
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     GPRAT_CUDA_CHECK(
-        cudaLaunchKernelEx(&cfg, potrf_inv_kernel<float>, A, lda, bs, row0, Linv, ldi, Linv32, ldi32, diag, status));
+        cudaLaunchKernelEx(&cfg, potrf_inv_kernel<float>, A, lda, bs, row0, Linv, ldi, Linv32, ldi32, diag, status,
+                           write_l ? 1 : 0));
     GPRAT_LAUNCH_CHECK();
 }
 

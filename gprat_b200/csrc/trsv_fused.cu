@@ -1,6 +1,6 @@
 // Single-launch blocked triangular solves L x = b and L^T x = b (FP64 right-
-// hand side; L in FP64 or FP32, row-major lower triangle; FP64 inverses of
-// the 128 x 128 diagonal blocks).
+// hand side; L in FP64 or FP32, row-major lower triangle; inverses of the
+// 128 x 128 diagonal blocks in FP64, or FP32 with an FP32 factor).
 //
 // forward_solve_tiled / backward_solve_tiled (core/src/cpu/tiled_algorithms.cpp:61-115)
 // walk the block columns one after another.  Launching one kernel per block
@@ -61,6 +61,20 @@ __device__ __forceinline__ void load_diag_inverse(double *dst, const double *Li)
         for (int c2 = lane; c2 < pairs; c2 += 32)
         {
             cp_async16(dst + packed_off(r) + 2 * c2, Li + r * FB + 2 * c2);
+        }
+    }
+}
+
+// FP32 inverse (mixed path): widened to FP64 into the same packed layout
+// (plain loads; the values are needed only after the block's last wait).
+__device__ __forceinline__ void load_diag_inverse(double *dst, const float *Li)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int r = warp; r < FB; r += FT / 32)
+    {
+        for (int c = lane; c <= r; c += 32)
+        {
+            dst[packed_off(r) + c] = static_cast<double>(Li[r * FB + c]);
         }
     }
 }
@@ -145,9 +159,9 @@ __device__ __forceinline__ double to_d(T v)
 }
 
 // flags[0] = ticket counter; b = right-hand side (copy); x = solution (sentinel-filled).
-template <typename T>
+template <typename T, typename TI>
 __global__ void __launch_bounds__(FT, 1) trsv_fwd_fused_kernel(const T *__restrict__ L, int64_t ld,
-                                                               const double *__restrict__ Linv, int n,
+                                                               const TI *__restrict__ Linv, int n,
                                                                const double *__restrict__ b, double *x, int *flags,
                                                                DeviceStatus *st)
 {
@@ -271,9 +285,9 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_fused_kernel(const T *__restri
     }
 }
 
-template <typename T>
+template <typename T, typename TI>
 __global__ void __launch_bounds__(FT, 1) trsv_bwd_fused_kernel(const T *__restrict__ L, int64_t ld,
-                                                               const double *__restrict__ Linv, int n, int nblk,
+                                                               const TI *__restrict__ Linv, int n, int nblk,
                                                                const double *__restrict__ b, double *x, int *flags,
                                                                DeviceStatus *st)
 {
@@ -403,26 +417,27 @@ void prepare(double *x, double *scratch, int n, int *flags, cudaStream_t s)
 // blocks by ticket until none is left (the solve then holds fewer SMs).
 int grid_for(int nblk, int max_ctas) { return max_ctas > 0 ? std::min(nblk, max_ctas) : nblk; }
 
-template <typename T>
-void fwd(const T *L, int64_t ld, const double *Linv, int n, double *x, int *flags, double *scratch, DeviceStatus *st,
+template <typename T, typename TI>
+void fwd(const T *L, int64_t ld, const TI *Linv, int n, double *x, int *flags, double *scratch, DeviceStatus *st,
          cudaStream_t s, int max_ctas)
 {
     const int nblk = ceil_div(n, FB);
-    ensure_smem_attr(reinterpret_cast<const void *>(trsv_fwd_fused_kernel<T>), static_cast<int>(SMEM_BYTES));
+    ensure_smem_attr(reinterpret_cast<const void *>(trsv_fwd_fused_kernel<T, TI>), static_cast<int>(SMEM_BYTES));
     prepare(x, scratch, n, flags, s);
-    trsv_fwd_fused_kernel<T><<<grid_for(nblk, max_ctas), FT, SMEM_BYTES, s>>>(L, ld, Linv, n, scratch, x, flags, st);
+    trsv_fwd_fused_kernel<T, TI>
+        <<<grid_for(nblk, max_ctas), FT, SMEM_BYTES, s>>>(L, ld, Linv, n, scratch, x, flags, st);
     GPRAT_LAUNCH_CHECK();
 }
 
-template <typename T>
-void bwd(const T *L, int64_t ld, const double *Linv, int n, double *x, int *flags, double *scratch, DeviceStatus *st,
+template <typename T, typename TI>
+void bwd(const T *L, int64_t ld, const TI *Linv, int n, double *x, int *flags, double *scratch, DeviceStatus *st,
          cudaStream_t s, int max_ctas)
 {
     const int nblk = ceil_div(n, FB);
-    ensure_smem_attr(reinterpret_cast<const void *>(trsv_bwd_fused_kernel<T>), static_cast<int>(SMEM_BYTES));
+    ensure_smem_attr(reinterpret_cast<const void *>(trsv_bwd_fused_kernel<T, TI>), static_cast<int>(SMEM_BYTES));
     prepare(x, scratch, n, flags, s);
-    trsv_bwd_fused_kernel<T><<<grid_for(nblk, max_ctas), FT, SMEM_BYTES, s>>>(L, ld, Linv, n, nblk, scratch, x,
-                                                                             flags, st);
+    trsv_bwd_fused_kernel<T, TI>
+        <<<grid_for(nblk, max_ctas), FT, SMEM_BYTES, s>>>(L, ld, Linv, n, nblk, scratch, x, flags, st);
     GPRAT_LAUNCH_CHECK();
 }
 
@@ -440,13 +455,13 @@ void trsv_fused_backward(const double *L, int64_t ld, const double *Linv, int n,
     bwd(L, ld, Linv, n, x, flags, scratch, st, s, max_ctas);
 }
 
-void trsv_fused_forward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+void trsv_fused_forward_f32(const float *L, int64_t ld, const float *Linv, int n, double *x, int *flags,
                             double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas)
 {
     fwd(L, ld, Linv, n, x, flags, scratch, st, s, max_ctas);
 }
 
-void trsv_fused_backward_f32(const float *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
+void trsv_fused_backward_f32(const float *L, int64_t ld, const float *Linv, int n, double *x, int *flags,
                              double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas)
 {
     bwd(L, ld, Linv, n, x, flags, scratch, st, s, max_ctas);
