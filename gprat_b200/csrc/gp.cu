@@ -22,7 +22,9 @@
 #include "gp_state.cuh"
 #include "gprat_cu.h"
 
+#include <algorithm>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -297,7 +299,9 @@ void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     const int parts = ceil_div(gp->n, 128);
     if (mixed(gp) && d_var != nullptr)
     {
-        variance_mixed(gp, d_xt, m, d_mean, d_var, s, row_offsets);
+        // a batch of separate requests (row_offsets) is served next to other
+        // work: short GEMMs only
+        variance_mixed(gp, d_xt, m, d_mean, d_var, s, row_offsets, 0, row_offsets == nullptr);
         return;
     }
     gp->mean_part.ensure(static_cast<int64_t>(m) * parts);
@@ -395,6 +399,102 @@ void set_last_error(const std::string &message) { g_last_error = message; }
 namespace gprat_cu
 {
 // Internal entry points used by the serving layer (serve.cu).
+namespace
+{
+std::mutex g_alloc_mtx;
+std::map<int, cudaStream_t> g_alloc_streams;  // per device
+
+cudaStream_t alloc_stream(int dev)
+{
+    std::lock_guard<std::mutex> lk(g_alloc_mtx);
+    auto it = g_alloc_streams.find(dev);
+    if (it != g_alloc_streams.end())
+    {
+        return it->second;
+    }
+    cudaStream_t st = nullptr;
+    GPRAT_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    g_alloc_streams[dev] = st;
+    return st;
+}
+
+std::map<int, int64_t> g_pool_hold;  // bytes the device's pool keeps reserved, per device (under g_alloc_mtx)
+
+void set_release_threshold(int dev, int64_t bytes)
+{
+    cudaMemPool_t pool = nullptr;
+    GPRAT_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t keep = static_cast<uint64_t>(bytes);
+    GPRAT_CUDA_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    GPRAT_CUDA_CHECK(cudaMemPoolTrimTo(pool, static_cast<size_t>(bytes)));
+}
+}  // namespace
+
+// The current device's pool keeps `bytes` more reserved after frees, and is
+// grown by that much now (mapping device memory into a pool can wait for the
+// kernels in flight; done once up front, later allocations reuse it).
+void pool_hold(int64_t bytes)
+{
+    int dev = 0;
+    GPRAT_CUDA_CHECK(cudaGetDevice(&dev));
+    int64_t total = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_alloc_mtx);
+        total = (g_pool_hold[dev] += bytes);
+    }
+    set_release_threshold(dev, total);
+    void *p = device_alloc(static_cast<size_t>(bytes));
+    device_free(p);
+}
+
+// Undoes pool_hold(bytes): the pool returns what it keeps beyond the rest.
+void pool_unhold(int64_t bytes)
+{
+    int dev = 0;
+    GPRAT_CUDA_CHECK(cudaGetDevice(&dev));
+    int64_t total = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_alloc_mtx);
+        total = (g_pool_hold[dev] = std::max<int64_t>(0, g_pool_hold[dev] - bytes));
+    }
+    set_release_threshold(dev, total);
+}
+
+void *device_alloc(size_t bytes)
+{
+    int dev = 0;
+    GPRAT_CUDA_CHECK(cudaGetDevice(&dev));
+    cudaStream_t st = alloc_stream(dev);
+    void *p = nullptr;
+    const cudaError_t e = cudaMallocAsync(&p, bytes, st);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        throw Error(e == cudaErrorMemoryAllocation ? GPRAT_CU_ERR_OOM : GPRAT_CU_ERR_CUDA,
+                    std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " +
+                        cudaGetErrorString(e));
+    }
+    GPRAT_CUDA_CHECK(cudaStreamSynchronize(st));
+    return p;
+}
+
+void device_free(void *p)
+{
+    if (p == nullptr)
+    {
+        return;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+    {
+        return;
+    }
+    cudaDeviceSynchronize();
+    cudaStream_t st = alloc_stream(dev);
+    cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+}
+
 void gp_fit(gprat_cu_gp *gp, const double hyper[3], cudaStream_t s)
 {
     upload_hyper(gp, hyper, s);

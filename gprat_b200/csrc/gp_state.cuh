@@ -15,6 +15,21 @@ namespace gprat_cu
 constexpr int NB = 128;   // diagonal block size (potrf + inverse)
 constexpr int NBO = 512;  // outer block of the two-level factorisation and solves
 
+// Device memory of the library's buffers.  Allocation is stream-ordered on a
+// private stream of the current device (cudaMallocAsync from the device's
+// default pool, then a wait on that stream only), so creating a model does
+// not wait for the kernels other handles or a server have in flight, as a
+// plain cudaMalloc may.  Freed memory goes back to the device (the pool keeps
+// only what pool_hold reserved).  Freeing first waits for the whole device
+// (the buffer may still be read by a kernel on any stream), like cudaFree.
+void *device_alloc(size_t bytes);
+void device_free(void *p);
+// A long-lived user of the current device (a server) asks the pool to keep
+// `bytes` reserved (pool_hold grows it by that much at once) and gives the
+// reservation back with pool_unhold.
+void pool_hold(int64_t bytes);
+void pool_unhold(int64_t bytes);
+
 template <typename T>
 struct DevBuf
 {
@@ -27,14 +42,14 @@ struct DevBuf
             return;
         }
         release();
-        GPRAT_CUDA_CHECK(cudaMalloc(&ptr, static_cast<size_t>(n) * sizeof(T)));
+        ptr = static_cast<T *>(device_alloc(static_cast<size_t>(n) * sizeof(T)));
         cap = n;
     }
     void release()
     {
         if (ptr != nullptr)
         {
-            cudaFree(ptr);
+            device_free(ptr);
         }
         ptr = nullptr;
         cap = 0;
@@ -151,7 +166,7 @@ namespace gprat_cu
 void factor_mixed(gprat_cu_gp *gp, cudaStream_t s);
 void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s, int solve_ctas = 0);
 void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s,
-                    const int64_t *row_offsets = nullptr, int max_ctas = 0);
+                    const int64_t *row_offsets = nullptr, int max_ctas = 0, bool recursive = true);
 void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s);
 
 // gp.cu: internal entry points for the serving layer (serve.cu)

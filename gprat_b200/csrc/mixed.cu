@@ -770,9 +770,12 @@ struct VarianceSolve
 // Mean (when d_mean != nullptr, from the refined alpha) and variance (when
 // d_var != nullptr) for m test points.  max_ctas bounds the grid of the
 // variance solve's GEMMs (0: every SM), so that another stream can run next
-// to it.
+// to it.  recursive: the variance solve may use recursive halving (for
+// RECURSIVE_MIN_ROWS rows or more); its deepest GEMMs hold every SM for
+// milliseconds, so callers that share the GPU with latency-sensitive work
+// (a serving batch) keep to the panel order, whose GEMMs are short.
 void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s,
-                    const int64_t *row_offsets, int max_ctas)
+                    const int64_t *row_offsets, int max_ctas, bool recursive)
 {
     const int n = gp->n;
     const int64_t ld32 = gp->ld32;
@@ -808,7 +811,7 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     {
         tc_make_operand(v.opWb, gp->Wb.ptr, m, static_cast<int>(ld32), ld32, TcKind::BF16);
     }
-    if (m >= RECURSIVE_MIN_ROWS)
+    if (recursive && m >= RECURSIVE_MIN_ROWS)
     {
         v.solve(0, n);
     }

@@ -126,11 +126,16 @@ struct Model
 
 }  // namespace
 
+// Most device memory a server reserves in the allocation pool when it starts
+// (at most its budget).
+constexpr int64_t POOL_RESERVE_MAX = int64_t{ 64 } << 30;
+
 struct gprat_cu_server
 {
     int device = 0;
     int precision = GPRAT_CU_PREC_FP64;
     int64_t budget = 0;
+    int64_t pool_reserved = 0;  // bytes pool_hold keeps for this server
     int64_t used = 0;
     std::mutex mtx;
     std::condition_variable cv_work, cv_done, cv_fit;
@@ -555,6 +560,11 @@ int gprat_cu_server_create(int device, int64_t memory_budget_bytes, int precisio
                 memory_budget_bytes = static_cast<int64_t>(0.8 * static_cast<double>(free_b));
             }
             sv->budget = memory_budget_bytes;
+            // Reserve device memory for the models up front: growing the
+            // allocation pool later, while batches run, can stall a fit for
+            // hundreds of milliseconds.
+            sv->pool_reserved = std::min<int64_t>(memory_budget_bytes, POOL_RESERVE_MAX);
+            pool_hold(sv->pool_reserved);
             gprat_cu_server *p = sv.get();
             sv->scheduler = std::thread(scheduler_loop, p);
             sv->fitter = std::thread(fitter_loop, p);
@@ -585,7 +595,11 @@ int gprat_cu_server_destroy(gprat_cu_server *sv)
             {
                 sv->fitter.join();
             }
+            const int64_t reserved = sv->pool_reserved;
+            const int dev = sv->device;
             delete sv;
+            cudaSetDevice(dev);
+            pool_unhold(reserved);
         });
 }
 
