@@ -78,7 +78,8 @@ struct gprat_cu_gp
 {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaStream_t side = nullptr;  // high-priority stream of the look-ahead panel factorisation
+    cudaStream_t side = nullptr;     // high-priority stream of the look-ahead panel factorisation
+    cudaStream_t vstream = nullptr;  // low-priority stream of the variance solve beside the factorisation
     std::vector<cudaEvent_t> events;  // look-ahead ordering events (created on first use)
     int n = 0, n_tiles = 0, T = 0, d = 0;
     int64_t n_in = 0;
@@ -118,6 +119,10 @@ struct gprat_cu_gp
         {
             cudaStreamSynchronize(side);
         }
+        if (vstream != nullptr)
+        {
+            cudaStreamSynchronize(vstream);
+        }
         for (gprat_cu::DevBuf<double> *b : { &x, &y, &K, &Linv, &alpha, &U, &partials, &xt, &W, &vacc, &mean_part,
                                              &mean, &var, &losses, &D64, &pcg_r, &pcg_z, &pcg_p, &pcg_q, &symv_part, &trsv_b })
         {
@@ -144,6 +149,10 @@ struct gprat_cu_gp
         {
             cudaStreamDestroy(side);
         }
+        if (vstream != nullptr)
+        {
+            cudaStreamDestroy(vstream);
+        }
         for (cudaEvent_t e : events)
         {
             cudaEventDestroy(e);
@@ -163,7 +172,7 @@ namespace gprat_cu
 {
 
 // mixed.cu
-void factor_mixed(gprat_cu_gp *gp, cudaStream_t s);
+void factor_mixed(gprat_cu_gp *gp, cudaStream_t s, int split_col = 0, cudaEvent_t split_ev = nullptr);
 void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s, int solve_ctas = 0);
 void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s,
                     const int64_t *row_offsets = nullptr, int max_ctas = 0, bool recursive = true);

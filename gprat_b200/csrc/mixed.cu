@@ -443,6 +443,7 @@ void ensure_lookahead(gprat_cu_gp *gp, int nevents)
         int least = 0, greatest = 0;
         GPRAT_CUDA_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         GPRAT_CUDA_CHECK(cudaStreamCreateWithPriority(&gp->side, cudaStreamNonBlocking, greatest));
+        GPRAT_CUDA_CHECK(cudaStreamCreateWithPriority(&gp->vstream, cudaStreamNonBlocking, least));
     }
     while (static_cast<int>(gp->events.size()) < nevents)
     {
@@ -453,8 +454,8 @@ void ensure_lookahead(gprat_cu_gp *gp, int nevents)
 }
 
 // Events of one factorisation (two per outer panel of at least one block,
-// one to start) and two for fit_predict_mixed, at the end.
-int lookahead_events(int n) { return 2 * ceil_div(n, NB) + 3; }
+// one to start) and five for fit_predict_mixed, at the end.
+int lookahead_events(int n) { return 2 * ceil_div(n, NB) + 6; }
 
 TcGemmArgs limited(TcGemmArgs a, int max_ctas)
 {
@@ -475,7 +476,10 @@ TcGemmArgs limited(TcGemmArgs a, int max_ctas)
 // Events order the two streams: panel k+1's columns are written by the
 // update of panel k-1 (main) before the side stream touches them, and the
 // update of panel k waits for panel k's factorisation.
-void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
+// split_ev (optional) is recorded on the side stream once columns
+// [0, split_col) of the factor are final (all rows), so that work which needs
+// only those columns can start before the factorisation ends.
+void factor_mixed(gprat_cu_gp *gp, cudaStream_t s, int split_col, cudaEvent_t split_ev)
 {
     const int n = gp->n;
     if (n % NB != 0)
@@ -573,7 +577,17 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
         }
     };
 
+    bool split_done = split_ev == nullptr;
+    auto maybe_split = [&](int done_cols)
+    {
+        if (!split_done && done_cols >= split_col)
+        {
+            GPRAT_CUDA_CHECK(cudaEventRecord(split_ev, side));
+            split_done = true;
+        }
+    };
     factor_panel(0, std::min(nbo, n), 0);
+    maybe_split(std::min(nbo, n));
     GPRAT_CUDA_CHECK(cudaEventRecord(evF(0), side));
     for (int k = 0; k < nout; ++k)
     {
@@ -614,6 +628,7 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s)
                         side_ctas),
                 side);
         factor_panel(pend, next_end, side_ctas);
+        maybe_split(next_end);
         GPRAT_CUDA_CHECK(cudaEventRecord(evF(k + 1), side));
     }
 }
@@ -831,30 +846,85 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
 #ifndef GPRAT_VARIANCE_PERCENT
 #define GPRAT_VARIANCE_PERCENT 75
 #endif
+#ifndef GPRAT_VARIANCE_EARLY_PERCENT
+#define GPRAT_VARIANCE_EARLY_PERCENT 70
+#endif
 
-// Fit, mean and variance (predict_with_uncertainty).  After the
-// factorisation the two remaining halves are independent: the variance solve
-// needs only the factor, alpha's refinement needs only the factor and K.  So
-// the variance solve's GEMMs run on `s` with GPRAT_VARIANCE_PERCENT % of the
-// SMs while the high-priority side stream refines alpha (FP64 PCG) and forms
-// the mean from it.  The side stream joins `s` at the end.
+// Fit, mean and variance (predict_with_uncertainty).
+//   caller's stream `s` + high-priority side stream: the factorisation;
+//   low-priority variance stream: the cross covariance K* (independent of the
+//     factor) from the start; with RECURSIVE_MIN_ROWS test rows or more, the
+//     first half of the recursive variance solve (its left half and the big
+//     update of the right half) as soon as the factor's left half is final,
+//     beside the factorisation's second half (whose panel chain leaves SMs
+//     idle), on GPRAT_VARIANCE_EARLY_PERCENT % of the SMs; the rest once the
+//     factor is complete, on GPRAT_VARIANCE_PERCENT %;
+//   side stream, after the factorisation: alpha's refinement (FP64 PCG) and
+//     the mean.
+// `s` waits for both at the end.
 void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
 {
-    factor_mixed(gp, s);
-    const int ne = lookahead_events(gp->n);
+    const int n = gp->n;
+    const int ne = lookahead_events(n);
     ensure_lookahead(gp, ne);
-    cudaEvent_t factored = gp->events[ne - 2], refined = gp->events[ne - 1];
-    cudaStream_t side = gp->side;
-    const int parts = ceil_div(gp->n, 128);
+    cudaEvent_t begin = gp->events[ne - 5], half = gp->events[ne - 4], factored = gp->events[ne - 3];
+    cudaEvent_t refined = gp->events[ne - 2], solved = gp->events[ne - 1];
+    cudaStream_t side = gp->side, vs = gp->vstream;
+    const int sms = device_sm_count();
+    const int parts = ceil_div(n, 128);
+    const bool early = m >= RECURSIVE_MIN_ROWS;
+    const int h = (n / NB / 2) * NB;  // the recursive solve's first split
+    // buffers first (an allocation must not fall between launches of different streams)
     gp->mean_part.ensure(static_cast<int64_t>(std::max(m, 1)) * parts);
+    gp->W32.ensure(static_cast<int64_t>(std::max(m, 1)) * gp->ld32);
+    gp->vacc.ensure(2 * static_cast<int64_t>(std::max(m, 1)));
+    if (gp->precision == GPRAT_CU_PREC_MIXED_BF16)
+    {
+        gp->Wb.ensure(static_cast<int64_t>(std::max(m, 1)) * gp->ld32);
+    }
+    GPRAT_CUDA_CHECK(cudaEventRecord(begin, s));
+    GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, begin, 0));
+    factor_mixed(gp, s, early ? h : 0, early ? half : nullptr);
     GPRAT_CUDA_CHECK(cudaEventRecord(factored, s));
     GPRAT_CUDA_CHECK(cudaStreamWaitEvent(side, factored, 0));
     if (m > 0)
     {
-        variance_mixed(gp, d_xt, m, nullptr, d_var, s, nullptr,
-                       std::max(1, device_sm_count() *
-                                       sm_percent("GPRAT_CU_VARIANCE_PERCENT", GPRAT_VARIANCE_PERCENT) / 100));
+        const int late_ctas =
+            std::max(1, sms * sm_percent("GPRAT_CU_VARIANCE_PERCENT", GPRAT_VARIANCE_PERCENT) / 100);
+        if (early)
+        {
+            float *W = gp->W32.ptr;
+            const int64_t ld32 = gp->ld32;
+            {
+                StepScope step("prediction", vs);
+                assemble_cross_f32(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, W, ld32, nullptr, nullptr, parts,
+                                   vs, nullptr);
+            }
+            StepScope step("forward KcK", vs);
+            GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->vacc.ptr, 0, 2 * m * sizeof(double), vs));
+            VarianceSolve v{ gp, make_ops(gp), {}, {}, W, ld32, m, 0, vs };
+            tc_make_operand(v.opW, W, m, static_cast<int>(ld32), ld32, TcKind::TF32);
+            if (gp->precision == GPRAT_CU_PREC_MIXED_BF16)
+            {
+                tc_make_operand(v.opWb, gp->Wb.ptr, m, static_cast<int>(ld32), ld32, TcKind::BF16);
+            }
+            GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, half, 0));
+            v.max_ctas = std::max(
+                1, sms * sm_percent("GPRAT_CU_VARIANCE_EARLY_PERCENT", GPRAT_VARIANCE_EARLY_PERCENT) / 100);
+            v.solve(0, h);
+            v.update(0, h, h, n);
+            GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, factored, 0));
+            v.max_ctas = late_ctas;
+            v.solve(h, n);
+            finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, vs, gp->vacc.ptr + m);
+        }
+        else
+        {
+            GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, factored, 0));
+            variance_mixed(gp, d_xt, m, nullptr, d_var, vs, nullptr, late_ctas);
+        }
     }
+    GPRAT_CUDA_CHECK(cudaEventRecord(solved, vs));
     {
         StepScope step("alpha refinement", side);
         alpha_mixed(gp, side, knob("GPRAT_CU_SOLVE_CTAS", GPRAT_SOLVE_CTAS, 0, 100000));
@@ -862,12 +932,13 @@ void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mea
     if (m > 0)
     {
         StepScope step("prediction", side);
-        assemble_cross(d_xt, m, gp->x.ptr, gp->n, gp->d, gp->params.ptr, nullptr, 0, gp->alpha.ptr,
-                       gp->mean_part.ptr, parts, side, nullptr);
+        assemble_cross(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, nullptr, 0, gp->alpha.ptr, gp->mean_part.ptr,
+                       parts, side, nullptr);
         reduce_mean(gp->mean_part.ptr, m, parts, d_mean, side);
     }
     GPRAT_CUDA_CHECK(cudaEventRecord(refined, side));
     GPRAT_CUDA_CHECK(cudaStreamWaitEvent(s, refined, 0));
+    GPRAT_CUDA_CHECK(cudaStreamWaitEvent(s, solved, 0));
 }
 
 }  // namespace gprat_cu
