@@ -7,6 +7,7 @@
 #include "tc_gemm.cuh"
 
 #include <initializer_list>
+#include <utility>
 #include <vector>
 
 namespace gprat_cu
@@ -172,7 +173,8 @@ namespace gprat_cu
 {
 
 // mixed.cu
-void factor_mixed(gprat_cu_gp *gp, cudaStream_t s, int split_col = 0, cudaEvent_t split_ev = nullptr);
+void factor_mixed(gprat_cu_gp *gp, cudaStream_t s,
+                  const std::vector<std::pair<int, cudaEvent_t>> &splits = {});
 void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s, int solve_ctas = 0);
 void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s,
                     const int64_t *row_offsets = nullptr, int max_ctas = 0, bool recursive = true);

@@ -454,8 +454,8 @@ void ensure_lookahead(gprat_cu_gp *gp, int nevents)
 }
 
 // Events of one factorisation (two per outer panel of at least one block,
-// one to start) and five for fit_predict_mixed, at the end.
-int lookahead_events(int n) { return 2 * ceil_div(n, NB) + 6; }
+// one to start) and six for fit_predict_mixed, at the end.
+int lookahead_events(int n) { return 2 * ceil_div(n, NB) + 7; }
 
 TcGemmArgs limited(TcGemmArgs a, int max_ctas)
 {
@@ -476,10 +476,10 @@ TcGemmArgs limited(TcGemmArgs a, int max_ctas)
 // Events order the two streams: panel k+1's columns are written by the
 // update of panel k-1 (main) before the side stream touches them, and the
 // update of panel k waits for panel k's factorisation.
-// split_ev (optional) is recorded on the side stream once columns
-// [0, split_col) of the factor are final (all rows), so that work which needs
+// splits (optional): (c, e) pairs; e is recorded on the side stream once
+// columns [0, c) of the factor are final (all rows), so that work which needs
 // only those columns can start before the factorisation ends.
-void factor_mixed(gprat_cu_gp *gp, cudaStream_t s, int split_col, cudaEvent_t split_ev)
+void factor_mixed(gprat_cu_gp *gp, cudaStream_t s, const std::vector<std::pair<int, cudaEvent_t>> &splits)
 {
     const int n = gp->n;
     if (n % NB != 0)
@@ -577,13 +577,13 @@ void factor_mixed(gprat_cu_gp *gp, cudaStream_t s, int split_col, cudaEvent_t sp
         }
     };
 
-    bool split_done = split_ev == nullptr;
+    size_t next_split = 0;  // splits are in ascending column order
     auto maybe_split = [&](int done_cols)
     {
-        if (!split_done && done_cols >= split_col)
+        while (next_split < splits.size() && done_cols >= splits[next_split].first)
         {
-            GPRAT_CUDA_CHECK(cudaEventRecord(split_ev, side));
-            split_done = true;
+            GPRAT_CUDA_CHECK(cudaEventRecord(splits[next_split].second, side));
+            ++next_split;
         }
     };
     factor_panel(0, std::min(nbo, n), 0);
@@ -856,9 +856,10 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
 //     factor) from the start; with RECURSIVE_MIN_ROWS test rows or more, the
 //     first half of the recursive variance solve (its left half and the big
 //     update of the right half) as soon as the factor's left half is final,
-//     beside the factorisation's second half (whose panel chain leaves SMs
-//     idle), on GPRAT_VARIANCE_EARLY_PERCENT % of the SMs; the rest once the
-//     factor is complete, on GPRAT_VARIANCE_PERCENT %;
+//     and the next quarter once three quarters are, beside the
+//     factorisation's second half (whose panel chain leaves SMs idle), on
+//     GPRAT_VARIANCE_EARLY_PERCENT % of the SMs; the rest once the factor is
+//     complete, on GPRAT_VARIANCE_PERCENT %;
 //   side stream, after the factorisation: alpha's refinement (FP64 PCG) and
 //     the mean.
 // `s` waits for both at the end.
@@ -867,13 +868,14 @@ void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mea
     const int n = gp->n;
     const int ne = lookahead_events(n);
     ensure_lookahead(gp, ne);
-    cudaEvent_t begin = gp->events[ne - 5], half = gp->events[ne - 4], factored = gp->events[ne - 3];
-    cudaEvent_t refined = gp->events[ne - 2], solved = gp->events[ne - 1];
+    cudaEvent_t begin = gp->events[ne - 6], half = gp->events[ne - 5], three_q = gp->events[ne - 4];
+    cudaEvent_t factored = gp->events[ne - 3], refined = gp->events[ne - 2], solved = gp->events[ne - 1];
     cudaStream_t side = gp->side, vs = gp->vstream;
     const int sms = device_sm_count();
     const int parts = ceil_div(n, 128);
     const bool early = m >= RECURSIVE_MIN_ROWS;
-    const int h = (n / NB / 2) * NB;  // the recursive solve's first split
+    const int h = (n / NB / 2) * NB;                      // the recursive solve's first split
+    const int h2 = h + ((n - h) / NB / 2) * NB;           // and the split of its right half
     // buffers first (an allocation must not fall between launches of different streams)
     gp->mean_part.ensure(static_cast<int64_t>(std::max(m, 1)) * parts);
     gp->W32.ensure(static_cast<int64_t>(std::max(m, 1)) * gp->ld32);
@@ -884,7 +886,14 @@ void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mea
     }
     GPRAT_CUDA_CHECK(cudaEventRecord(begin, s));
     GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, begin, 0));
-    factor_mixed(gp, s, early ? h : 0, early ? half : nullptr);
+    std::vector<std::pair<int, cudaEvent_t>> splits;
+    // GPRAT_CU_VARIANCE_SPLITS: 1 starts only the first half early, 2 (default) also the next quarter
+    const bool two = knob("GPRAT_CU_VARIANCE_SPLITS", 2, 1, 2) == 2;
+    if (early)
+    {
+        splits = { { h, half }, { two ? h2 : n + 1, three_q } };
+    }
+    factor_mixed(gp, s, splits);
     GPRAT_CUDA_CHECK(cudaEventRecord(factored, s));
     GPRAT_CUDA_CHECK(cudaStreamWaitEvent(side, factored, 0));
     if (m > 0)
@@ -913,9 +922,12 @@ void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mea
                 1, sms * sm_percent("GPRAT_CU_VARIANCE_EARLY_PERCENT", GPRAT_VARIANCE_EARLY_PERCENT) / 100);
             v.solve(0, h);
             v.update(0, h, h, n);
+            GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, three_q, 0));
+            v.solve(h, h2);
+            v.update(h, h2, h2, n);
             GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, factored, 0));
             v.max_ctas = late_ctas;
-            v.solve(h, n);
+            v.solve(h2, n);
             finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, vs, gp->vacc.ptr + m);
         }
         else
