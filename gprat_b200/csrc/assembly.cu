@@ -76,7 +76,7 @@ constexpr int RECUR_MIN_D = 16;
 
 // mode 0: K (lower tiles of size T incl. full diagonal tiles, + noise on the
 //         global diagonal); mode 1: cross / prior (all entries, no noise).
-// out32 (optional, mode 0): the same entries rounded to FP32 (mixed path).
+// out32 (optional): the same entries rounded to FP32 (mixed path).
 template <int MODE, typename OutT>
 __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
                                                int rows,
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
         {
             out[static_cast<int64_t>(gi) * ldo + gj] = static_cast<OutT>(val);
         }
-        if (MODE == 0 && inside && out32 != nullptr)
+        if (inside && out32 != nullptr)
         {
             out32[static_cast<int64_t>(gi) * ld32 + gj] = static_cast<float>(val);
         }
@@ -312,6 +312,67 @@ void assemble_cross_f32(const double *xt, int m, const double *x, int n, int n_r
         throw Error(1, "assemble_cross: mean_parts must be ceil(n/128)");
     }
     launch_se<1>(xt, m, x, n, n_reg, 1, p, Kx, ldx, alpha, mean_partial, mean_parts, s, row_offsets);
+}
+
+void assemble_cross_dual(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p,
+                         double *Kx, int64_t ldx, float *Kx32, int64_t ld32, cudaStream_t s)
+{
+    launch_se<1>(xt, m, x, n, n_reg, 1, p, Kx, ldx, nullptr, nullptr, 0, s, nullptr, Kx32, ld32);
+}
+
+namespace
+{
+// mean[r] = sum_c Kx[r][c] alpha[c]: one warp per row, 16-byte loads, a fixed
+// summation order (deterministic).  HBM-bound: reads Kx once.
+constexpr int MV_WARPS = 8;
+
+__global__ void __launch_bounds__(32 * MV_WARPS) cross_mv_kernel(const double *__restrict__ Kx, int64_t ldx, int m,
+                                                                 int n, const double *__restrict__ alpha,
+                                                                 double *__restrict__ mean)
+{
+    const int r = blockIdx.x * MV_WARPS + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= m)
+    {
+        return;
+    }
+    const double *row = Kx + static_cast<int64_t>(r) * ldx;
+    double s = 0.0;
+    const int n2 = n & ~1;
+    for (int c = 2 * lane; c < n2; c += 64)
+    {
+        const double2 k = *reinterpret_cast<const double2 *>(row + c);
+        const double2 a = *reinterpret_cast<const double2 *>(alpha + c);
+        s += k.x * a.x + k.y * a.y;
+    }
+    if ((n & 1) && lane == 0)
+    {
+        s += row[n - 1] * alpha[n - 1];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    }
+    if (lane == 0)
+    {
+        mean[r] = s;
+    }
+}
+}  // namespace
+
+void cross_times_alpha(const double *Kx, int64_t ldx, int m, int n, const double *alpha, double *mean, cudaStream_t s)
+{
+    if (m <= 0)
+    {
+        return;
+    }
+    if ((ldx & 1) != 0 || (reinterpret_cast<uintptr_t>(Kx) & 15) != 0 || (reinterpret_cast<uintptr_t>(alpha) & 15) != 0)
+    {
+        throw Error(1, "cross_times_alpha: Kx and alpha must be 16-byte aligned with an even leading dimension");
+    }
+    cross_mv_kernel<<<ceil_div(m, MV_WARPS), 32 * MV_WARPS, 0, s>>>(Kx, ldx, m, n, alpha, mean);
+    GPRAT_LAUNCH_CHECK();
 }
 
 void reduce_mean(const double *mean_partial, int m, int parts, double *mean, cudaStream_t s)

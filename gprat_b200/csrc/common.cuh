@@ -196,6 +196,11 @@ void assemble_cross(const double *xt, int m, const double *x, int n, int n_reg, 
 void assemble_cross_f32(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p, float *Kx,
                         int64_t ldx, const double *alpha, double *mean_partial, int mean_parts, cudaStream_t s,
                         const int64_t *row_offsets = nullptr);
+// Cross covariance in FP64 (Kx, ldx) and its FP32 twin (Kx32, ld32) in one pass.
+void assemble_cross_dual(const double *xt, int m, const double *x, int n, int n_reg, const DeviceParams *p,
+                         double *Kx, int64_t ldx, float *Kx32, int64_t ld32, cudaStream_t s);
+// mean = Kx alpha (m rows of Kx, n columns; deterministic).
+void cross_times_alpha(const double *Kx, int64_t ldx, int m, int n, const double *alpha, double *mean, cudaStream_t s);
 void reduce_mean(const double *mean_partial, int m, int parts, double *mean, cudaStream_t s);
 
 // Prior covariance matrix K**[r][c] = k(xt_r, xt_c) (gen_tile_full_prior_covariance,

@@ -454,8 +454,8 @@ void ensure_lookahead(gprat_cu_gp *gp, int nevents)
 }
 
 // Events of one factorisation (two per outer panel of at least one block,
-// one to start) and six for fit_predict_mixed, at the end.
-int lookahead_events(int n) { return 2 * ceil_div(n, NB) + 7; }
+// one to start) and seven for fit_predict_mixed, at the end.
+int lookahead_events(int n) { return 2 * ceil_div(n, NB) + 8; }
 
 TcGemmArgs limited(TcGemmArgs a, int max_ctas)
 {
@@ -861,13 +861,14 @@ void variance_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
 //     GPRAT_VARIANCE_EARLY_PERCENT % of the SMs; the rest once the factor is
 //     complete, on GPRAT_VARIANCE_PERCENT %;
 //   side stream, after the factorisation: alpha's refinement (FP64 PCG) and
-//     the mean.
+//     the mean (from K* kept in FP64 by the variance stream's assembly).
 // `s` waits for both at the end.
 void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
 {
     const int n = gp->n;
     const int ne = lookahead_events(n);
     ensure_lookahead(gp, ne);
+    cudaEvent_t kx_ready = gp->events[ne - 7];
     cudaEvent_t begin = gp->events[ne - 6], half = gp->events[ne - 5], three_q = gp->events[ne - 4];
     cudaEvent_t factored = gp->events[ne - 3], refined = gp->events[ne - 2], solved = gp->events[ne - 1];
     cudaStream_t side = gp->side, vs = gp->vstream;
@@ -880,6 +881,10 @@ void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mea
     gp->mean_part.ensure(static_cast<int64_t>(std::max(m, 1)) * parts);
     gp->W32.ensure(static_cast<int64_t>(std::max(m, 1)) * gp->ld32);
     gp->vacc.ensure(2 * static_cast<int64_t>(std::max(m, 1)));
+    if (early)
+    {
+        gp->W.ensure(static_cast<int64_t>(m) * gp->ld);  // K* in FP64, for the mean
+    }
     if (gp->precision == GPRAT_CU_PREC_MIXED_BF16)
     {
         gp->Wb.ensure(static_cast<int64_t>(std::max(m, 1)) * gp->ld32);
@@ -905,9 +910,11 @@ void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mea
             float *W = gp->W32.ptr;
             const int64_t ld32 = gp->ld32;
             {
+                // K* once, in FP64 (kept for the mean: a mat-vec with alpha
+                // once alpha is refined, instead of a second assembly) and FP32
                 StepScope step("prediction", vs);
-                assemble_cross_f32(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, W, ld32, nullptr, nullptr, parts,
-                                   vs, nullptr);
+                assemble_cross_dual(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, gp->W.ptr, gp->ld, W, ld32, vs);
+                GPRAT_CUDA_CHECK(cudaEventRecord(kx_ready, vs));
             }
             StepScope step("forward KcK", vs);
             GPRAT_CUDA_CHECK(cudaMemsetAsync(gp->vacc.ptr, 0, 2 * m * sizeof(double), vs));
@@ -944,9 +951,17 @@ void fit_predict_mixed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mea
     if (m > 0)
     {
         StepScope step("prediction", side);
-        assemble_cross(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, nullptr, 0, gp->alpha.ptr, gp->mean_part.ptr,
-                       parts, side, nullptr);
-        reduce_mean(gp->mean_part.ptr, m, parts, d_mean, side);
+        if (early)
+        {
+            GPRAT_CUDA_CHECK(cudaStreamWaitEvent(side, kx_ready, 0));
+            cross_times_alpha(gp->W.ptr, gp->ld, m, n, gp->alpha.ptr, d_mean, side);
+        }
+        else
+        {
+            assemble_cross(d_xt, m, gp->x.ptr, n, gp->d, gp->params.ptr, nullptr, 0, gp->alpha.ptr,
+                           gp->mean_part.ptr, parts, side, nullptr);
+            reduce_mean(gp->mean_part.ptr, m, parts, d_mean, side);
+        }
     }
     GPRAT_CUDA_CHECK(cudaEventRecord(refined, side));
     GPRAT_CUDA_CHECK(cudaStreamWaitEvent(s, refined, 0));
