@@ -1,23 +1,26 @@
 // Mixed-precision pipeline (GPRAT_CU_PREC_MIXED_TF32 / _BF16).
 //
-// Factorisation: K is assembled in FP64 and copied to an FP32 working matrix
-// K32.  Two-level right-looking blocked Cholesky as in the FP64 path, but
+// Factorisation (factor_mixed): K in FP64 and its FP32 working copy K32 in one
+// pass; right-looking blocked Cholesky of
+// K32 in outer panels of 1024 columns with a look-ahead of one panel, inside
+// a panel left-looking over 128-column blocks:
 //   - each 128 x 128 diagonal block is factored and inverted in FP64
-//     (potrf_diag on an FP64 copy), its FP64 diagonal kept for the
-//     log-determinant;
-//   - the panel solves P = P Linv^T run on the tcgen05 tensor cores (TF32
-//     operands, FP32 accumulation in TMEM), in place;
-//   - the inner (K = 128) and outer (K = 512) trailing updates run on the
-//     tcgen05 tensor cores with TF32 operands (MIXED_TF32) or BF16 operands
-//     (MIXED_BF16, from a BF16 copy of the factor), FP32 accumulation.
-// alpha: preconditioned conjugate gradients in FP64 on the exact FP64 K
-// (a lower-storage symmetric mat-vec), preconditioned by the low-precision
-// factor, to a relative residual of 1e-12.  The loss uses that alpha and
-// the FP64 diagonal of the factor.
-// Mean: FP64 cross covariance fused with the refined alpha.
-// Variance: the cross covariance stored in FP32 and the solve W L^T = K*
-// on the tensor cores with the same two-level blocking, row sums of W^2
-// accumulated in FP64.  Its error is that of the low-precision factor.
+//     (potrf_diag_f32), its FP64 diagonal kept for the log-determinant, its
+//     inverse stored in FP32;
+//   - panel solves P = P Linv^T and all updates run on the tcgen05 tensor
+//     cores with TF32 operands (MIXED_TF32) or BF16 operands (MIXED_BF16, from
+//     a BF16 copy of the factor), FP32 accumulation in TMEM.
+// alpha (alpha_mixed): preconditioned conjugate gradients in FP64 on the
+// exact FP64 K (a lower-storage symmetric mat-vec), preconditioned by the
+// low-precision factor, to a relative residual of 1e-12.  The loss uses that
+// alpha and the FP64 diagonal of the factor.
+// Mean: the FP64 cross covariance with the refined alpha.
+// Variance (variance_mixed, fit_predict_mixed): the cross covariance in FP32
+// and the solve W L^T = K* on the tensor cores (recursive halving, or
+// 512-column panels for few rows), row sums of W^2 accumulated in FP64.  Its
+// error is that of the low-precision factor.
+// fit_predict_mixed overlaps the variance solve with the factorisation and
+// alpha's refinement on separate streams.
 #include "gp_state.cuh"
 
 #include <cmath>
