@@ -9,7 +9,7 @@ Stated tolerances (error of this path, not of the reference):
 7.3e-3 and 2.1e-2 for the variance.)
 The variance and the log-determinant carry the error of the low-precision
 factor; alpha, and with it the mean and the data-fit term, are refined to a
-1e-12 relative residual.
+1e-10 relative residual.
 """
 import numpy as np
 import pytest
