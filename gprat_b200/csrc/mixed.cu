@@ -734,6 +734,10 @@ struct VarianceSolve
     // W[:, cols) -= W[:, k0:k1) L[cols, k0:k1)^T
     void update(int k0, int k1, int c0, int c1) const
     {
+        if (k1 <= k0 || c1 <= c0)
+        {
+            return;
+        }
         tc_gemm(wt(), ops.trail(),
                 limited(tc_args(m, c1 - c0, k1 - k0, 0, k0, c0, k0, W + c0, ld32, -1.0f, 1.0f, false, nullptr,
                                 gp->status.ptr),
@@ -773,6 +777,10 @@ struct VarianceSolve
     // panels of the factorisation would read and write it n / 512 times).
     void solve(int c0, int c1) const
     {
+        if (c1 <= c0)
+        {
+            return;  // an empty range (a split of a factor with fewer than four blocks)
+        }
         if (c1 - c0 <= NB)
         {
             leaf(c0);

@@ -110,3 +110,20 @@ def test_mixed_variance_recursive_solve(capi, problem, prec):
     assert np.max(np.abs(var2 - ov2) / ov2) <= VAR_TOL[prec]
     mean1, var1 = gp.predict_with_uncertainty(p["h"], xt2[: 512 + p["d"]], 1, 512)
     assert np.max(np.abs(var1 - var2[:512]) / ov2[:512]) <= VAR_TOL[prec]
+
+
+@pytest.mark.parametrize("n", [128, 256, 384])
+def test_mixed_overlapped_pipeline_small_factor(capi, n):
+    """predict_with_uncertainty with 2048 test rows or more starts the variance
+    solve beside the factorisation at fixed splits of the columns; with one to
+    three 128-column blocks some of those ranges are empty."""
+    m, d, T = 2048, 8, 128
+    h = (1.0, 1.0, 0.1)
+    x, y, xt = O.synthetic(n, m, d)
+    o = O.OracleGP(x, y, n // T, T, d, h)
+    om, ov = o.predict_with_uncertainty(xt, 1, m)
+    gp = capi.CudaGP(x, y, n // T, T, d)
+    gp.set_precision(capi.PREC_MIXED_TF32)
+    mean, var = gp.predict_with_uncertainty(h, xt, 1, m)
+    assert np.max(np.abs(mean - om)) / np.max(np.abs(om)) <= 1e-8
+    assert np.max(np.abs(var - ov) / ov) <= VAR_TOL[1]
