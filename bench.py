@@ -397,9 +397,9 @@ PRECISIONS = {"fp64": 0, "mixed-tf32": 1, "mixed-bf16": 2}
 TRAFFIC_SAMPLE = {
     "mixed-tf32": {
         "launch": "tc_gemm_pair_kernel<TF32>, trailing update after panel 0 at n_train=16384: "
-                  "lower 15360 x 15360, K=512, 51 CTA pairs",
-        "dram_bytes": 520.9e6 + 416.5e6,
-        "algorithmic_bytes": 2 * 15360 * 15361 / 2 * 4 + 15360 * 512 * 4,
+                  "lower 14336 x 14336, K=1024, 51 CTA pairs",
+        "dram_bytes": 587.0e6 + 378.9e6,
+        "algorithmic_bytes": 2 * 14336 * 14337 / 2 * 4 + 14336 * 1024 * 4,
         "source": "profiles/tc_gemm_trailing_update_c1.md",
     },
     "fp64": {
