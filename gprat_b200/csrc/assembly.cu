@@ -136,6 +136,12 @@ __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
         int g = j0 + q;
         xc[q] = (g < cols + d - 1) ? xcol[g] : 0.0;
     }
+    // mode 0: first column past the tile of each row (one division per row, not per entry)
+    __shared__ int rowlim[AR];
+    if (MODE == 0 && threadIdx.x < AR)
+    {
+        rowlim[threadIdx.x] = ((i0 + threadIdx.x) / T + 1) * T;
+    }
     __syncthreads();
 
     const double l = p->hyper[0];
@@ -155,7 +161,7 @@ __global__ void __launch_bounds__(AC) se_kernel(const double *__restrict__ xrow,
         bool inside = gi < rows && gj < cols;
         if (MODE == 0)
         {
-            inside = inside && (gj / T <= gi / T);
+            inside = inside && (gj < rowlim[r]);  // tile of column gj at or left of gi's tile
             if (gi == gj)
             {
                 val += noise;
