@@ -88,6 +88,14 @@ def _load() -> ctypes.CDLL:
                                                _dp, _i64p]
     lib.gprat_cu_server_wait.argtypes = [_vp, _i64, _dp, _dp, _ip, _dp]
     lib.gprat_cu_server_stats.argtypes = [_vp, _dp, _dp, _dp, _i64p, _i64p]
+    lib.gprat_cu_multiserver_create.argtypes = [_ip, ctypes.c_int, _i64, ctypes.c_int, ctypes.POINTER(_vp)]
+    lib.gprat_cu_multiserver_destroy.argtypes = [_vp]
+    lib.gprat_cu_multiserver_add_model.argtypes = lib.gprat_cu_server_add_model.argtypes
+    lib.gprat_cu_multiserver_submit_predict.argtypes = lib.gprat_cu_server_submit_predict.argtypes
+    lib.gprat_cu_multiserver_submit_fit.argtypes = lib.gprat_cu_server_submit_fit.argtypes
+    lib.gprat_cu_multiserver_wait.argtypes = lib.gprat_cu_server_wait.argtypes
+    lib.gprat_cu_multiserver_stats.argtypes = lib.gprat_cu_server_stats.argtypes
+    lib.gprat_cu_multiserver_replica_completed.argtypes = [_vp, ctypes.c_int, _i64p]
     return lib
 
 

@@ -1,9 +1,12 @@
-"""Serving front end over the C ABI's gprat_cu_server_* entry points.
+"""Serving front end over the C ABI's gprat_cu_server_* and
+gprat_cu_multiserver_* entry points.
 
 A :class:`Server` keeps fitted GP models resident on one GPU (factor and
-weights stay in HBM) and answers asynchronous predict and fit requests.  The
-batching, scheduling and memory admission run natively in the library
-(gprat_b200/csrc/serve.cu); this module only marshals arrays.  There is no
+weights stay in HBM) and answers asynchronous predict and fit requests.  A
+:class:`MultiServer` replicates every model on several GPUs and spreads the
+predict requests over them.  The batching, scheduling, memory admission and
+replica routing run natively in the library (gprat_b200/csrc/serve.cu,
+multiserve.cu); this module only marshals arrays.  There is no
 counterpart in the reference, whose predict calls re-factorise the training
 covariance every time (core/src/cpu/gp_functions.cpp:110-189).
 """
@@ -37,17 +40,25 @@ class Server:
     device memory free at creation.
     """
 
+    _PREFIX = "gprat_cu_server_"
+
     def __init__(self, device: int = 0, memory_budget_bytes: int = 0, precision: int = capi.PREC_FP64):
         h = ctypes.c_void_p()
         capi.check(capi.lib.gprat_cu_server_create(int(device), int(memory_budget_bytes), int(precision),
                                                    ctypes.byref(h)))
+        self._init_handle(h)
+
+    def _init_handle(self, h: ctypes.c_void_p) -> None:
         self._h = h
         self._m = {}      # request id -> number of test points (0 for fits)
         self._reg = {}    # model id -> regressors
 
+    def _fn(self, name: str):
+        return getattr(capi.lib, self._PREFIX + name)
+
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
-            capi.check(capi.lib.gprat_cu_server_destroy(self._h))
+            capi.check(self._fn("destroy")(self._h))
         self._h = None
 
     def __enter__(self):
@@ -67,7 +78,7 @@ class Server:
         """Fits a model synchronously; returns its id."""
         x, y, hy = capi._arr(x), capi._arr(y), capi._hyper(hyper)
         mid = ctypes.c_int()
-        capi.check(capi.lib.gprat_cu_server_add_model(self._h, capi._p(x), x.size, capi._p(y), y.size, int(n_tiles),
+        capi.check(self._fn("add_model")(self._h, capi._p(x), x.size, capi._p(y), y.size, int(n_tiles),
                                                       int(n_tile_size), int(n_reg), capi._p(hy), ctypes.byref(mid)))
         self._reg[mid.value] = int(n_reg)
         return mid.value
@@ -78,7 +89,7 @@ class Server:
         if m is None:
             m = xt.size - self._reg.get(model_id, 1) + 1
         rid = ctypes.c_int64()
-        capi.check(capi.lib.gprat_cu_server_submit_predict(self._h, int(model_id), capi._p(xt), xt.size, int(m),
+        capi.check(self._fn("submit_predict")(self._h, int(model_id), capi._p(xt), xt.size, int(m),
                                                            ctypes.byref(rid)))
         self._m[rid.value] = int(m)
         return rid.value
@@ -88,7 +99,7 @@ class Server:
         """Queues the fit of a new model; wait() on the id returns the model id."""
         x, y, hy = capi._arr(x), capi._arr(y), capi._hyper(hyper)
         rid = ctypes.c_int64()
-        capi.check(capi.lib.gprat_cu_server_submit_fit(self._h, capi._p(x), x.size, capi._p(y), y.size, int(n_tiles),
+        capi.check(self._fn("submit_fit")(self._h, capi._p(x), x.size, capi._p(y), y.size, int(n_tiles),
                                                        int(n_tile_size), int(n_reg), capi._p(hy), ctypes.byref(rid)))
         self._m[rid.value] = 0
         self._reg[("fit", rid.value)] = int(n_reg)
@@ -103,7 +114,7 @@ class Server:
         var = np.empty(m) if m else None
         mid = ctypes.c_int()
         lat = ctypes.c_double()
-        capi.check(capi.lib.gprat_cu_server_wait(self._h, int(request_id), capi._p(mean) if m else None,
+        capi.check(self._fn("wait")(self._h, int(request_id), capi._p(mean) if m else None,
                                                  capi._p(var) if m else None, ctypes.byref(mid), ctypes.byref(lat)))
         n_reg = self._reg.pop(("fit", request_id), None)
         if n_reg is not None:
@@ -113,6 +124,35 @@ class Server:
     def stats(self) -> ServerStats:
         p50, p99, pps = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         done, batches = ctypes.c_int64(), ctypes.c_int64()
-        capi.check(capi.lib.gprat_cu_server_stats(self._h, ctypes.byref(p50), ctypes.byref(p99), ctypes.byref(pps),
+        capi.check(self._fn("stats")(self._h, ctypes.byref(p50), ctypes.byref(p99), ctypes.byref(pps),
                                                   ctypes.byref(done), ctypes.byref(batches)))
         return ServerStats(p50.value, p99.value, pps.value, done.value, batches.value)
+
+
+class MultiServer(Server):
+    """Replica serving over several devices (one server per entry of
+    ``devices``; a device may repeat).  Every model is fitted on each replica
+    and keeps one model id; a predict request goes to the replica with the
+    fewest test points outstanding and its result is bit-identical to the same
+    request on a single :class:`Server`.  memory_budget_bytes and precision
+    apply to each replica."""
+
+    _PREFIX = "gprat_cu_multiserver_"
+
+    def __init__(self, devices: Sequence[int] = (0,), memory_budget_bytes: int = 0,
+                 precision: int = capi.PREC_FP64):
+        devs = (ctypes.c_int * len(devices))(*[int(d) for d in devices])
+        h = ctypes.c_void_p()
+        capi.check(capi.lib.gprat_cu_multiserver_create(devs, len(devices), int(memory_budget_bytes),
+                                                        int(precision), ctypes.byref(h)))
+        self.n_replicas = len(devices)
+        self._init_handle(h)
+
+    def replica_completed(self) -> list:
+        """Predict requests waited on, per replica that served them."""
+        out = []
+        for r in range(self.n_replicas):
+            c = ctypes.c_int64()
+            capi.check(capi.lib.gprat_cu_multiserver_replica_completed(self._h, r, ctypes.byref(c)))
+            out.append(c.value)
+        return out

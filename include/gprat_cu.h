@@ -346,6 +346,69 @@ int gprat_cu_server_stats(gprat_cu_server *server,
                           int64_t *completed,
                           int64_t *batches);
 
+/*
+ * Replica serving over several GPUs (no counterpart in the reference): one
+ * server per entry of devices (a device may repeat), every model replicated
+ * on each.  Test points are independent given a model's factor and alpha, so
+ * predict throughput scales with the replicas and no data crosses between
+ * GPUs.  add_model and submit_fit run on every replica (the pipeline is
+ * deterministic, so the copies are identical) and yield one model id;
+ * submit_predict goes to the replica with the fewest test points submitted
+ * and not yet waited on.  A predict result is bit-identical to the same
+ * request on a single server.  wait/stats as for a server: latencies are the
+ * serving replica's (a fit's is its slowest replica's), predictions_per_s
+ * and batches are summed over the replicas.  replica_completed: predict
+ * requests waited on that replica served.  memory_budget_bytes and
+ * precision apply to each replica.
+ */
+typedef struct gprat_cu_multiserver gprat_cu_multiserver;
+
+int gprat_cu_multiserver_create(const int *devices,
+                                int n_devices,
+                                int64_t memory_budget_bytes,
+                                int precision,
+                                gprat_cu_multiserver **out);
+int gprat_cu_multiserver_destroy(gprat_cu_multiserver *server);
+int gprat_cu_multiserver_add_model(gprat_cu_multiserver *server,
+                                   const double *train_in,
+                                   int64_t n_in,
+                                   const double *train_out,
+                                   int64_t n_out,
+                                   int n_tiles,
+                                   int n_tile_size,
+                                   int n_regressors,
+                                   const double hyper[3],
+                                   int *model_id);
+int gprat_cu_multiserver_submit_predict(gprat_cu_multiserver *server,
+                                        int model_id,
+                                        const double *test_in,
+                                        int64_t n_test_in,
+                                        int m,
+                                        int64_t *request_id);
+int gprat_cu_multiserver_submit_fit(gprat_cu_multiserver *server,
+                                    const double *train_in,
+                                    int64_t n_in,
+                                    const double *train_out,
+                                    int64_t n_out,
+                                    int n_tiles,
+                                    int n_tile_size,
+                                    int n_regressors,
+                                    const double hyper[3],
+                                    int64_t *request_id);
+int gprat_cu_multiserver_wait(gprat_cu_multiserver *server,
+                              int64_t request_id,
+                              double *mean,
+                              double *var,
+                              int *model_id,
+                              double *latency_ms);
+int gprat_cu_multiserver_stats(gprat_cu_multiserver *server,
+                               double *p50_ms,
+                               double *p99_ms,
+                               double *predictions_per_s,
+                               int64_t *completed,
+                               int64_t *batches);
+int gprat_cu_multiserver_replica_completed(gprat_cu_multiserver *server, int replica, int64_t *completed);
+
 #ifdef __cplusplus
 }
 #endif
