@@ -30,6 +30,9 @@ PREC_FP64 = 0
 PREC_MIXED_TF32 = 1
 PREC_MIXED_BF16 = 2
 
+REPLICATE_COPY = 0
+REPLICATE_REFIT = 1
+
 
 class GpratCudaError(RuntimeError):
     def __init__(self, code: int, message: str):
@@ -96,6 +99,7 @@ def _load() -> ctypes.CDLL:
     lib.gprat_cu_multiserver_wait.argtypes = lib.gprat_cu_server_wait.argtypes
     lib.gprat_cu_multiserver_stats.argtypes = lib.gprat_cu_server_stats.argtypes
     lib.gprat_cu_multiserver_replica_completed.argtypes = [_vp, ctypes.c_int, _i64p]
+    lib.gprat_cu_multiserver_set_replication.argtypes = [_vp, ctypes.c_int]
     return lib
 
 

@@ -551,6 +551,87 @@ void gp_reserve_predict(gprat_cu_gp *gp, int m)
     }
 }
 
+namespace
+{
+// dst takes src's capacity; the contents follow unless `contents` is false.
+template <typename T>
+int64_t copy_buf(gprat_cu_gp *dst, DevBuf<T> &d, const gprat_cu_gp *src, const DevBuf<T> &b, bool contents)
+{
+    if (b.cap == 0)
+    {
+        return 0;
+    }
+    d.ensure(b.cap);
+    if (!contents)
+    {
+        return 0;
+    }
+    const size_t bytes = static_cast<size_t>(b.cap) * sizeof(T);
+    if (dst->device == src->device)
+    {
+        GPRAT_CUDA_CHECK(cudaMemcpyAsync(d.ptr, b.ptr, bytes, cudaMemcpyDeviceToDevice, dst->stream));
+    }
+    else
+    {
+        GPRAT_CUDA_CHECK(cudaMemcpyPeerAsync(d.ptr, dst->device, b.ptr, src->device, bytes, dst->stream));
+    }
+    return static_cast<int64_t>(bytes);
+}
+}  // namespace
+
+int64_t gp_copy_fitted(gprat_cu_gp *dst, gprat_cu_gp *src)
+{
+    if (dst->n != src->n || dst->T != src->T || dst->d != src->d || dst->n_in != src->n_in ||
+        dst->ld != src->ld || dst->ld32 != src->ld32 || dst->precision != src->precision)
+    {
+        throw Error(GPRAT_CU_ERR_INVALID_ARG, "model copy between handles of different shape or precision");
+    }
+    {
+        DeviceGuard guard(src->device);
+        for (cudaStream_t st : { src->stream, src->side, src->vstream })
+        {
+            if (st != nullptr)
+            {
+                GPRAT_CUDA_CHECK(cudaStreamSynchronize(st));
+            }
+        }
+    }
+    DeviceGuard guard(dst->device);
+    int64_t bytes = 0;
+    // fitted state: training data, factor (FP64 and low-precision copies),
+    // diagonal-block inverses, alpha, parameters, status, solver scratch
+    for (auto pr : { std::make_pair(&dst->x, &src->x), std::make_pair(&dst->y, &src->y),
+                     std::make_pair(&dst->K, &src->K), std::make_pair(&dst->Linv, &src->Linv),
+                     std::make_pair(&dst->alpha, &src->alpha), std::make_pair(&dst->U, &src->U),
+                     std::make_pair(&dst->partials, &src->partials), std::make_pair(&dst->losses, &src->losses),
+                     std::make_pair(&dst->D64, &src->D64), std::make_pair(&dst->pcg_r, &src->pcg_r),
+                     std::make_pair(&dst->pcg_z, &src->pcg_z), std::make_pair(&dst->pcg_p, &src->pcg_p),
+                     std::make_pair(&dst->pcg_q, &src->pcg_q), std::make_pair(&dst->symv_part, &src->symv_part),
+                     std::make_pair(&dst->trsv_b, &src->trsv_b) })
+    {
+        bytes += copy_buf(dst, *pr.first, src, *pr.second, true);
+    }
+    bytes += copy_buf(dst, dst->K32, src, src->K32, true);
+    bytes += copy_buf(dst, dst->Linv32, src, src->Linv32, true);
+    bytes += copy_buf(dst, dst->Lb, src, src->Lb, true);
+    bytes += copy_buf(dst, dst->pcg_s, src, src->pcg_s, true);
+    bytes += copy_buf(dst, dst->flags, src, src->flags, true);
+    bytes += copy_buf(dst, dst->params, src, src->params, true);
+    bytes += copy_buf(dst, dst->status, src, src->status, true);
+    // per-batch predict working set: same capacity, no contents
+    for (auto pr : { std::make_pair(&dst->xt, &src->xt), std::make_pair(&dst->W, &src->W),
+                     std::make_pair(&dst->vacc, &src->vacc), std::make_pair(&dst->mean_part, &src->mean_part),
+                     std::make_pair(&dst->mean, &src->mean), std::make_pair(&dst->var, &src->var) })
+    {
+        copy_buf(dst, *pr.first, src, *pr.second, false);
+    }
+    copy_buf(dst, dst->W32, src, src->W32, false);
+    copy_buf(dst, dst->Wb, src, src->Wb, false);
+    GPRAT_CUDA_CHECK(cudaStreamSynchronize(dst->stream));
+    dst->pcg_last_iters = src->pcg_last_iters;
+    return bytes;
+}
+
 int64_t gp_predict_bytes(const gprat_cu_gp *gp, int m)
 {
     // solve matrix + mean partials + variance accumulator for m rows

@@ -189,6 +189,12 @@ int64_t gp_resident_bytes(const gprat_cu_gp *gp);
 int64_t gp_predict_bytes(const gprat_cu_gp *gp, int m);
 // Allocates the predict working set for m test points now (no later growth).
 void gp_reserve_predict(gprat_cu_gp *gp, int m);
+// Makes dst (created with the same training data, tiling and precision,
+// possibly on another device) hold src's fitted state: every device buffer
+// src has allocated is allocated in dst and, except the per-batch predict
+// working set, copied over (peer copies across devices).  src must be idle.
+// Returns the bytes copied.
+int64_t gp_copy_fitted(gprat_cu_gp *dst, gprat_cu_gp *src);
 void loss_mixed(gprat_cu_gp *gp, cudaStream_t s);
 
 }  // namespace gprat_cu

@@ -2,12 +2,16 @@
 // (serve.cu), every model replicated on each, predict requests sent to the
 // replica with the fewest test points outstanding.  Test points are
 // independent given a model's factor and alpha, so this scales predict
-// throughput with the number of GPUs with no change to the algorithm; fits
-// run on every replica (the pipeline is deterministic, so the replicas hold
-// identical models).  No counterpart in the reference.
+// throughput with the number of GPUs with no change to the algorithm.  A
+// model is fitted once, on the first replica, and its fitted state (factor,
+// alpha, training data) is copied to the others over NVLink (peer copies,
+// copy engines only), or, in the refit mode, fitted on every replica at once
+// (the pipeline is deterministic, so the copies are identical either way).
+// No counterpart in the reference.
 #include "gp_state.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -18,6 +22,9 @@
 namespace gprat_cu
 {
 void set_last_error(const std::string &message);
+int server_add_model_copy(gprat_cu_server *dst, gprat_cu_server *src, int src_model, const double *train_in,
+                          int64_t n_in, const double *train_out, int64_t n_out, int n_tiles, int n_tile_size,
+                          int n_regressors, int *model_id);
 }
 
 using namespace gprat_cu;
@@ -32,6 +39,9 @@ struct Pending
     int64_t rows = 0;                // predict: test points (load accounting)
     int model = -1;                  // predict: the global model id
     std::vector<int64_t> local_ids;  // per replica (fit) or one (predict)
+    // fit in the copy mode: the training data and tiling for the copies
+    std::vector<double> x, y;
+    int n_tiles = 0, T = 0, d = 0;
 };
 
 }  // namespace
@@ -47,6 +57,7 @@ struct gprat_cu_multiserver
     std::unordered_map<int64_t, Pending> pending;
     std::vector<double> latencies_ms;
     int64_t next_id = 1;
+    int replication = GPRAT_CU_REPLICATE_COPY;
 };
 
 namespace
@@ -127,6 +138,54 @@ void on_every_replica(gprat_cu_multiserver *ms, F &&f)
     }
 }
 
+// Copies replica 0's model id0 to every other replica; ids[0] = id0.
+void copy_to_replicas(gprat_cu_multiserver *ms, int id0, const double *x, int64_t nx, const double *y, int64_t ny,
+                      int n_tiles, int T, int d, std::vector<int> &ids)
+{
+    ids.assign(ms->servers.size(), -1);
+    ids[0] = id0;
+    on_every_replica(ms,
+                     [&](int r)
+                     {
+                         if (r == 0)
+                         {
+                             return static_cast<int>(GPRAT_CU_OK);
+                         }
+                         return server_add_model_copy(ms->servers[r], ms->servers[0], id0, x, nx, y, ny, n_tiles, T,
+                                                      d, &ids[r]);
+                     });
+}
+
+// Lets each replica's device read every other replica's memory directly
+// (NVLink), where the devices differ and support it.
+void enable_peer_access(const std::vector<int> &devices)
+{
+    int prev = 0;
+    cudaGetDevice(&prev);
+    for (int a : devices)
+    {
+        for (int b : devices)
+        {
+            int can = 0;
+            if (a == b || cudaDeviceCanAccessPeer(&can, a, b) != cudaSuccess || !can)
+            {
+                continue;
+            }
+            cudaSetDevice(a);
+            const cudaError_t e = cudaDeviceEnablePeerAccess(b, 0);
+            if (e == cudaErrorPeerAccessAlreadyEnabled)
+            {
+                cudaGetLastError();
+            }
+            else
+            {
+                GPRAT_CUDA_CHECK(e);
+            }
+        }
+    }
+    cudaSetDevice(prev);
+}
+
 }  // namespace
 
 extern "C" {
@@ -159,6 +218,18 @@ int gprat_cu_multiserver_create(const int *devices, int n_devices, int64_t memor
             }
             ms->outstanding.assign(n_devices, 0);
             ms->completed.assign(n_devices, 0);
+            try
+            {
+                enable_peer_access(ms->devices);
+            }
+            catch (...)
+            {
+                for (gprat_cu_server *sv : ms->servers)
+                {
+                    gprat_cu_server_destroy(sv);
+                }
+                throw;
+            }
             *out = ms.release();
         });
 }
@@ -189,12 +260,23 @@ int gprat_cu_multiserver_add_model(gprat_cu_multiserver *ms, const double *train
         {
             require_ms(ms != nullptr && model_id != nullptr, "arguments must not be NULL");
             std::vector<int> ids(ms->servers.size(), -1);
-            on_every_replica(ms,
-                             [&](int r)
-                             {
-                                 return gprat_cu_server_add_model(ms->servers[r], train_in, n_in, train_out, n_out,
-                                                                  n_tiles, n_tile_size, n_regressors, hyper, &ids[r]);
-                             });
+            if (ms->replication == GPRAT_CU_REPLICATE_COPY)
+            {
+                int id0 = -1;
+                check_rc(gprat_cu_server_add_model(ms->servers[0], train_in, n_in, train_out, n_out, n_tiles,
+                                                   n_tile_size, n_regressors, hyper, &id0));
+                copy_to_replicas(ms, id0, train_in, n_in, train_out, n_out, n_tiles, n_tile_size, n_regressors, ids);
+            }
+            else
+            {
+                on_every_replica(ms,
+                                 [&](int r)
+                                 {
+                                     return gprat_cu_server_add_model(ms->servers[r], train_in, n_in, train_out,
+                                                                      n_out, n_tiles, n_tile_size, n_regressors,
+                                                                      hyper, &ids[r]);
+                                 });
+            }
             std::lock_guard<std::mutex> lk(ms->mtx);
             ms->model_ids.push_back(ids);
             *model_id = static_cast<int>(ms->model_ids.size()) - 1;
@@ -253,8 +335,19 @@ int gprat_cu_multiserver_submit_fit(gprat_cu_multiserver *ms, const double *trai
             require_ms(ms != nullptr && request_id != nullptr, "arguments must not be NULL");
             Pending p;
             p.fit = true;
-            p.local_ids.assign(ms->servers.size(), 0);
-            for (size_t r = 0; r < ms->servers.size(); ++r)
+            const bool copy = ms->replication == GPRAT_CU_REPLICATE_COPY;
+            if (copy)
+            {
+                require_ms(train_in != nullptr && train_out != nullptr && n_in >= 0 && n_out >= 0,
+                           "arguments must not be NULL");
+                p.x.assign(train_in, train_in + n_in);
+                p.y.assign(train_out, train_out + n_out);
+                p.n_tiles = n_tiles;
+                p.T = n_tile_size;
+                p.d = n_regressors;
+            }
+            p.local_ids.assign(copy ? 1 : ms->servers.size(), 0);
+            for (size_t r = 0; r < p.local_ids.size(); ++r)
             {
                 const int rc = gprat_cu_server_submit_fit(ms->servers[r], train_in, n_in, train_out, n_out, n_tiles,
                                                           n_tile_size, n_regressors, hyper, &p.local_ids[r]);
@@ -313,16 +406,28 @@ int gprat_cu_multiserver_wait(gprat_cu_multiserver *ms, int64_t request_id, doub
             // a fit: every replica's copy, then one global model id
             std::vector<int> ids(ms->servers.size(), -1);
             double worst = 0.0;
-            std::vector<double> lats(ms->servers.size(), 0.0);
-            on_every_replica(ms,
-                             [&](int r)
-                             {
-                                 return gprat_cu_server_wait(ms->servers[r], p.local_ids[r], nullptr, nullptr, &ids[r],
-                                                             &lats[r]);
-                             });
-            for (double l : lats)
+            if (p.local_ids.size() == 1)
             {
-                worst = std::max(worst, l);
+                // fitted on replica 0; the copies to the others count in the latency
+                check_rc(gprat_cu_server_wait(ms->servers[0], p.local_ids[0], nullptr, nullptr, &ids[0], &worst));
+                const auto t0 = std::chrono::steady_clock::now();
+                copy_to_replicas(ms, ids[0], p.x.data(), static_cast<int64_t>(p.x.size()), p.y.data(),
+                                 static_cast<int64_t>(p.y.size()), p.n_tiles, p.T, p.d, ids);
+                worst += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            }
+            else
+            {
+                std::vector<double> lats(ms->servers.size(), 0.0);
+                on_every_replica(ms,
+                                 [&](int r)
+                                 {
+                                     return gprat_cu_server_wait(ms->servers[r], p.local_ids[r], nullptr, nullptr,
+                                                                 &ids[r], &lats[r]);
+                                 });
+                for (double l : lats)
+                {
+                    worst = std::max(worst, l);
+                }
             }
             std::lock_guard<std::mutex> lk(ms->mtx);
             ms->model_ids.push_back(ids);
@@ -393,6 +498,19 @@ int gprat_cu_multiserver_stats(gprat_cu_multiserver *ms, double *p50_ms, double 
             {
                 *batches = nb;
             }
+        });
+}
+
+int gprat_cu_multiserver_set_replication(gprat_cu_multiserver *ms, int mode)
+{
+    return guarded_ms(
+        [&]
+        {
+            require_ms(ms != nullptr, "multi-server must not be NULL");
+            require_ms(mode == GPRAT_CU_REPLICATE_COPY || mode == GPRAT_CU_REPLICATE_REFIT,
+                       "replication mode must be GPRAT_CU_REPLICATE_COPY or GPRAT_CU_REPLICATE_REFIT");
+            std::lock_guard<std::mutex> lk(ms->mtx);
+            ms->replication = mode;
         });
 }
 

@@ -165,9 +165,10 @@ void fail_request(Request *r, int code, const std::string &msg)
     r->t_done = Clock::now();
 }
 
-// Creates and fits one model (synchronous on the calling thread).
+// Creates and fits one model (synchronous on the calling thread); with
+// `from` set, the fitted state is copied from that model instead of fitted.
 std::unique_ptr<Model> make_model(gprat_cu_server *sv, const double *x, int64_t nx, const double *y, int64_t ny,
-                                  int n_tiles, int T, int d, const double hyper[3])
+                                  int n_tiles, int T, int d, const double hyper[3], gprat_cu_gp *from = nullptr)
 {
     auto m = std::make_unique<Model>();
     gprat_cu_gp *gp = nullptr;
@@ -186,7 +187,14 @@ std::unique_ptr<Model> make_model(gprat_cu_server *sv, const double *x, int64_t 
             throw Error(rc, gprat_cu_last_error());
         }
     }
-    gp_fit(gp, hyper, gp->stream);
+    if (from != nullptr)
+    {
+        gp_copy_fitted(gp, from);
+    }
+    else
+    {
+        gp_fit(gp, hyper, gp->stream);
+    }
     gp_check(gp, gp->stream);
     // reserve a full batch: device working set, staging and pinned buffers
     gp_reserve_predict(gp, RESERVED_ROWS);
@@ -619,6 +627,44 @@ int gprat_cu_server_add_model(gprat_cu_server *sv, const double *train_in, int64
             *model_id = static_cast<int>(sv->models.size()) - 1;
         });
 }
+
+}  // extern "C"
+
+namespace gprat_cu
+{
+// Adds to dst a copy of src's fitted model src_model (the replica layer,
+// multiserve.cu): dst's handle is created from the same training data and
+// tiling, then takes src's device state instead of fitting.  src_model must
+// have no batch in flight.
+int server_add_model_copy(gprat_cu_server *dst, gprat_cu_server *src, int src_model, const double *train_in,
+                          int64_t n_in, const double *train_out, int64_t n_out, int n_tiles, int n_tile_size,
+                          int n_regressors, int *model_id)
+{
+    return guarded_sv(
+        [&]
+        {
+            need(dst != nullptr && src != nullptr && model_id != nullptr, "arguments must not be NULL");
+            need(dst->precision == src->precision, "replicas of different precision");
+            gprat_cu_gp *from = nullptr;
+            {
+                std::lock_guard<std::mutex> lk(src->mtx);
+                need(src_model >= 0 && src_model < static_cast<int>(src->models.size()), "unknown model id");
+                need(!src->models[src_model]->busy, "model has a batch in flight");
+                from = src->models[src_model]->gp;
+            }
+            GPRAT_CUDA_CHECK(cudaSetDevice(dst->device));
+            const double no_hyper[3] = { 0.0, 0.0, 0.0 };
+            auto m = make_model(dst, train_in, n_in, train_out, n_out, n_tiles, n_tile_size, n_regressors, no_hyper,
+                                from);
+            std::lock_guard<std::mutex> lk(dst->mtx);
+            dst->used += m->resident;
+            dst->models.push_back(std::move(m));
+            *model_id = static_cast<int>(dst->models.size()) - 1;
+        });
+}
+}  // namespace gprat_cu
+
+extern "C" {
 
 int gprat_cu_server_submit_predict(gprat_cu_server *sv, int model_id, const double *test_in, int64_t n_test_in, int m,
                                    int64_t *request_id)

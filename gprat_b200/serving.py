@@ -134,19 +134,22 @@ class MultiServer(Server):
     ``devices``; a device may repeat).  Every model is fitted on each replica
     and keeps one model id; a predict request goes to the replica with the
     fewest test points outstanding and its result is bit-identical to the same
-    request on a single :class:`Server`.  memory_budget_bytes and precision
-    apply to each replica."""
+    request on a single :class:`Server`.  replication: ``capi.REPLICATE_COPY``
+    fits a model on the first replica and copies its fitted state to the
+    others (peer copies); ``capi.REPLICATE_REFIT`` fits it on every replica at
+    once.  memory_budget_bytes and precision apply to each replica."""
 
     _PREFIX = "gprat_cu_multiserver_"
 
     def __init__(self, devices: Sequence[int] = (0,), memory_budget_bytes: int = 0,
-                 precision: int = capi.PREC_FP64):
+                 precision: int = capi.PREC_FP64, replication: int = capi.REPLICATE_COPY):
         devs = (ctypes.c_int * len(devices))(*[int(d) for d in devices])
         h = ctypes.c_void_p()
         capi.check(capi.lib.gprat_cu_multiserver_create(devs, len(devices), int(memory_budget_bytes),
                                                         int(precision), ctypes.byref(h)))
         self.n_replicas = len(devices)
         self._init_handle(h)
+        capi.check(capi.lib.gprat_cu_multiserver_set_replication(self._h, int(replication)))
 
     def replica_completed(self) -> list:
         """Predict requests waited on, per replica that served them."""

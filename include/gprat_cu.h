@@ -351,8 +351,12 @@ int gprat_cu_server_stats(gprat_cu_server *server,
  * server per entry of devices (a device may repeat), every model replicated
  * on each.  Test points are independent given a model's factor and alpha, so
  * predict throughput scales with the replicas and no data crosses between
- * GPUs.  add_model and submit_fit run on every replica (the pipeline is
- * deterministic, so the copies are identical) and yield one model id;
+ * GPUs.  add_model and submit_fit yield one model id for all replicas:
+ * by default (GPRAT_CU_REPLICATE_COPY) the model is fitted on the first
+ * replica and its fitted state (factor, alpha, training data) copied to the
+ * others over NVLink, the copy counted in the fit's latency; with
+ * GPRAT_CU_REPLICATE_REFIT (set_replication) every replica fits it at once
+ * (the pipeline is deterministic, so the copies are identical either way);
  * submit_predict goes to the replica with the fewest test points submitted
  * and not yet waited on.  A predict result is bit-identical to the same
  * request on a single server.  wait/stats as for a server: latencies are the
@@ -408,6 +412,9 @@ int gprat_cu_multiserver_stats(gprat_cu_multiserver *server,
                                int64_t *completed,
                                int64_t *batches);
 int gprat_cu_multiserver_replica_completed(gprat_cu_multiserver *server, int replica, int64_t *completed);
+#define GPRAT_CU_REPLICATE_COPY 0
+#define GPRAT_CU_REPLICATE_REFIT 1
+int gprat_cu_multiserver_set_replication(gprat_cu_multiserver *server, int mode);
 
 #ifdef __cplusplus
 }

@@ -1,6 +1,6 @@
 """Replica serving (gprat_cu_multiserver_*): every model replicated on each
-replica, predict requests spread over the replicas by outstanding test
-points, fits run on every replica.
+replica (fitted once and copied, or fitted on every replica), predict
+requests spread over the replicas by outstanding test points.
 
 The property under test: a result is bit-identical to the same request on a
 single server, whichever replica served it, and the replicas share the load.
@@ -47,15 +47,15 @@ def _add(sv, models):
     return [sv.add_model(md["x"], md["y"], md["n"] // md["T"], md["T"], md["d"], md["h"]) for md in models]
 
 
-@pytest.mark.parametrize("prec", [0, 1])
-def test_replicas_bit_identical_to_single_server(serving, prec):
+@pytest.mark.parametrize("prec,replication", [(0, 0), (1, 0), (1, 1)])
+def test_replicas_bit_identical_to_single_server(serving, prec, replication):
     capi, S = serving
     models = _models()
     reqs = _requests(len(models), 8, 30)
     with S.Server(memory_budget_bytes=BUDGET, precision=prec) as sv:
         ids = _add(sv, models)
         single = [sv.wait(sv.submit_predict(ids[mid], series, m)) for mid, m, series in reqs]
-    with S.MultiServer([0, 0], memory_budget_bytes=BUDGET, precision=prec) as ms:
+    with S.MultiServer([0, 0], memory_budget_bytes=BUDGET, precision=prec, replication=replication) as ms:
         gids = _add(ms, models)
         assert gids == [0, 1]
         rids = [ms.submit_predict(gids[mid], series, m) for mid, m, series in reqs]
@@ -71,15 +71,16 @@ def test_replicas_bit_identical_to_single_server(serving, prec):
     assert st.completed == len(reqs) and 0.0 < st.p50_ms <= st.p99_ms
 
 
-def test_fit_replicated_on_every_replica(serving):
+@pytest.mark.parametrize("prec,replication", [(0, 0), (0, 1), (2, 0)])
+def test_fit_replicated_on_every_replica(serving, prec, replication):
     capi, S = serving
     fx, fy, _ = O.synthetic(1024, 16, 8, seeds=(71, 72, 73))
     hyper = (1.1, 1.0, 0.1)
     series = np.random.default_rng(4).uniform(-1, 1, 200 + 7)
-    with S.Server(memory_budget_bytes=BUDGET) as sv:
+    with S.Server(memory_budget_bytes=BUDGET, precision=prec) as sv:
         _, _, mid, _ = sv.wait(sv.submit_fit(fx, fy, 8, 128, 8, hyper))
         ref_mean, ref_var, _, _ = sv.wait(sv.submit_predict(mid, series, 200))
-    with S.MultiServer([0, 0], memory_budget_bytes=BUDGET) as ms:
+    with S.MultiServer([0, 0], memory_budget_bytes=BUDGET, precision=prec, replication=replication) as ms:
         _, _, gid, _ = ms.wait(ms.submit_fit(fx, fy, 8, 128, 8, hyper))
         # enough requests that both replicas serve the fitted model
         rids = [ms.submit_predict(gid, series, 200) for _ in range(6)]
@@ -90,8 +91,9 @@ def test_fit_replicated_on_every_replica(serving):
         assert np.array_equal(mean, ref_mean) and np.array_equal(var, ref_var)
     o = O.OracleGP(fx, fy, 8, 128, 8, hyper)
     om, ov = o.predict_with_uncertainty(series, 1, 200)
-    assert np.max(np.abs(ref_mean - om)) <= 1e-10 * max(1.0, np.max(np.abs(om)))
-    assert np.max(np.abs(ref_var - ov) / ov) <= 1e-10
+    tol_m, tol_v = {0: (1e-10, 1e-10), 1: (1e-8, 1.5e-2), 2: (1e-8, 5e-2)}[prec]
+    assert np.max(np.abs(ref_mean - om)) <= tol_m * max(1.0, np.max(np.abs(om)))
+    assert np.max(np.abs(ref_var - ov) / ov) <= tol_v
 
 
 def test_multiserver_invalid_requests(serving):
@@ -100,6 +102,8 @@ def test_multiserver_invalid_requests(serving):
         S.MultiServer([])
     with pytest.raises(capi.GpratCudaError):
         S.MultiServer([0, 10_000])  # no such device; the first replica is released
+    with pytest.raises(capi.GpratCudaError):
+        S.MultiServer([0], replication=7)
     with S.MultiServer([0, 0], memory_budget_bytes=BUDGET) as ms:
         with pytest.raises(capi.GpratCudaError):
             ms.submit_predict(0, np.zeros(10), 3)  # no model yet
