@@ -81,6 +81,7 @@ def _load() -> ctypes.CDLL:
                                           ctypes.c_int]
     _vp, _i64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)
     lib.gprat_cu_steps_enable.argtypes = [ctypes.c_int]
+    lib.gprat_cu_test_trsv.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int]
     lib.gprat_cu_steps_csv.argtypes = [ctypes.c_char_p, _i64, _i64p]
     lib.gprat_cu_server_create.argtypes = [ctypes.c_int, _i64, ctypes.c_int, ctypes.POINTER(_vp)]
     lib.gprat_cu_server_destroy.argtypes = [_vp]
@@ -185,6 +186,18 @@ def test_tc_gemm(kind: int, A: np.ndarray, B: np.ndarray, C: np.ndarray, alpha: 
     check(lib.gprat_cu_test_tc_gemm(int(kind), M, N, K, A.ctypes.data_as(_fp), K, B.ctypes.data_as(_fp), K,
                                     C.ctypes.data_as(_fp), C.shape[1], float(alpha), float(beta), int(bool(lower)),
                                     rp, int(tile_mode)))
+
+
+def test_trsv(kind: int, L: np.ndarray, b: np.ndarray, max_ctas: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+    """Runs the fused triangular solves on the lower triangle of L (n x n):
+    returns (L^-1 b, L^-T b).  kind 0 = FP64 factor, 1 = FP32 factor and
+    inverses (the mixed path's preconditioner)."""
+    L = np.ascontiguousarray(L, dtype=np.float64)
+    b = _arr(b)
+    n = L.shape[0]
+    xf, xb = np.empty(n), np.empty(n)
+    check(lib.gprat_cu_test_trsv(int(kind), n, _p(L), _p(b), _p(xf), _p(xb), int(max_ctas)))
+    return xf, xb
 
 
 def _arr(a) -> np.ndarray:

@@ -1,8 +1,10 @@
 // Kernel-level test entry points of the C ABI (gprat_cu_test_*): run one
 // kernel on host-provided data so that tests can compare it in isolation.
+#include "common.cuh"
 #include "gprat_cu.h"
 #include "tc_gemm.cuh"
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -107,6 +109,131 @@ extern "C" int gprat_cu_test_tc_gemm(int kind, int M, int N, int K, const float 
             {
                 rowsq[i] = halves[i] + halves[M + i];
             }
+        }
+        set_last_error("");
+        return GPRAT_CU_OK;
+    }
+    catch (const Error &e)
+    {
+        set_last_error(e.what());
+        return e.code;
+    }
+    catch (const std::exception &e)
+    {
+        set_last_error(e.what());
+        return GPRAT_CU_ERR_INVALID_ARG;
+    }
+}
+
+extern "C" int gprat_cu_test_trsv(int kind, int n, const double *L, const double *b, double *x_fwd, double *x_bwd,
+                                  int max_ctas)
+{
+    try
+    {
+        if (L == nullptr || b == nullptr || x_fwd == nullptr || x_bwd == nullptr || n <= 0 || (kind != 0 && kind != 1) ||
+            max_ctas < 0)
+        {
+            throw Error(GPRAT_CU_ERR_INVALID_ARG, "gprat_cu_test_trsv: invalid arguments");
+        }
+        constexpr int B = 128;
+        const int nblk = (n + B - 1) / B;
+        const int64_t ld = round_up(n, 64);
+        // inverses of the diagonal blocks (host, forward substitution per column)
+        std::vector<double> inv(static_cast<size_t>(nblk) * B * B, 0.0);
+        for (int k = 0; k < nblk; ++k)
+        {
+            const int r0 = k * B, bs = std::min(B, n - r0);
+            double *X = inv.data() + static_cast<size_t>(k) * B * B;
+            for (int c = 0; c < bs; ++c)
+            {
+                for (int r = c; r < bs; ++r)
+                {
+                    double s = (r == c) ? 1.0 : 0.0;
+                    for (int t = c; t < r; ++t)
+                    {
+                        s -= L[static_cast<int64_t>(r0 + r) * n + r0 + t] * X[t * B + c];
+                    }
+                    X[r * B + c] = s / L[static_cast<int64_t>(r0 + r) * n + r0 + r];
+                }
+            }
+        }
+        const size_t es = kind == 0 ? sizeof(double) : sizeof(float);
+        std::vector<char> hL(static_cast<size_t>(n) * ld * es, 0), hI(inv.size() * es, 0);
+        for (int r = 0; r < n; ++r)
+        {
+            for (int c = 0; c <= r; ++c)
+            {
+                const double v = L[static_cast<int64_t>(r) * n + c];
+                if (kind == 0)
+                {
+                    reinterpret_cast<double *>(hL.data())[static_cast<int64_t>(r) * ld + c] = v;
+                }
+                else
+                {
+                    reinterpret_cast<float *>(hL.data())[static_cast<int64_t>(r) * ld + c] = static_cast<float>(v);
+                }
+            }
+        }
+        for (size_t q = 0; q < inv.size(); ++q)
+        {
+            if (kind == 0)
+            {
+                reinterpret_cast<double *>(hI.data())[q] = inv[q];
+            }
+            else
+            {
+                reinterpret_cast<float *>(hI.data())[q] = static_cast<float>(inv[q]);
+            }
+        }
+        Buf dL(hL.size()), dI(hI.size()), dx(n * sizeof(double)), dscr(n * sizeof(double)), dflags(16),
+            dStatus(sizeof(DeviceStatus));
+        GPRAT_CUDA_CHECK(cudaMemcpy(dL.p, hL.data(), hL.size(), cudaMemcpyHostToDevice));
+        GPRAT_CUDA_CHECK(cudaMemcpy(dI.p, hI.data(), hI.size(), cudaMemcpyHostToDevice));
+        GPRAT_CUDA_CHECK(cudaMemset(dStatus.p, 0, sizeof(DeviceStatus)));
+        cudaStream_t s = nullptr;
+        auto *st = static_cast<DeviceStatus *>(dStatus.p);
+        auto *x = static_cast<double *>(dx.p);
+        for (int dir = 0; dir < 2; ++dir)
+        {
+            GPRAT_CUDA_CHECK(cudaMemcpy(x, b, n * sizeof(double), cudaMemcpyHostToDevice));
+            if (kind == 0)
+            {
+                const auto *l = static_cast<const double *>(dL.p);
+                const auto *li = static_cast<const double *>(dI.p);
+                if (dir == 0)
+                {
+                    trsv_fused_forward(l, ld, li, n, x, static_cast<int *>(dflags.p), static_cast<double *>(dscr.p),
+                                       st, s, max_ctas);
+                }
+                else
+                {
+                    trsv_fused_backward(l, ld, li, n, x, static_cast<int *>(dflags.p), static_cast<double *>(dscr.p),
+                                        st, s, max_ctas);
+                }
+            }
+            else
+            {
+                const auto *l = static_cast<const float *>(dL.p);
+                const auto *li = static_cast<const float *>(dI.p);
+                if (dir == 0)
+                {
+                    trsv_fused_forward_f32(l, ld, li, n, x, static_cast<int *>(dflags.p),
+                                           static_cast<double *>(dscr.p), st, s, max_ctas);
+                }
+                else
+                {
+                    trsv_fused_backward_f32(l, ld, li, n, x, static_cast<int *>(dflags.p),
+                                            static_cast<double *>(dscr.p), st, s, max_ctas);
+                }
+            }
+            GPRAT_CUDA_CHECK(cudaStreamSynchronize(s));
+            GPRAT_CUDA_CHECK(cudaMemcpy(dir == 0 ? x_fwd : x_bwd, x, n * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+        DeviceStatus hst{};
+        GPRAT_CUDA_CHECK(cudaMemcpy(&hst, dStatus.p, sizeof(hst), cudaMemcpyDeviceToHost));
+        if (hst.timeout != 0)
+        {
+            throw Error(GPRAT_CU_ERR_TIMEOUT, "triangular solve: a bounded wait timed out");
         }
         set_last_error("");
         return GPRAT_CU_OK;

@@ -405,6 +405,425 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_fused_kernel(const T *__restri
     }
 }
 
+// FP32 factor and FP32 inverses (the preconditioner of the mixed path): the
+// two products that follow the arrival of the neighbouring block -- with the
+// last off-diagonal block and with the diagonal inverse -- are the chain from
+// one row block to the next, and they run from registers:
+//   * when a CTA takes its block, each thread loads its half row (forward)
+//     or half column (backward) of the diagonal inverse into registers and
+//     starts a cp.async copy of the last off-diagonal tile into shared memory
+//     (laid out so that the later reads are free of bank conflicts); both
+//     land while the blocks before are accumulated;
+//   * those blocks are multiplied in FP32 (four products per row and lane)
+//     and summed in FP64, and the lane partials are reduced into the
+//     right-hand side (a reduce-scatter butterfly, 16 shuffles for 16 rows)
+//     before the last block arrives;
+//   * each thread then moves its part of the off-diagonal tile into
+//     registers and waits;
+//   * after the arrival, the block of x is staged in shared memory; 64 FP32
+//     FMAs and one shuffle give each row's (column's) update, and the same
+//     with the inverse gives x_i.
+// Products round to FP32 (the preconditioner's accuracy is that of the FP32
+// factor); sums over blocks stay in FP64.
+constexpr int TSTR = 144;  // row stride (floats) of the backward tiles: conflict-free column reads
+constexpr size_t SMEM_F32_FWD = 16 * FT * sizeof(float4) + FB * sizeof(double) + 2 * FB * sizeof(float) + 16;
+constexpr size_t SMEM_F32_BWD =
+    FB * TSTR * sizeof(float) + (FB + (FT / 32) * FB) * sizeof(double) + 2 * FB * sizeof(float) + 16;
+
+// 64-term FP32 dot product of registers with shared memory (16-byte reads).
+__device__ __forceinline__ float dot64(const float (&a)[64], const float *v)
+{
+    const float4 *v4 = reinterpret_cast<const float4 *>(v);
+    float acc[4] = { 0.f, 0.f, 0.f, 0.f };
+#pragma unroll
+    for (int k4 = 0; k4 < 16; ++k4)
+    {
+        const float4 q = v4[k4];
+        acc[k4 & 3] = fmaf(a[4 * k4], q.x, acc[k4 & 3]);
+        acc[k4 & 3] = fmaf(a[4 * k4 + 1], q.y, acc[k4 & 3]);
+        acc[k4 & 3] = fmaf(a[4 * k4 + 2], q.z, acc[k4 & 3]);
+        acc[k4 & 3] = fmaf(a[4 * k4 + 3], q.w, acc[k4 & 3]);
+    }
+    return (acc[0] + acc[1]) + (acc[2] + acc[3]);
+}
+
+// Sum over the warp of 16 per-lane values: lane l returns the total of value
+// (l >> 1) & 15 (a reduce-scatter over lane bits 4..1, then one exchange).
+__device__ __forceinline__ double reduce_scatter16(double (&v)[16])
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int half = 8, bit = 16; half >= 1; half >>= 1, bit >>= 1)
+    {
+        const bool hi = (lane & bit) != 0;
+#pragma unroll
+        for (int t = 0; t < half; ++t)
+        {
+            const double send = hi ? v[t] : v[t + half];
+            const double keep = hi ? v[t + half] : v[t];
+            v[t] = keep + __shfl_xor_sync(0xffffffffu, send, bit);
+        }
+    }
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+__global__ void __launch_bounds__(FT, 1) trsv_fwd_f32_kernel(const float *__restrict__ L, int64_t ld,
+                                                             const float *__restrict__ Linv, int n,
+                                                             const double *__restrict__ b, double *x, int *flags,
+                                                             DeviceStatus *st)
+{
+    extern __shared__ __align__(16) double sm[];
+    // L_{i,i-1} in thread-major order: tileL[k4][t] = the four floats
+    // 64h + 4k4 .. of row t >> 1 (h = t & 1), so thread t reads its half row
+    // conflict-free
+    float4 *tileL = reinterpret_cast<float4 *>(sm);
+    double *rhs = reinterpret_cast<double *>(tileL + 16 * FT);  // b_i - sum_{j < i-1} L_ij x_j
+    float *xs = reinterpret_cast<float *>(rhs + FB);              // x_{i-1}
+    float *rs = xs + FB;                                          // b_i - sum_{j < i} L_ij x_j
+    int *shared_int = reinterpret_cast<int *>(rs + FB);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int rr = tid >> 1, h = tid & 1;  // the row and column half of this thread in the two products
+    const int nblk = (n + FB - 1) / FB;
+    for (;;)
+    {
+    if (tid == 0)
+    {
+        shared_int[0] = atomicAdd(flags, 1);
+    }
+    __syncthreads();
+    const int i = shared_int[0];
+    __syncthreads();  // every thread has its ticket before thread 0 draws the next
+    if (i >= nblk)
+    {
+        break;
+    }
+    const int r0 = i * FB;
+    const int bs = min(FB, n - r0);
+    // start the copy of L_{i,i-1}: copy m moves chunk k4 = m of thread slot
+    // t = tid (consecutive threads fill consecutive 16-byte slots)
+    if (i > 0)
+    {
+#pragma unroll 4
+        for (int m = 0; m < 16; ++m)
+        {
+            const int c = 64 * h + 4 * m;
+            cp_async16(tileL + m * FT + tid, L + static_cast<int64_t>(r0 + min(rr, bs - 1)) * ld + (i - 1) * FB + c);
+        }
+    }
+    // this thread's half row of Linv_ii (zero above the diagonal; defined on
+    // rows and columns < bs only)
+    float ireg[64];
+    {
+        const float4 *ip = reinterpret_cast<const float4 *>(Linv + static_cast<int64_t>(i) * FB * FB + rr * FB + 64 * h);
+#pragma unroll
+        for (int k4 = 0; k4 < 16; ++k4)
+        {
+            const float4 q = ip[k4];
+            ireg[4 * k4] = q.x;
+            ireg[4 * k4 + 1] = q.y;
+            ireg[4 * k4 + 2] = q.z;
+            ireg[4 * k4 + 3] = q.w;
+        }
+    }
+    if (tid < FB)
+    {
+        rhs[tid] = (tid < bs) ? b[r0 + tid] : 0.0;
+    }
+    __syncthreads();  // rhs rows are updated below by other threads
+
+    // blocks j < i - 1: rows warp + 8q, lanes own columns lane + 32c, FP64 sums
+    double part[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+    {
+        part[q] = 0.0;
+    }
+    for (int j = 0; j < i - 1; ++j)
+    {
+        const int c0 = j * FB;
+        float v[16][4];
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+        {
+            const int r = warp + 8 * q;
+            const float *lr = L + static_cast<int64_t>(r0 + min(r, bs - 1)) * ld + c0 + lane;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                v[q][c] = lr[32 * c];
+            }
+        }
+        double xv[4];
+        {
+            const double *xp[4] = { x + c0 + lane, x + c0 + lane + 32, x + c0 + lane + 64, x + c0 + lane + 96 };
+            await_x<4>(xp, xv, j == i - 2, st);
+        }
+        float xf[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+        {
+            xf[c] = static_cast<float>(xv[c]);
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+        {
+            float s2 = v[q][0] * xf[0];
+#pragma unroll
+            for (int c = 1; c < 4; ++c)
+            {
+                s2 = fmaf(v[q][c], xf[c], s2);
+            }
+            part[q] += static_cast<double>(s2);
+        }
+    }
+    if (i > 1)
+    {
+        const double s2 = reduce_scatter16(part);
+        if ((lane & 1) == 0)
+        {
+            rhs[warp + 8 * ((lane >> 1) & 15)] -= s2;
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();  // tile landed, rhs complete
+    float lreg[64];
+    if (bs < FB)
+    {
+        // a ragged last block: the inverse is defined on rows and columns < bs only
+#pragma unroll
+        for (int k = 0; k < 64; ++k)
+        {
+            ireg[k] = (rr < bs && 64 * h + k < bs) ? ireg[k] : 0.f;
+        }
+    }
+    if (i > 0)
+    {
+#pragma unroll
+        for (int k4 = 0; k4 < 16; ++k4)
+        {
+            const float4 q = tileL[k4 * FT + tid];
+            lreg[4 * k4] = q.x;
+            lreg[4 * k4 + 1] = q.y;
+            lreg[4 * k4 + 2] = q.z;
+            lreg[4 * k4 + 3] = q.w;
+        }
+        if (warp == 0)
+        {
+            const int c0 = (i - 1) * FB;
+            double xv[4];
+            const double *xp[4] = { x + c0 + lane, x + c0 + lane + 32, x + c0 + lane + 64, x + c0 + lane + 96 };
+            await_x<4>(xp, xv, true, st);
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                xs[lane + 32 * c] = static_cast<float>(xv[c]);
+            }
+        }
+        __syncthreads();  // x_{i-1} staged
+        float s1 = dot64(lreg, xs + 64 * h);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+        if (h == 0)
+        {
+            rs[rr] = static_cast<float>(rhs[rr] - static_cast<double>(s1));
+        }
+    }
+    else if (h == 0)
+    {
+        rs[rr] = static_cast<float>(rhs[rr]);
+    }
+    __syncthreads();
+    float s1 = dot64(ireg, rs + 64 * h);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+    if (h == 0 && rr < bs)
+    {
+        x[r0 + rr] = static_cast<double>(s1);
+    }
+    __syncthreads();  // shared memory is refilled for the next block
+    }
+}
+
+__global__ void __launch_bounds__(FT, 1) trsv_bwd_f32_kernel(const float *__restrict__ L, int64_t ld,
+                                                             const float *__restrict__ Linv, int n, int nblk,
+                                                             const double *__restrict__ b, double *x, int *flags,
+                                                             DeviceStatus *st)
+{
+    extern __shared__ __align__(16) double sm[];
+    // L_{i+1,i} (rows of block i+1) row-major with stride TSTR; thread (cc, h)
+    // reads column cc, rows 2k + h
+    float *tileL = reinterpret_cast<float *>(sm);
+    double *rhs = reinterpret_cast<double *>(tileL + FB * TSTR);  // b_i - sum_{j > i+1} L_ji^T x_j
+    double *colpart = rhs + FB;                                     // [8][FB]
+    // x_{i+1} and the final right-hand side, split by row parity: v[p] at
+    // 64 (p & 1) + (p >> 1)
+    float *xs = reinterpret_cast<float *>(colpart + (FT / 32) * FB);
+    float *rs = xs + FB;
+    int *shared_int = reinterpret_cast<int *>(rs + FB);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int cc = tid >> 1, h = tid & 1;  // the column and row parity of this thread in the two products
+    for (;;)
+    {
+    if (tid == 0)
+    {
+        shared_int[0] = nblk - 1 - atomicAdd(flags, 1);
+    }
+    __syncthreads();
+    const int i = shared_int[0];
+    __syncthreads();  // every thread has its ticket before thread 0 draws the next
+    if (i < 0)
+    {
+        break;
+    }
+    const int c0 = i * FB;
+    const int bs = min(FB, n - c0);
+    const bool has_next = i + 1 < nblk;
+    const int rs1 = has_next ? min(FB, n - (i + 1) * FB) : 0;  // rows of block i + 1
+    // start the copy of L_{i+1,i} (16-byte chunks, row by row)
+    if (has_next)
+    {
+#pragma unroll 4
+        for (int m = 0; m < 16; ++m)
+        {
+            const int g = tid + FT * m, row = g >> 5, ch = g & 31;
+            cp_async16(tileL + row * TSTR + 4 * ch,
+                       L + static_cast<int64_t>((i + 1) * FB + min(row, rs1 - 1)) * ld + c0 + 4 * ch);
+        }
+    }
+    // this thread's rows 2k + h of column cc of Linv_ii (zero above the
+    // diagonal; defined on rows and columns < bs only)
+    float ireg[64];
+    {
+        const float *ip = Linv + static_cast<int64_t>(i) * FB * FB + cc;
+#pragma unroll
+        for (int k = 0; k < 64; ++k)
+        {
+            ireg[k] = ip[(2 * k + h) * FB];
+        }
+    }
+    if (tid < FB)
+    {
+        rhs[tid] = (tid < bs) ? b[c0 + tid] : 0.0;
+    }
+    // blocks j > i + 1: lanes own columns lane + 32c of block i, warps rows warp + 8q of block j
+    double part[4] = { 0.0, 0.0, 0.0, 0.0 };
+    for (int j = nblk - 1; j > i + 1; --j)
+    {
+        const int r0 = j * FB;
+        const int rsj = min(FB, n - r0);
+        float v[16][4];
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+        {
+            const int r = warp + 8 * q;
+            const float *lr = L + static_cast<int64_t>(r0 + min(r, rsj - 1)) * ld + c0 + lane;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                v[q][c] = (lane + 32 * c < bs) ? lr[32 * c] : 0.f;
+            }
+        }
+        double xv[16];
+        {
+            const double *xp[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+            {
+                xp[q] = x + r0 + min(warp + 8 * q, rsj - 1);
+            }
+            await_x<16>(xp, xv, j == i + 2, st);
+        }
+        float s2[4] = { 0.f, 0.f, 0.f, 0.f };
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+        {
+            const int r = warp + 8 * q;
+            const float xr = (r < rsj) ? static_cast<float>(xv[q]) : 0.f;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                s2[c] = fmaf(v[q][c], xr, s2[c]);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+        {
+            part[c] += static_cast<double>(s2[c]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+    {
+        colpart[warp * FB + lane + 32 * c] = part[c];
+    }
+    cp_async_wait_all();
+    __syncthreads();  // tile landed, column partials written
+    if (tid < FB)
+    {
+        double s2 = 0.0;
+#pragma unroll
+        for (int w = 0; w < FT / 32; ++w)
+        {
+            s2 += colpart[w * FB + tid];
+        }
+        rhs[tid] -= s2;
+    }
+    float lreg[64];
+    if (bs < FB)
+    {
+        // a ragged last block: the inverse is defined on rows and columns < bs only
+#pragma unroll
+        for (int k = 0; k < 64; ++k)
+        {
+            ireg[k] = (cc < bs && 2 * k + h < bs) ? ireg[k] : 0.f;
+        }
+    }
+    if (has_next)
+    {
+#pragma unroll
+        for (int k = 0; k < 64; ++k)
+        {
+            lreg[k] = tileL[(2 * k + h) * TSTR + cc];
+        }
+        if (warp == 0)
+        {
+            const int r0 = (i + 1) * FB;
+            double xv[4];
+            const double *xp[4] = { x + r0 + min(lane, rs1 - 1), x + r0 + min(lane + 32, rs1 - 1),
+                                    x + r0 + min(lane + 64, rs1 - 1), x + r0 + min(lane + 96, rs1 - 1) };
+            await_x<4>(xp, xv, true, st);
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                const int p = lane + 32 * c;
+                xs[64 * (p & 1) + (p >> 1)] = (p < rs1) ? static_cast<float>(xv[c]) : 0.f;
+            }
+        }
+        __syncthreads();  // x_{i+1} staged, rhs complete
+        float s1 = dot64(lreg, xs + 64 * h);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+        if (h == 0)
+        {
+            rs[64 * (cc & 1) + (cc >> 1)] = static_cast<float>(rhs[cc] - static_cast<double>(s1));
+        }
+    }
+    else
+    {
+        __syncthreads();  // rhs complete
+        if (h == 0)
+        {
+            rs[64 * (cc & 1) + (cc >> 1)] = static_cast<float>(rhs[cc]);
+        }
+    }
+    __syncthreads();
+    float s1 = dot64(ireg, rs + 64 * h);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+    if (h == 0 && cc < bs)
+    {
+        x[c0 + cc] = static_cast<double>(s1);
+    }
+    __syncthreads();  // shared memory is refilled for the next block
+    }
+}
+
 // x: in = b, out = solution.  scratch: n doubles (receives b).
 void prepare(double *x, double *scratch, int n, int *flags, cudaStream_t s)
 {
@@ -458,13 +877,30 @@ void trsv_fused_backward(const double *L, int64_t ld, const double *Linv, int n,
 void trsv_fused_forward_f32(const float *L, int64_t ld, const float *Linv, int n, double *x, int *flags,
                             double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas)
 {
-    fwd(L, ld, Linv, n, x, flags, scratch, st, s, max_ctas);
+    if ((ld & 3) != 0 || (reinterpret_cast<uintptr_t>(L) & 15) != 0 || (reinterpret_cast<uintptr_t>(Linv) & 15) != 0)
+    {
+        throw Error(1, "trsv_fused_forward_f32: L and Linv must be 16-byte aligned, ld a multiple of 4");
+    }
+    const int nblk = ceil_div(n, FB);
+    ensure_smem_attr(reinterpret_cast<const void *>(trsv_fwd_f32_kernel), static_cast<int>(SMEM_F32_FWD));
+    prepare(x, scratch, n, flags, s);
+    trsv_fwd_f32_kernel<<<grid_for(nblk, max_ctas), FT, SMEM_F32_FWD, s>>>(L, ld, Linv, n, scratch, x, flags, st);
+    GPRAT_LAUNCH_CHECK();
 }
 
 void trsv_fused_backward_f32(const float *L, int64_t ld, const float *Linv, int n, double *x, int *flags,
                              double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas)
 {
-    bwd(L, ld, Linv, n, x, flags, scratch, st, s, max_ctas);
+    if ((ld & 3) != 0 || (reinterpret_cast<uintptr_t>(L) & 15) != 0 || (reinterpret_cast<uintptr_t>(Linv) & 15) != 0)
+    {
+        throw Error(1, "trsv_fused_backward_f32: L and Linv must be 16-byte aligned, ld a multiple of 4");
+    }
+    const int nblk = ceil_div(n, FB);
+    ensure_smem_attr(reinterpret_cast<const void *>(trsv_bwd_f32_kernel), static_cast<int>(SMEM_F32_BWD));
+    prepare(x, scratch, n, flags, s);
+    trsv_bwd_f32_kernel<<<grid_for(nblk, max_ctas), FT, SMEM_F32_BWD, s>>>(L, ld, Linv, n, nblk, scratch, x, flags,
+                                                                        st);
+    GPRAT_LAUNCH_CHECK();
 }
 
 }  // namespace gprat_cu

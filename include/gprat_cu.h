@@ -280,6 +280,18 @@ int gprat_cu_test_tc_gemm(int kind,
                           int tile_mode);
 
 /*
+ * Kernel-level test entry (no counterpart in the reference): the
+ * single-launch blocked triangular solves of the library on the current
+ * device.  L: n x n row-major host matrix whose lower triangle (diagonal
+ * included) is the factor.  The inverses of its 128 x 128 diagonal blocks
+ * are formed on the host; kind 0 = FP64 factor and inverses (the FP64
+ * alpha solve), 1 = both rounded to FP32 (the preconditioner of the
+ * mixed-precision refinement).  x_fwd = L^-1 b and x_bwd = L^-T b, each
+ * from b.  max_ctas > 0 bounds the grid.
+ */
+int gprat_cu_test_trsv(int kind, int n, const double *L, const double *b, double *x_fwd, double *x_bwd, int max_ctas);
+
+/*
  * Serving (no counterpart in the reference, whose every predict call
  * re-assembles and re-factorises K, core/src/cpu/gp_functions.cpp:110-189).
  * A server owns fitted models resident on one GPU (factor L and alpha stay
