@@ -405,30 +405,28 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_fused_kernel(const T *__restri
     }
 }
 
-// FP32 factor and FP32 inverses (the preconditioner of the mixed path): the
-// two products that follow the arrival of the neighbouring block -- with the
-// last off-diagonal block and with the diagonal inverse -- are the chain from
-// one row block to the next, and they run from registers:
-//   * when a CTA takes its block, each thread loads its half row (forward)
-//     or half column (backward) of the diagonal inverse into registers and
-//     starts a cp.async copy of the last off-diagonal tile into shared memory
-//     (laid out so that the later reads are free of bank conflicts); both
-//     land while the blocks before are accumulated;
-//   * those blocks are multiplied in FP32 (four products per row and lane)
-//     and summed in FP64, and the lane partials are reduced into the
-//     right-hand side (a reduce-scatter butterfly, 16 shuffles for 16 rows)
-//     before the last block arrives;
-//   * each thread then moves its part of the off-diagonal tile into
-//     registers and waits;
-//   * after the arrival, the block of x is staged in shared memory; 64 FP32
-//     FMAs and one shuffle give each row's (column's) update, and the same
-//     with the inverse gives x_i.
+// FP32 factor and FP32 inverses (the preconditioner of the mixed path).  The
+// chain from one row block to the next runs from registers:
+//   * when a CTA takes block i, each thread loads its half row (forward) or
+//     half column (backward) of the diagonal inverse into registers and
+//     starts cp.async copies of the two nearest off-diagonal tiles (blocks
+//     i-2 and i-1 forward, i+2 and i+1 backward) into shared memory, laid
+//     out so that the later reads are free of bank conflicts;
+//   * the farther blocks are multiplied in FP32 (four products per row and
+//     lane) and summed in FP64; the lane partials are reduced into the
+//     right-hand side (a reduce-scatter butterfly, 16 shuffles for 16 rows);
+//   * each thread moves its part of both near tiles into registers, and one
+//     warp stages the two nearest blocks of x in shared memory as they
+//     arrive; nothing else waits for the block two steps back, so its
+//     arrival costs the chain nothing;
+//   * after the neighbour's arrival, 128 FP32 FMAs and one shuffle give each
+//     row's (column's) update, and 64 more with the inverse give x_i.
 // Products round to FP32 (the preconditioner's accuracy is that of the FP32
-// factor); sums over blocks stay in FP64.
+// factor); sums over the far blocks stay in FP64.
 constexpr int TSTR = 144;  // row stride (floats) of the backward tiles: conflict-free column reads
-constexpr size_t SMEM_F32_FWD = 16 * FT * sizeof(float4) + FB * sizeof(double) + 2 * FB * sizeof(float) + 16;
+constexpr size_t SMEM_F32_FWD = 2 * 16 * FT * sizeof(float4) + FB * sizeof(double) + 3 * FB * sizeof(float) + 16;
 constexpr size_t SMEM_F32_BWD =
-    FB * TSTR * sizeof(float) + (FB + (FT / 32) * FB) * sizeof(double) + 2 * FB * sizeof(float) + 16;
+    2 * FB * TSTR * sizeof(float) + (FB + (FT / 32) * FB) * sizeof(double) + 3 * FB * sizeof(float) + 16;
 
 // 64-term FP32 dot product of registers with shared memory (16-byte reads).
 __device__ __forceinline__ float dot64(const float (&a)[64], const float *v)
@@ -473,16 +471,16 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_f32_kernel(const float *__rest
                                                              DeviceStatus *st)
 {
     extern __shared__ __align__(16) double sm[];
-    // L_{i,i-1} in thread-major order: tileL[k4][t] = the four floats
-    // 64h + 4k4 .. of row t >> 1 (h = t & 1), so thread t reads its half row
-    // conflict-free
-    float4 *tileL = reinterpret_cast<float4 *>(sm);
-    double *rhs = reinterpret_cast<double *>(tileL + 16 * FT);  // b_i - sum_{j < i-1} L_ij x_j
-    float *xs = reinterpret_cast<float *>(rhs + FB);              // x_{i-1}
-    float *rs = xs + FB;                                          // b_i - sum_{j < i} L_ij x_j
+    // L_{i,i-2} (tile 0) and L_{i,i-1} (tile 1) in thread-major order:
+    // tile[k4][t] = the four floats 64h + 4k4 .. of row t >> 1 (h = t & 1), so
+    // thread t reads its half row conflict-free
+    float4 *tiles = reinterpret_cast<float4 *>(sm);
+    double *rhs = reinterpret_cast<double *>(tiles + 2 * 16 * FT);  // b_i - sum_{j < i-2} L_ij x_j
+    float *xs = reinterpret_cast<float *>(rhs + FB);                 // x_{i-2}, x_{i-1}
+    float *rs = xs + 2 * FB;                                         // b_i - sum_{j < i} L_ij x_j
     int *shared_int = reinterpret_cast<int *>(rs + FB);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int rr = tid >> 1, h = tid & 1;  // the row and column half of this thread in the two products
+    const int rr = tid >> 1, h = tid & 1;  // the row and column half of this thread in the products
     const int nblk = (n + FB - 1) / FB;
     for (;;)
     {
@@ -499,15 +497,20 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_f32_kernel(const float *__rest
     }
     const int r0 = i * FB;
     const int bs = min(FB, n - r0);
-    // start the copy of L_{i,i-1}: copy m moves chunk k4 = m of thread slot
-    // t = tid (consecutive threads fill consecutive 16-byte slots)
-    if (i > 0)
+    // start the copies of the near tiles: copy m moves chunk k4 = m of thread
+    // slot t = tid (consecutive threads fill consecutive 16-byte slots)
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
     {
-#pragma unroll 4
-        for (int m = 0; m < 16; ++m)
+        const int j = i - 2 + t;
+        if (j >= 0)
         {
-            const int c = 64 * h + 4 * m;
-            cp_async16(tileL + m * FT + tid, L + static_cast<int64_t>(r0 + min(rr, bs - 1)) * ld + (i - 1) * FB + c);
+            const float *src = L + static_cast<int64_t>(r0 + min(rr, bs - 1)) * ld + j * FB + 64 * h;
+#pragma unroll 4
+            for (int m = 0; m < 16; ++m)
+            {
+                cp_async16(tiles + (t * 16 + m) * FT + tid, src + 4 * m);
+            }
         }
     }
     // this thread's half row of Linv_ii (zero above the diagonal; defined on
@@ -531,14 +534,14 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_f32_kernel(const float *__rest
     }
     __syncthreads();  // rhs rows are updated below by other threads
 
-    // blocks j < i - 1: rows warp + 8q, lanes own columns lane + 32c, FP64 sums
+    // blocks j < i - 2: rows warp + 8q, lanes own columns lane + 32c, FP64 sums
     double part[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q)
     {
         part[q] = 0.0;
     }
-    for (int j = 0; j < i - 1; ++j)
+    for (int j = 0; j < i - 2; ++j)
     {
         const int c0 = j * FB;
         float v[16][4];
@@ -556,7 +559,7 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_f32_kernel(const float *__rest
         double xv[4];
         {
             const double *xp[4] = { x + c0 + lane, x + c0 + lane + 32, x + c0 + lane + 64, x + c0 + lane + 96 };
-            await_x<4>(xp, xv, j == i - 2, st);
+            await_x<4>(xp, xv, j == i - 3, st);
         }
         float xf[4];
 #pragma unroll
@@ -576,7 +579,7 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_f32_kernel(const float *__rest
             part[q] += static_cast<double>(s2);
         }
     }
-    if (i > 1)
+    if (i > 2)
     {
         const double s2 = reduce_scatter16(part);
         if ((lane & 1) == 0)
@@ -585,8 +588,7 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_f32_kernel(const float *__rest
         }
     }
     cp_async_wait_all();
-    __syncthreads();  // tile landed, rhs complete
-    float lreg[64];
+    __syncthreads();  // tiles landed, rhs complete
     if (bs < FB)
     {
         // a ragged last block: the inverse is defined on rows and columns < bs only
@@ -598,29 +600,59 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_f32_kernel(const float *__rest
     }
     if (i > 0)
     {
+        float la[64], lb[64];  // L_{i,i-2} (zero for i = 1) and L_{i,i-1}
 #pragma unroll
         for (int k4 = 0; k4 < 16; ++k4)
         {
-            const float4 q = tileL[k4 * FT + tid];
-            lreg[4 * k4] = q.x;
-            lreg[4 * k4 + 1] = q.y;
-            lreg[4 * k4 + 2] = q.z;
-            lreg[4 * k4 + 3] = q.w;
+            const float4 q = tiles[(16 + k4) * FT + tid];
+            lb[4 * k4] = q.x;
+            lb[4 * k4 + 1] = q.y;
+            lb[4 * k4 + 2] = q.z;
+            lb[4 * k4 + 3] = q.w;
+        }
+        if (i > 1)
+        {
+#pragma unroll
+            for (int k4 = 0; k4 < 16; ++k4)
+            {
+                const float4 q = tiles[k4 * FT + tid];
+                la[4 * k4] = q.x;
+                la[4 * k4 + 1] = q.y;
+                la[4 * k4 + 2] = q.z;
+                la[4 * k4 + 3] = q.w;
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int k = 0; k < 64; ++k)
+            {
+                la[k] = 0.f;
+            }
         }
         if (warp == 0)
         {
-            const int c0 = (i - 1) * FB;
-            double xv[4];
-            const double *xp[4] = { x + c0 + lane, x + c0 + lane + 32, x + c0 + lane + 64, x + c0 + lane + 96 };
-            await_x<4>(xp, xv, true, st);
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+            for (int t = 0; t < 2; ++t)
             {
-                xs[lane + 32 * c] = static_cast<float>(xv[c]);
+                const int j = i - 2 + t;
+                double xv[4] = { 0.0, 0.0, 0.0, 0.0 };
+                if (j >= 0)
+                {
+                    const int c0 = j * FB;
+                    const double *xp[4] = { x + c0 + lane, x + c0 + lane + 32, x + c0 + lane + 64,
+                                            x + c0 + lane + 96 };
+                    await_x<4>(xp, xv, true, st);
+                }
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                {
+                    xs[t * FB + lane + 32 * c] = static_cast<float>(xv[c]);
+                }
             }
         }
-        __syncthreads();  // x_{i-1} staged
-        float s1 = dot64(lreg, xs + 64 * h);
+        __syncthreads();  // x_{i-2}, x_{i-1} staged
+        float s1 = dot64(la, xs + 64 * h) + dot64(lb, xs + FB + 64 * h);
         s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
         if (h == 0)
         {
@@ -648,18 +680,18 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_f32_kernel(const float *__rest
                                                              DeviceStatus *st)
 {
     extern __shared__ __align__(16) double sm[];
-    // L_{i+1,i} (rows of block i+1) row-major with stride TSTR; thread (cc, h)
-    // reads column cc, rows 2k + h
-    float *tileL = reinterpret_cast<float *>(sm);
-    double *rhs = reinterpret_cast<double *>(tileL + FB * TSTR);  // b_i - sum_{j > i+1} L_ji^T x_j
-    double *colpart = rhs + FB;                                     // [8][FB]
-    // x_{i+1} and the final right-hand side, split by row parity: v[p] at
-    // 64 (p & 1) + (p >> 1)
+    // L_{i+2,i} (tile 0) and L_{i+1,i} (tile 1), row-major with stride TSTR;
+    // thread (cc, h) reads column cc, rows 2k + h
+    float *tiles = reinterpret_cast<float *>(sm);
+    double *rhs = reinterpret_cast<double *>(tiles + 2 * FB * TSTR);  // b_i - sum_{j > i+2} L_ji^T x_j
+    double *colpart = rhs + FB;                                         // [8][FB]
+    // x_{i+2}, x_{i+1} and the final right-hand side, split by row parity:
+    // v[p] at 64 (p & 1) + (p >> 1)
     float *xs = reinterpret_cast<float *>(colpart + (FT / 32) * FB);
-    float *rs = xs + FB;
+    float *rs = xs + 2 * FB;
     int *shared_int = reinterpret_cast<int *>(rs + FB);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int cc = tid >> 1, h = tid & 1;  // the column and row parity of this thread in the two products
+    const int cc = tid >> 1, h = tid & 1;  // the column and row parity of this thread in the products
     for (;;)
     {
     if (tid == 0)
@@ -675,17 +707,22 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_f32_kernel(const float *__rest
     }
     const int c0 = i * FB;
     const int bs = min(FB, n - c0);
-    const bool has_next = i + 1 < nblk;
-    const int rs1 = has_next ? min(FB, n - (i + 1) * FB) : 0;  // rows of block i + 1
-    // start the copy of L_{i+1,i} (16-byte chunks, row by row)
-    if (has_next)
+    // start the copies of the near tiles (16-byte chunks, row by row); block
+    // i is full whenever a later block exists
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
     {
-#pragma unroll 4
-        for (int m = 0; m < 16; ++m)
+        const int j = i + 2 - t;
+        if (j < nblk)
         {
-            const int g = tid + FT * m, row = g >> 5, ch = g & 31;
-            cp_async16(tileL + row * TSTR + 4 * ch,
-                       L + static_cast<int64_t>((i + 1) * FB + min(row, rs1 - 1)) * ld + c0 + 4 * ch);
+            const int rsj = min(FB, n - j * FB);
+#pragma unroll 4
+            for (int m = 0; m < 16; ++m)
+            {
+                const int g = tid + FT * m, row = g >> 5, ch = g & 31;
+                cp_async16(tiles + (t * FB + row) * TSTR + 4 * ch,
+                           L + static_cast<int64_t>(j * FB + min(row, rsj - 1)) * ld + c0 + 4 * ch);
+            }
         }
     }
     // this thread's rows 2k + h of column cc of Linv_ii (zero above the
@@ -703,9 +740,9 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_f32_kernel(const float *__rest
     {
         rhs[tid] = (tid < bs) ? b[c0 + tid] : 0.0;
     }
-    // blocks j > i + 1: lanes own columns lane + 32c of block i, warps rows warp + 8q of block j
+    // blocks j > i + 2: lanes own columns lane + 32c of block i, warps rows warp + 8q of block j
     double part[4] = { 0.0, 0.0, 0.0, 0.0 };
-    for (int j = nblk - 1; j > i + 1; --j)
+    for (int j = nblk - 1; j > i + 2; --j)
     {
         const int r0 = j * FB;
         const int rsj = min(FB, n - r0);
@@ -729,7 +766,7 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_f32_kernel(const float *__rest
             {
                 xp[q] = x + r0 + min(warp + 8 * q, rsj - 1);
             }
-            await_x<16>(xp, xv, j == i + 2, st);
+            await_x<16>(xp, xv, j == i + 3, st);
         }
         float s2[4] = { 0.f, 0.f, 0.f, 0.f };
 #pragma unroll
@@ -755,7 +792,7 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_f32_kernel(const float *__rest
         colpart[warp * FB + lane + 32 * c] = part[c];
     }
     cp_async_wait_all();
-    __syncthreads();  // tile landed, column partials written
+    __syncthreads();  // tiles landed, column partials written
     if (tid < FB)
     {
         double s2 = 0.0;
@@ -766,7 +803,6 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_f32_kernel(const float *__rest
         }
         rhs[tid] -= s2;
     }
-    float lreg[64];
     if (bs < FB)
     {
         // a ragged last block: the inverse is defined on rows and columns < bs only
@@ -776,29 +812,55 @@ __global__ void __launch_bounds__(FT, 1) trsv_bwd_f32_kernel(const float *__rest
             ireg[k] = (cc < bs && 2 * k + h < bs) ? ireg[k] : 0.f;
         }
     }
-    if (has_next)
+    if (i + 1 < nblk)
     {
+        float la[64], lb[64];  // L_{i+2,i} (zero when block i+2 does not exist) and L_{i+1,i}
 #pragma unroll
         for (int k = 0; k < 64; ++k)
         {
-            lreg[k] = tileL[(2 * k + h) * TSTR + cc];
+            lb[k] = tiles[(FB + 2 * k + h) * TSTR + cc];
+        }
+        if (i + 2 < nblk)
+        {
+#pragma unroll
+            for (int k = 0; k < 64; ++k)
+            {
+                la[k] = tiles[(2 * k + h) * TSTR + cc];
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int k = 0; k < 64; ++k)
+            {
+                la[k] = 0.f;
+            }
         }
         if (warp == 0)
         {
-            const int r0 = (i + 1) * FB;
-            double xv[4];
-            const double *xp[4] = { x + r0 + min(lane, rs1 - 1), x + r0 + min(lane + 32, rs1 - 1),
-                                    x + r0 + min(lane + 64, rs1 - 1), x + r0 + min(lane + 96, rs1 - 1) };
-            await_x<4>(xp, xv, true, st);
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+            for (int t = 0; t < 2; ++t)
             {
-                const int p = lane + 32 * c;
-                xs[64 * (p & 1) + (p >> 1)] = (p < rs1) ? static_cast<float>(xv[c]) : 0.f;
+                const int j = i + 2 - t;
+                const int rsj = (j < nblk) ? min(FB, n - j * FB) : 0;
+                double xv[4] = { 0.0, 0.0, 0.0, 0.0 };
+                if (j < nblk)
+                {
+                    const int r0 = j * FB;
+                    const double *xp[4] = { x + r0 + min(lane, rsj - 1), x + r0 + min(lane + 32, rsj - 1),
+                                            x + r0 + min(lane + 64, rsj - 1), x + r0 + min(lane + 96, rsj - 1) };
+                    await_x<4>(xp, xv, true, st);
+                }
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                {
+                    const int p = lane + 32 * c;
+                    xs[t * FB + 64 * (p & 1) + (p >> 1)] = (p < rsj) ? static_cast<float>(xv[c]) : 0.f;
+                }
             }
         }
-        __syncthreads();  // x_{i+1} staged, rhs complete
-        float s1 = dot64(lreg, xs + 64 * h);
+        __syncthreads();  // x_{i+2}, x_{i+1} staged, rhs complete
+        float s1 = dot64(la, xs + 64 * h) + dot64(lb, xs + FB + 64 * h);
         s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
         if (h == 0)
         {
