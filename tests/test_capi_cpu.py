@@ -56,3 +56,34 @@ def test_null_handle_is_rejected():
     rc = capi.lib.gprat_cu_compute_loss(None, h.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(v))
     assert rc == capi.ERR_INVALID_ARG
     assert b"NULL" in capi.lib.gprat_cu_last_error()
+
+
+def test_multiserver_rejects_empty_device_list():
+    from gprat_b200 import serving
+    with pytest.raises(capi.GpratCudaError) as e:
+        serving.MultiServer([])
+    assert e.value.code == capi.ERR_INVALID_ARG
+
+
+def test_multiserver_without_a_device():
+    if capi.device_count() > 0:
+        pytest.skip("a GPU is visible")
+    from gprat_b200 import serving
+    with pytest.raises(capi.GpratCudaError) as e:
+        serving.MultiServer([0, 0])
+    assert e.value.code == capi.ERR_NO_DEVICE
+
+
+def test_multiserver_null_handle_is_rejected():
+    v = ctypes.c_int64()
+    assert capi.lib.gprat_cu_multiserver_wait(None, 1, None, None, None, None) == capi.ERR_INVALID_ARG
+    assert capi.lib.gprat_cu_multiserver_set_replication(None, capi.REPLICATE_COPY) == capi.ERR_INVALID_ARG
+    assert capi.lib.gprat_cu_multiserver_replica_completed(None, 0, ctypes.byref(v)) == capi.ERR_INVALID_ARG
+    assert capi.lib.gprat_cu_multiserver_destroy(None) == capi.OK
+
+
+def test_trsv_entry_rejects_bad_arguments():
+    L = np.eye(4)
+    with pytest.raises(capi.GpratCudaError) as e:
+        capi.test_trsv(2, L, np.ones(4))  # no such kind
+    assert e.value.code == capi.ERR_INVALID_ARG
