@@ -1,6 +1,8 @@
 // Single-launch blocked triangular solves L x = b and L^T x = b (FP64 right-
-// hand side; L in FP64 or FP32, row-major lower triangle; inverses of the
-// 128 x 128 diagonal blocks in FP64, or FP32 with an FP32 factor).
+// hand side; L row-major lower triangle with the inverses of its 128 x 128
+// diagonal blocks): the FP64 solves of alpha (trsv_fwd/bwd_fused_kernel) and
+// the FP32 solves of the mixed path's preconditioner (trsv_fwd/bwd_f32_kernel,
+// further down, which keep their chain in registers).
 //
 // forward_solve_tiled / backward_solve_tiled (core/src/cpu/tiled_algorithms.cpp:61-115)
 // walk the block columns one after another.  Launching one kernel per block
@@ -61,20 +63,6 @@ __device__ __forceinline__ void load_diag_inverse(double *dst, const double *Li)
         for (int c2 = lane; c2 < pairs; c2 += 32)
         {
             cp_async16(dst + packed_off(r) + 2 * c2, Li + r * FB + 2 * c2);
-        }
-    }
-}
-
-// FP32 inverse (mixed path): widened to FP64 into the same packed layout
-// (plain loads; the values are needed only after the block's last wait).
-__device__ __forceinline__ void load_diag_inverse(double *dst, const float *Li)
-{
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int r = warp; r < FB; r += FT / 32)
-    {
-        for (int c = lane; c <= r; c += 32)
-        {
-            dst[packed_off(r) + c] = static_cast<double>(Li[r * FB + c]);
         }
     }
 }
