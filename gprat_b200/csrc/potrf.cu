@@ -257,6 +257,122 @@ __device__ __forceinline__ void load_lower_async(const T *__restrict__ A, int64_
     }
 }
 
+// Barrier over the nthreads threads of warps first .. (a named barrier; id 0
+// with every thread is __syncthreads).
+__device__ __forceinline__ void bar_sync(int id, int nthreads)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Inverse of row block s (rows 32s .. 32s + 31), in place in sa, whose rows
+// < 32s already hold Linv:  Linv_s,<s = -X_s (L_s,<s Linv_<s,<s),  Linv_ss = X_s.
+// Run by nwarps warps starting at first_warp; barrier bar_id (over those
+// warps) separates the reads of L_s,<s from the writes that replace it.
+__device__ __forceinline__ void assemble_row_block(double *sa, const double *xs, double *tbuf, int s, int first_warp,
+                                                   int nwarps, int bar_id)
+{
+    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) - first_warp;
+    const int g = lane >> 2, t = lane & 3;
+    const int c0 = s * SB;
+    if (s > 0)
+    {
+        // T = L[c0.., 0..c0) Linv[0..c0, 0..c0)   (32 x c0; Linv lower: k >= n)
+        const int nt_count = c0 / 8;
+        for (int tile = w; tile < 2 * nt_count; tile += nwarps)
+        {
+            const int mi = tile / nt_count, nt = tile % nt_count;
+            double cf[4] = { 0.0, 0.0, 0.0, 0.0 };
+            for (int kk = nt; kk < nt_count; ++kk)
+            {
+                double af[4], bf[2];
+                frag_a(af, sa, PS, c0 + 16 * mi, 8 * kk, g, t);
+                frag_b(bf, sa, PS, 8 * nt, 8 * kk, g, t);
+                dmma(cf, af, bf);
+            }
+            double *c = tbuf + (16 * mi + g) * TS + 8 * nt + 2 * t;
+            c[0] = cf[0];
+            c[1] = cf[1];
+            c[8 * TS] = cf[2];
+            c[8 * TS + 1] = cf[3];
+        }
+        bar_sync(bar_id, nwarps * 32);
+        // Linv[c0.., 0..c0) = -X T   (X lower: k <= row)
+        for (int tile = w; tile < 2 * nt_count; tile += nwarps)
+        {
+            const int mi = tile / nt_count, nt = tile % nt_count;
+            double cf[4] = { 0.0, 0.0, 0.0, 0.0 };
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+            {
+                if (kk <= 2 * mi + 1)
+                {
+                    double af[4], bf[2];
+                    frag_a(af, xs, XS, 16 * mi, 8 * kk, g, t);
+                    frag_b(bf, tbuf, TS, 8 * nt, 8 * kk, g, t);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                    {
+                        af[e] = -af[e];
+                    }
+                    dmma(cf, af, bf);
+                }
+            }
+            double *c = sa + (c0 + 16 * mi + g) * PS + 8 * nt + 2 * t;
+            c[0] = cf[0];
+            c[1] = cf[1];
+            c[8 * PS] = cf[2];
+            c[8 * PS + 1] = cf[3];
+        }
+    }
+    // diagonal block: X_s (zero above the diagonal)
+    for (int q = w * 32 + lane; q < SB * SB; q += nwarps * 32)
+    {
+        const int i = q / SB, j = q % SB;
+        sa[(c0 + i) * PS + c0 + j] = (j <= i) ? xs[i * XS + j] : 0.0;
+    }
+}
+
+// Writes row block c0 .. c0 + 31 of L (lower triangle with the diagonal, rows
+// < bs) back to A: in pairs of columns when the block is 16-byte aligned,
+// else element by element.
+template <typename T>
+__device__ __forceinline__ void write_l_block(T *A, int64_t lda, const double *sa, int c0, int bs, bool aligned)
+{
+    using Pair = typename PairOf<T>::type;
+    for (int q = threadIdx.x; q < SB * (PB / 2); q += PTHREADS)
+    {
+        const int i = c0 + (q >> 6), c = 2 * (q & 63);
+        if (i >= bs || c > i)
+        {
+            continue;
+        }
+        T *dst = A + static_cast<int64_t>(i) * lda + c;
+        if (aligned)
+        {
+            const double2 v = *reinterpret_cast<const double2 *>(sa + i * PS + c);
+            if (c + 1 <= i)
+            {
+                Pair w;
+                w.x = static_cast<T>(v.x);
+                w.y = static_cast<T>(v.y);
+                *reinterpret_cast<Pair *>(dst) = w;
+            }
+            else
+            {
+                dst[0] = static_cast<T>(v.x);
+            }
+        }
+        else
+        {
+            dst[0] = static_cast<T>(sa[i * PS + c]);
+            if (c + 1 <= i)
+            {
+                dst[1] = static_cast<T>(sa[i * PS + c + 1]);
+            }
+        }
+    }
+}
+
 // True when the block and its rows start on 16-byte boundaries.
 template <typename T>
 __device__ __forceinline__ bool aligned16(const T *A, int64_t lda)
@@ -303,6 +419,7 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
     }
     __syncthreads();
 
+    const bool al = aligned16(A, lda);
 #pragma unroll 1
     for (int s = 0; s < 4; ++s)
     {
@@ -312,8 +429,24 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
         {
             diag_factor_invert(sa, c0, bs, row0, &bad, dinv + c0, colbuf);
         }
+        else if (s > 0)
+        {
+            // the previous row block's inverse, beside this sub-block's pivots
+            // (disjoint rows; later steps never read rows above c0)
+            assemble_row_block(sa, xall + (s - 1) * SB * XS, tbuf, s - 1, 1, NWARPS - 1, 1);
+        }
         __syncthreads();
         diag_inverse_all_warps(sa, c0, dinv + c0, xs);
+        // row block s of L is final: write it back (and its diagonal) before
+        // the assembly replaces it with Linv
+        if (write_l)
+        {
+            write_l_block(A, lda, sa, c0, bs, al);
+        }
+        if (diag_out != nullptr && tid < SB && c0 + tid < bs)
+        {
+            diag_out[c0 + tid] = sa[(c0 + tid) * PS + c0 + tid];
+        }
         __syncthreads();
         if (s == 3)
         {
@@ -402,113 +535,8 @@ __global__ void __launch_bounds__(PTHREADS, 1) potrf_inv_kernel(T *__restrict__ 
     {
         atomicCAS(&status->not_spd_row, 0, bad);
     }
-    // write L (lower triangle incl. diagonal) back, unless the caller has no
-    // use for it: in pairs of columns when the block is 16-byte aligned, else
-    // element by element
-    if (write_l && aligned16(A, lda))
-    {
-        using Pair = typename PairOf<T>::type;
-#pragma unroll 8
-        for (int q = 0; q < PB * PB / 2 / PTHREADS; ++q)
-        {
-            const int idx = q * PTHREADS + tid;
-            const int i = idx >> 6, c = 2 * (idx & 63);
-            T *dst = A + static_cast<int64_t>(i) * lda + c;
-            const double2 v = *reinterpret_cast<const double2 *>(sa + i * PS + c);
-            if (i < bs && c + 1 <= i)
-            {
-                Pair w;
-                w.x = static_cast<T>(v.x);
-                w.y = static_cast<T>(v.y);
-                *reinterpret_cast<Pair *>(dst) = w;
-            }
-            else if (i < bs && c == i)
-            {
-                dst[0] = static_cast<T>(v.x);
-            }
-        }
-    }
-    else if (write_l)
-    {
-        for (int q = tid; q < PB * PB; q += PTHREADS)
-        {
-            const int i = q >> 7, c = q & (PB - 1);
-            if (i < bs && c <= i)
-            {
-                A[static_cast<int64_t>(i) * lda + c] = static_cast<T>(sa[i * PS + c]);
-            }
-        }
-    }
-    if (diag_out != nullptr && tid < bs)
-    {
-        diag_out[tid] = sa[tid * PS + tid];
-    }
+    assemble_row_block(sa, xall + 3 * SB * XS, tbuf, 3, 0, NWARPS, 0);
     __syncthreads();
-
-    // --- full inverse, block row by block row (rows < c0 already hold Linv) --
-#pragma unroll 1
-    for (int s = 0; s < 4; ++s)
-    {
-        const int c0 = s * SB;
-        const double *xs = xall + s * SB * XS;
-        if (s > 0)
-        {
-            // T = L[c0.., 0..c0) Linv[0..c0, 0..c0)   (32 x c0; Linv lower: k >= n)
-            const int nt_count = c0 / 8;
-            for (int tile = warp; tile < 2 * nt_count; tile += NWARPS)
-            {
-                const int mi = tile / nt_count, nt = tile % nt_count;
-                double cf[4] = { 0.0, 0.0, 0.0, 0.0 };
-                for (int kk = nt; kk < nt_count; ++kk)
-                {
-                    double af[4], bf[2];
-                    frag_a(af, sa, PS, c0 + 16 * mi, 8 * kk, g, t);
-                    frag_b(bf, sa, PS, 8 * nt, 8 * kk, g, t);
-                    dmma(cf, af, bf);
-                }
-                double *c = tbuf + (16 * mi + g) * TS + 8 * nt + 2 * t;
-                c[0] = cf[0];
-                c[1] = cf[1];
-                c[8 * TS] = cf[2];
-                c[8 * TS + 1] = cf[3];
-            }
-            __syncthreads();
-            // Linv[c0.., 0..c0) = -X T   (X lower: k <= row)
-            for (int tile = warp; tile < 2 * nt_count; tile += NWARPS)
-            {
-                const int mi = tile / nt_count, nt = tile % nt_count;
-                double cf[4] = { 0.0, 0.0, 0.0, 0.0 };
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk)
-                {
-                    if (kk <= 2 * mi + 1)
-                    {
-                        double af[4], bf[2];
-                        frag_a(af, xs, XS, 16 * mi, 8 * kk, g, t);
-                        frag_b(bf, tbuf, TS, 8 * nt, 8 * kk, g, t);
-#pragma unroll
-                        for (int e = 0; e < 4; ++e)
-                        {
-                            af[e] = -af[e];
-                        }
-                        dmma(cf, af, bf);
-                    }
-                }
-                double *c = sa + (c0 + 16 * mi + g) * PS + 8 * nt + 2 * t;
-                c[0] = cf[0];
-                c[1] = cf[1];
-                c[8 * PS] = cf[2];
-                c[8 * PS + 1] = cf[3];
-            }
-        }
-        // diagonal block: X_s (zero above the diagonal)
-        for (int q = tid; q < SB * SB; q += PTHREADS)
-        {
-            const int i = q / SB, j = q % SB;
-            sa[(c0 + i) * PS + c0 + j] = (j <= i) ? xs[i * XS + j] : 0.0;
-        }
-        __syncthreads();
-    }
     pdl_launch_dependents();  // only the stores are left
     // store Linv (zero above the diagonal) in pairs of columns
 #pragma unroll 8
