@@ -14,10 +14,14 @@
 //   2. panel solve P = A_rs X_s^T and trailing update A_rr -= P P^T on the
 //      FP64 tensor cores (mma.sync m16n8k8 f64; upper-triangular zero blocks
 //      of X_s are skipped);
-// then the full inverse is assembled block row by block row on the tensor
+// and the full inverse is assembled block row by block row on the tensor
 // cores,  Linv_s,<s = -X_s (L_s,<s Linv_<s,<s),  Linv_ss = X_s,
 // which turns every later triangular solve against this block (panel trsm,
-// trsv, variance solve) into a GEMM.  L is written back to the lower
+// trsv, variance solve) into a GEMM.  Row block s is assembled by warps 1-7
+// while warp 0 runs the pivot chain of sub-block s+1 (the two touch disjoint
+// rows, and no later step reads rows above the current sub-block), so only
+// the last row block's assembly follows the factorisation; each row block of
+// L is written back before its assembly replaces it.  L is written back to the lower
 // triangle only (the strict upper triangle in global memory is never
 // touched, matching dpotrf2('L')).  A non-positive or NaN pivot is recorded
 // in the status word (first failing global row, 1-based); the reference
