@@ -29,6 +29,7 @@ ERR_NO_DEVICE = 6
 PREC_FP64 = 0
 PREC_MIXED_TF32 = 1
 PREC_MIXED_BF16 = 2
+PREC_FP64_INT8 = 3  # FP64 data, every product emulated on the int8 tensor cores (Ozaki scheme)
 
 REPLICATE_COPY = 0
 REPLICATE_REFIT = 1
@@ -60,6 +61,7 @@ def _load() -> ctypes.CDLL:
                                        ctypes.POINTER(ctypes.c_void_p)]
     lib.gprat_cu_gp_destroy.argtypes = [ctypes.c_void_p]
     lib.gprat_cu_gp_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.gprat_cu_gp_set_int8_slices.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.gprat_cu_cholesky.argtypes = [ctypes.c_void_p, _dp, _dp]
     lib.gprat_cu_predict.argtypes = [ctypes.c_void_p, _dp, _dp, _i64, ctypes.c_int, ctypes.c_int, _dp]
     for name in ("gprat_cu_predict_with_uncertainty", "gprat_cu_predict_with_full_cov"):
@@ -82,6 +84,11 @@ def _load() -> ctypes.CDLL:
     _vp, _i64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)
     lib.gprat_cu_steps_enable.argtypes = [ctypes.c_int]
     lib.gprat_cu_test_trsv.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int]
+    _i8p, _i32p = ctypes.POINTER(ctypes.c_int8), ctypes.POINTER(ctypes.c_int32)
+    lib.gprat_cu_test_oz_split.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, _i8p, _i32p]
+    lib.gprat_cu_test_oz_gemm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
+                                          ctypes.c_int]
     lib.gprat_cu_steps_csv.argtypes = [ctypes.c_char_p, _i64, _i64p]
     lib.gprat_cu_server_create.argtypes = [ctypes.c_int, _i64, ctypes.c_int, ctypes.POINTER(_vp)]
     lib.gprat_cu_server_destroy.argtypes = [_vp]
@@ -200,6 +207,36 @@ def test_trsv(kind: int, L: np.ndarray, b: np.ndarray, max_ctas: int = 0) -> Tup
     return xf, xb
 
 
+def test_oz_split(src: np.ndarray, s: int, block: bool) -> Tuple[np.ndarray, np.ndarray]:
+    """Splits src (rows x cols, cols a multiple of 128) into s int8 digit
+    planes on the device; returns (digits[s, rows, cols], exponents) with one
+    exponent per row and 128-column block (block=False) or per 128 x 128 block."""
+    src = np.ascontiguousarray(src, dtype=np.float64)
+    rows, cols = src.shape
+    digits = np.empty((s, rows, cols), dtype=np.int8)
+    er = (rows + 127) // 128 if block else rows
+    exps = np.empty((er, cols // 128), dtype=np.int32)
+    check(lib.gprat_cu_test_oz_split(rows, cols, _p(src), int(s), int(bool(block)),
+                                     digits.ctypes.data_as(ctypes.POINTER(ctypes.c_int8)),
+                                     exps.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+    return digits, exps
+
+
+def test_oz_gemm(A: np.ndarray, B: np.ndarray, C: np.ndarray, alpha: float, beta: float, s: int, groups: int = 0,
+                 lower: bool = False, rowsq: Optional[np.ndarray] = None, max_ctas: int = 0) -> None:
+    """Runs the int8-emulated FP64 GEMM C = beta*C + alpha*A B^T in place
+    (A: M x K, B: N x K, C: M x N, float64, K a multiple of 128; s digit
+    planes, `groups` digit groups kept, 0 = s)."""
+    for a in (A, B, C):
+        if a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise ValueError("A, B and C must be C-contiguous float64 arrays")
+    M, K = A.shape
+    N = B.shape[0]
+    rp = _p(rowsq) if rowsq is not None else None
+    check(lib.gprat_cu_test_oz_gemm(M, N, K, _p(A), _p(B), _p(C), float(alpha), float(beta), int(bool(lower)),
+                                    int(s), int(groups), rp, int(max_ctas)))
+
+
 def _arr(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
 
@@ -242,6 +279,10 @@ class CudaGP:
 
     def set_precision(self, precision: int) -> None:
         check(lib.gprat_cu_gp_set_precision(self._h, int(precision)))
+
+    def set_int8_slices(self, slices: int) -> None:
+        """Digit planes of the int8-emulated FP64 products (PREC_FP64_INT8), 3..8."""
+        check(lib.gprat_cu_gp_set_int8_slices(self._h, int(slices)))
 
     def cholesky(self, hyper) -> List[Optional[np.ndarray]]:
         nt, t = self.n_tiles, self.n_tile_size

@@ -202,23 +202,15 @@ void factor_fp64(gprat_cu_gp *gp, cudaStream_t s)
     cholesky_blocked(gp, s);
 }
 
-void solve_alpha_fp64(gprat_cu_gp *gp, cudaStream_t s)
+// The TF32 / BF16 modes: a low-precision working copy of the factor, alpha
+// refined by PCG, the variance from the low-precision factor.
+bool mixed(const gprat_cu_gp *gp)
 {
-    GPRAT_CUDA_CHECK(
-        cudaMemcpyAsync(gp->alpha.ptr, gp->y.ptr, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    gp->flags.ensure(2);
-    gp->trsv_b.ensure(gp->n);
-    {
-        StepScope step("forward", s);
-        trsv_fused_forward(gp->K.ptr, gp->ld, gp->Linv.ptr, gp->n, gp->alpha.ptr, gp->flags.ptr, gp->trsv_b.ptr,
-                           gp->status.ptr, s);
-    }
-    StepScope step("backward", s);
-    trsv_fused_backward(gp->K.ptr, gp->ld, gp->Linv.ptr, gp->n, gp->alpha.ptr, gp->flags.ptr, gp->trsv_b.ptr,
-                        gp->status.ptr, s);
+    return gp->precision == GPRAT_CU_PREC_MIXED_TF32 || gp->precision == GPRAT_CU_PREC_MIXED_BF16;
 }
 
-bool mixed(const gprat_cu_gp *gp) { return gp->precision != GPRAT_CU_PREC_FP64; }
+// The int8-emulated FP64 mode: an FP64 factor in K (loss and alpha as in FP64 mode).
+bool int8_fp64(const gprat_cu_gp *gp) { return gp->precision == GPRAT_CU_PREC_FP64_INT8; }
 
 // Factorisation + alpha in the handle's precision mode.
 void fit(gprat_cu_gp *gp, cudaStream_t s)
@@ -229,12 +221,22 @@ void fit(gprat_cu_gp *gp, cudaStream_t s)
         StepScope step("alpha refinement", s);
         alpha_mixed(gp, s);
     }
+    else if (int8_fp64(gp))
+    {
+        factor_oz(gp, s);
+        solve_alpha_fp64(gp, s);
+    }
     else
     {
         factor_fp64(gp, s);
         solve_alpha_fp64(gp, s);
     }
 }
+
+// Fit, mean and variance on the handle's streams: the overlapped pipelines
+// of the tensor-core modes, or fit then predict (FP64).  Used by the
+// host-buffer entry points and by the device-resident one alike.
+void fit_predict_var(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s);
 
 void loss_after_fit(gprat_cu_gp *gp, cudaStream_t s)
 {
@@ -304,6 +306,11 @@ void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
         variance_mixed(gp, d_xt, m, d_mean, d_var, s, row_offsets, 0, row_offsets == nullptr);
         return;
     }
+    if (int8_fp64(gp) && d_var != nullptr)
+    {
+        variance_oz(gp, d_xt, m, d_mean, d_var, s, row_offsets, 0, row_offsets == nullptr);
+        return;
+    }
     gp->mean_part.ensure(static_cast<int64_t>(m) * parts);
     if (d_var == nullptr)
     {
@@ -328,6 +335,23 @@ void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     }
     StepScope step("prediction uncertainty", s);
     finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, s);
+}
+
+void fit_predict_var(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
+{
+    if (mixed(gp))
+    {
+        fit_predict_mixed(gp, d_xt, m, d_mean, d_var, s);
+    }
+    else if (int8_fp64(gp))
+    {
+        fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);
+    }
+    else
+    {
+        fit(gp, s);
+        predict_device(gp, d_xt, m, d_mean, d_var, s);
+    }
 }
 
 void finish_and_check(gprat_cu_gp *gp)
@@ -524,9 +548,16 @@ void gp_check(gprat_cu_gp *gp, cudaStream_t s)
 int64_t gp_resident_bytes(const gprat_cu_gp *gp)
 {
     int64_t b = static_cast<int64_t>(gp->n) * gp->ld * 8 + static_cast<int64_t>(gp->nblk) * NB * NB * 8;
-    if (gp->precision != GPRAT_CU_PREC_FP64)
+    if (mixed(gp))
     {
         b += static_cast<int64_t>(gp->n) * gp->ld32 * (gp->precision == GPRAT_CU_PREC_MIXED_BF16 ? 6 : 4);
+    }
+    else if (int8_fp64(gp))
+    {
+        // row and block digit planes of L, their exponents, the inverses' planes, the panel scratch
+        const int64_t n = gp->n;
+        b += 2 * gp->oz_slices * n * n + (n * (n / 128) + (n / 128) * (n / 128)) * 4 +
+             static_cast<int64_t>(gp->oz_slices) * (gp->nblk * NB * NB + n * 128);
     }
     return b;
 }
@@ -540,6 +571,15 @@ void gp_reserve_predict(gprat_cu_gp *gp, int m)
     if (gp->precision == GPRAT_CU_PREC_FP64)
     {
         gp->W.ensure(static_cast<int64_t>(m) * gp->ld);
+    }
+    else if (int8_fp64(gp))
+    {
+        const int64_t S = gp->oz_slices;
+        gp->W.ensure(static_cast<int64_t>(m) * gp->ld);
+        gp->oz_w.ensure(S * m * gp->n);
+        gp->oz_w_e.ensure(static_cast<int64_t>(m) * (gp->n / 128));
+        gp->oz_wp.ensure(S * m * 128);
+        gp->oz_wp_e.ensure(m);
     }
     else
     {
@@ -615,6 +655,18 @@ int64_t gp_copy_fitted(gprat_cu_gp *dst, gprat_cu_gp *src)
     bytes += copy_buf(dst, dst->Linv32, src, src->Linv32, true);
     bytes += copy_buf(dst, dst->Lb, src, src->Lb, true);
     bytes += copy_buf(dst, dst->pcg_s, src, src->pcg_s, true);
+    // int8-emulated FP64 mode: the factor's and the inverses' digit planes
+    for (auto pr : { std::make_pair(&dst->oz_lr, &src->oz_lr), std::make_pair(&dst->oz_lb, &src->oz_lb),
+                     std::make_pair(&dst->oz_inv, &src->oz_inv), std::make_pair(&dst->oz_p, &src->oz_p) })
+    {
+        bytes += copy_buf(dst, *pr.first, src, *pr.second, true);
+    }
+    for (auto pr : { std::make_pair(&dst->oz_lr_e, &src->oz_lr_e), std::make_pair(&dst->oz_lb_e, &src->oz_lb_e),
+                     std::make_pair(&dst->oz_inv_e, &src->oz_inv_e), std::make_pair(&dst->oz_p_e, &src->oz_p_e) })
+    {
+        bytes += copy_buf(dst, *pr.first, src, *pr.second, true);
+    }
+    dst->oz_slices = src->oz_slices;
     bytes += copy_buf(dst, dst->flags, src, src->flags, true);
     bytes += copy_buf(dst, dst->params, src, src->params, true);
     bytes += copy_buf(dst, dst->status, src, src->status, true);
@@ -627,6 +679,11 @@ int64_t gp_copy_fitted(gprat_cu_gp *dst, gprat_cu_gp *src)
     }
     copy_buf(dst, dst->W32, src, src->W32, false);
     copy_buf(dst, dst->Wb, src, src->Wb, false);
+    copy_buf(dst, dst->oz_w, src, src->oz_w, false);
+    copy_buf(dst, dst->oz_wp, src, src->oz_wp, false);
+    copy_buf(dst, dst->oz_w_e, src, src->oz_w_e, false);
+    copy_buf(dst, dst->oz_wp_e, src, src->oz_wp_e, false);
+    copy_buf(dst, dst->Kx, src, src->Kx, false);
     GPRAT_CUDA_CHECK(cudaStreamSynchronize(dst->stream));
     dst->pcg_last_iters = src->pcg_last_iters;
     return bytes;
@@ -635,8 +692,13 @@ int64_t gp_copy_fitted(gprat_cu_gp *dst, gprat_cu_gp *src)
 int64_t gp_predict_bytes(const gprat_cu_gp *gp, int m)
 {
     // solve matrix + mean partials + variance accumulator for m rows
-    const int64_t w = gp->precision == GPRAT_CU_PREC_FP64 ? static_cast<int64_t>(m) * gp->ld * 8
-                                                          : static_cast<int64_t>(m) * gp->ld32 * 4;
+    int64_t w = gp->precision == GPRAT_CU_PREC_FP64 ? static_cast<int64_t>(m) * gp->ld * 8
+                                                    : static_cast<int64_t>(m) * gp->ld32 * 4;
+    if (int8_fp64(gp))
+    {
+        // FP64 W plus its digit planes
+        w = static_cast<int64_t>(m) * (gp->ld * 8 + static_cast<int64_t>(gp->oz_slices) * (gp->n + 128) + gp->n / 32 + 4);
+    }
     return w + static_cast<int64_t>(m) * (ceil_div(gp->n, 128) + 2) * 8;
 }
 }  // namespace gprat_cu
@@ -748,12 +810,25 @@ int gprat_cu_gp_set_precision(gprat_cu_gp *gp, int precision)
         {
             check_gp(gp);
             require(precision == GPRAT_CU_PREC_FP64 || precision == GPRAT_CU_PREC_MIXED_TF32 ||
-                        precision == GPRAT_CU_PREC_MIXED_BF16,
+                        precision == GPRAT_CU_PREC_MIXED_BF16 || precision == GPRAT_CU_PREC_FP64_INT8,
                     "unknown precision mode " + std::to_string(precision));
             require(precision == GPRAT_CU_PREC_FP64 || gp->n % NB == 0,
-                    "mixed precision needs n_tiles * n_tile_size to be a multiple of 128 (got " +
+                    "the tensor-core precision modes need n_tiles * n_tile_size to be a multiple of 128 (got " +
                         std::to_string(gp->n) + ")");
             gp->precision = precision;
+        });
+}
+
+int gprat_cu_gp_set_int8_slices(gprat_cu_gp *gp, int slices)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(slices >= OZ_MIN_SLICES && slices <= OZ_MAX_SLICES,
+                    "int8 slices must be in [" + std::to_string(OZ_MIN_SLICES) + ", " + std::to_string(OZ_MAX_SLICES) +
+                        "] (got " + std::to_string(slices) + ")");
+            gp->oz_slices = slices;
         });
 }
 
@@ -832,15 +907,7 @@ static int predict_var_common(gprat_cu_gp *gp, const double hyper[3], const doub
             upload_test(gp, test_in, n_test_in, m);
             gp->mean.ensure(std::max(m, 1));
             gp->var.ensure(std::max(m, 1));
-            if (mixed(gp))
-            {
-                fit_predict_mixed(gp, gp->xt.ptr, m, gp->mean.ptr, gp->var.ptr, gp->stream);
-            }
-            else
-            {
-                fit(gp, gp->stream);
-                predict_device(gp, gp->xt.ptr, m, gp->mean.ptr, gp->var.ptr, gp->stream);
-            }
+            fit_predict_var(gp, gp->xt.ptr, m, gp->mean.ptr, gp->var.ptr, gp->stream);
             download(gp, mean, gp->mean.ptr, m);
             download(gp, var, gp->var.ptr, m);
             finish_and_check(gp);
@@ -1044,8 +1111,16 @@ int gprat_cu_fit_predict_device(gprat_cu_gp *gp, const double hyper[3], const do
             DeviceGuard guard(gp->device);
             cudaStream_t s = stream != nullptr ? static_cast<cudaStream_t>(stream) : gp->stream;
             upload_hyper(gp, hyper, s);
-            fit(gp, s);
-            predict_device(gp, d_test_in, m, d_mean, d_var, s);
+            if (d_var != nullptr)
+            {
+                // the schedule gprat_cu_predict_with_uncertainty runs
+                fit_predict_var(gp, d_test_in, m, d_mean, d_var, s);
+            }
+            else
+            {
+                fit(gp, s);
+                predict_device(gp, d_test_in, m, d_mean, nullptr, s);
+            }
         });
 }
 

@@ -4,6 +4,7 @@
 
 #include "common.cuh"
 #include "gprat_cu.h"
+#include "ozaki.cuh"
 #include "tc_gemm.cuh"
 
 #include <initializer_list>
@@ -107,6 +108,16 @@ struct gprat_cu_gp
     gprat_cu::DevBuf<int> flags;         // ticket counter of the single-launch solves
     gprat_cu::DevBuf<double> trsv_b;     // right-hand side copy of the single-launch solves
 
+    // int8-emulated FP64 path (GPRAT_CU_PREC_FP64_INT8): digit planes of the
+    // solved factor L with row exponents (A role) and block exponents (B
+    // role), of the diagonal-block inverses (B role), of one unsolved panel
+    // block (A role, scratch), of the solved rows of W and of one unsolved W
+    // block (A role); the cross covariance kept in FP64 for the mean
+    int oz_slices = 6;
+    gprat_cu::DevBuf<int8_t> oz_lr, oz_lb, oz_inv, oz_p, oz_w, oz_wp;
+    gprat_cu::DevBuf<int32_t> oz_lr_e, oz_lb_e, oz_inv_e, oz_p_e, oz_w_e, oz_wp_e;
+    gprat_cu::DevBuf<double> Kx;
+
     ~gprat_cu_gp()
     {
         int prev = -1;
@@ -135,6 +146,15 @@ struct gprat_cu_gp
         Lb.release();
         Wb.release();
         pcg_s.release();
+        for (gprat_cu::DevBuf<int8_t> *b : { &oz_lr, &oz_lb, &oz_inv, &oz_p, &oz_w, &oz_wp })
+        {
+            b->release();
+        }
+        for (gprat_cu::DevBuf<int32_t> *b : { &oz_lr_e, &oz_lb_e, &oz_inv_e, &oz_p_e, &oz_w_e, &oz_wp_e })
+        {
+            b->release();
+        }
+        Kx.release();
         flags.release();
         params.release();
         status.release();
@@ -196,5 +216,27 @@ void gp_reserve_predict(gprat_cu_gp *gp, int m);
 // Returns the bytes copied.
 int64_t gp_copy_fitted(gprat_cu_gp *dst, gprat_cu_gp *src);
 void loss_mixed(gprat_cu_gp *gp, cudaStream_t s);
+
+// mixed.cu: helpers shared by the look-ahead pipelines
+// A tuning knob: the environment variable `name` if it holds an integer in
+// [lo, hi], else the compiled default.
+int knob(const char *name, int dflt, int lo, int hi);
+// A share of the SMs in percent (knob in [10, 100]).
+int sm_percent(const char *name, int dflt);
+// Creates the side and variance streams and at least nevents events.
+void ensure_lookahead(gprat_cu_gp *gp, int nevents);
+// Events one look-ahead pipeline over n training points uses.
+int lookahead_events(int n);
+
+// ozaki_path.cu: the FP64-accurate pipeline on the int8 tensor cores
+// (GPRAT_CU_PREC_FP64_INT8).  The factor is FP64 (in K, with Linv), every
+// product runs as an int8-emulated FP64 GEMM, alpha comes from the FP64
+// triangular solves.
+void factor_oz(gprat_cu_gp *gp, cudaStream_t s, const std::vector<std::pair<int, cudaEvent_t>> &splits = {});
+void variance_oz(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s,
+                 const int64_t *row_offsets = nullptr, int max_ctas = 0, bool recursive = true);
+void fit_predict_oz(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s);
+// FP64 forward and backward solves for alpha with the FP64 factor in K.
+void solve_alpha_fp64(gprat_cu_gp *gp, cudaStream_t s, int max_ctas = 0);
 
 }  // namespace gprat_cu

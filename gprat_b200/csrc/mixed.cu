@@ -402,8 +402,7 @@ void precondition(gprat_cu_gp *gp, const double *r, double *z, cudaStream_t s, i
 
 }  // namespace
 
-namespace
-{
+// Helpers shared with the int8-emulated FP64 pipeline (ozaki_path.cu).
 
 // Share of the SMs the main stream's trailing update may hold while the
 // look-ahead stream works next to it (persistent CTAs never yield their SM,
@@ -467,8 +466,6 @@ TcGemmArgs limited(TcGemmArgs a, int max_ctas)
     a.max_ctas = max_ctas;
     return a;
 }
-
-}  // namespace
 
 // Right-looking Cholesky of the FP32 working copy in outer panels of nbo
 // columns (inner blocks of NB), with a look-ahead of one panel:

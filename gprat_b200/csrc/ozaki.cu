@@ -1,0 +1,891 @@
+// FP64 matrix products on the int8 tensor cores (Ozaki scheme); the method
+// and the slice representation are described in ozaki.cuh.
+//
+// oz_split_kernel: one CTA per 128 x 128 block of the FP64 source, 8 warps of
+// 16 rows; a lane holds 4 consecutive values of a row.  Pass 1 finds the
+// row maxima (and the block maximum), pass 2 re-reads the block (L1/L2) and
+// writes s digit planes, 4 bytes per lane and plane (128-byte rows).  Digits
+// are peeled with the 1.5 * 2^52 rounding trick: y = t + 1.5 * 2^52 rounds t
+// to the nearest integer d (ties to even), d is the low word of y, and
+// t <- (t - d) * 128 is exact, so D_0 .. D_{s-1} are the leading s balanced
+// base-128 digits of x * 2^(6 - e).
+//
+// oz_gemm_kernel: persistent, warp-specialised CTA pair (cluster of 2, 320
+// threads each), one 256 x 128 output tile per pair at a time:
+//   warp 0, one lane (both CTAs): TMA producer.  For each 128-column block k
+//     and group g it loads A digit plane g (this CTA's 128 rows, 16 KB) into
+//     a ring of OZ_RA slots, then the B digit planes g - p, p = 0..g (this
+//     CTA's 64 rows, 8 KB) into a ring of OZ_RB slots.  The A planes of a
+//     block stay resident until its last group, so each A tile crosses from
+//     L2 once per block and each B tile once per pair (p, g - p).
+//   warp 1, one lane (leader): MMA issuer.  Group g of block k is one unit:
+//     for p = 0..g, four tcgen05.mma.cta_group::2.kind::i8 (M 256, N 128,
+//     K 32) of A_p against B_{g-p} into one int32 accumulator in tensor
+//     memory (four accumulators of 128 columns rotate); tcgen05.commit frees
+//     B slots, the accumulator, and after the block's last group its A slots.
+//   warps 2..9 (both CTAs): epilogue.  Two warps per TMEM lane quarter, 64
+//     columns each; every unit is read with tcgen05.ld, converted exactly to
+//     FP64 (2^52 + 2^31 bias trick) and added with its scale
+//     2^(eA + eB - 12 - 7 g) into 64 FP64 registers per thread.  After the
+//     tile's last unit, alpha * acc is staged per warp in shared memory
+//     (16-byte XOR swizzle) and written to C with coalesced 16-byte accesses
+//     (beta = 1 adds to C).
+// Every mbarrier wait is bounded (tcgen05_ptx.cuh); a wait that gives up
+// raises the CTA's abort flag, the roles leave their loops, TMA copies in
+// flight get 200 us to land, the MMA issuer drains, TMEM is freed and the
+// status word's timeout flag is set.  No TMA multicast is used.
+#include "ozaki.cuh"
+#include "tcgen05_ptx.cuh"
+
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+
+namespace gprat_cu
+{
+namespace
+{
+
+using namespace tcx;
+
+constexpr int OZ_ZERO_EXP = -2000;  // an all-zero domain: digits 0
+constexpr int OZ_BAD_EXP = 4000;    // a NaN or infinity in the domain: the product becomes NaN
+constexpr double RND = 6755399441055744.0;      // 1.5 * 2^52
+constexpr double I2D_BIAS = 4503601774854144.0;  // 2^52 + 2^31
+
+__device__ __forceinline__ double pow2(int e)
+{
+    e = max(-1022, min(1023, e));
+    return __longlong_as_double(static_cast<long long>(e + 1023) << 52);
+}
+
+// e with max|x| < 2^e over a domain whose maximum is vmax
+__device__ __forceinline__ int exp_of(double vmax, bool bad)
+{
+    if (bad)
+    {
+        return OZ_BAD_EXP;
+    }
+    if (vmax == 0.0)
+    {
+        return OZ_ZERO_EXP;
+    }
+    const int e = ilogb(vmax) + 1;
+    return e < -960 ? OZ_ZERO_EXP : e;
+}
+
+// s digit planes of 4 consecutive values (4 bytes per plane at out + p * plane)
+__device__ __forceinline__ void write_digits(const double v[4], int e, int s, int8_t *out, int64_t plane)
+{
+    double t[4];
+    const bool zero = (e == OZ_ZERO_EXP || e == OZ_BAD_EXP);
+    const double sc = zero ? 0.0 : pow2(6 - e);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        t[i] = __dmul_rn(v[i], sc);
+    }
+    for (int p = 0; p < s; ++p)
+    {
+        uint32_t word = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+            const double y = __dadd_rn(t[i], RND);
+            const int d = __double2loint(y);
+            const double r = __dsub_rn(y, RND);
+            t[i] = __dmul_rn(__dsub_rn(t[i], r), 128.0);
+            word |= (static_cast<uint32_t>(d) & 0xffu) << (8 * i);
+        }
+        *reinterpret_cast<uint32_t *>(out + p * plane) = word;
+    }
+}
+
+constexpr int SPLIT_THREADS = 256;
+
+__global__ void __launch_bounds__(SPLIT_THREADS) oz_split_kernel(const double *__restrict__ src, int64_t lds, int rows,
+                                                                 int8_t *rdig, int64_t rld, int64_t rplane,
+                                                                 int32_t *rexp, int rldE, int8_t *bdig, int64_t bld,
+                                                                 int64_t bplane, int32_t *bexp, int bldE, int dst_row0,
+                                                                 int dst_kb0, int s)
+{
+    __shared__ double wmax[SPLIT_THREADS / 32];
+    __shared__ int wbad[SPLIT_THREADS / 32];
+    pdl_wait();
+    const int rb = blockIdx.x, kb = blockIdx.y;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t col = static_cast<int64_t>(kb) * OZ_KB + lane * 4;
+    const int r_first = rb * 128 + warp * 16;
+    int er[16];
+    double bm = 0.0;
+    bool bbad = false;
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+    {
+        const int r = r_first + i;
+        double m = 0.0;
+        bool bad = false;
+        if (r < rows)
+        {
+            const double2 *p2 = reinterpret_cast<const double2 *>(src + static_cast<int64_t>(r) * lds + col);
+            const double2 a = p2[0], b = p2[1];
+            const double v[4] = { a.x, a.y, b.x, b.y };
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const double av = fabs(v[j]);
+                bad = bad || !(av <= 1.0e308);
+                m = fmax(m, av);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        }
+        bad = __any_sync(0xffffffffu, bad);
+        er[i] = exp_of(m, bad);
+        if (rdig != nullptr && r < rows && lane == 0)
+        {
+            rexp[static_cast<int64_t>(dst_row0 + r) * rldE + dst_kb0 + kb] = er[i];
+        }
+        bm = fmax(bm, m);
+        bbad = bbad || bad;
+    }
+    if (lane == 0)
+    {
+        wmax[warp] = bm;
+        wbad[warp] = bbad ? 1 : 0;
+    }
+    __syncthreads();
+    double blk = 0.0;
+    bool blkbad = false;
+#pragma unroll
+    for (int w = 0; w < SPLIT_THREADS / 32; ++w)
+    {
+        blk = fmax(blk, wmax[w]);
+        blkbad = blkbad || wbad[w] != 0;
+    }
+    const int eb = exp_of(blk, blkbad);
+    if (bdig != nullptr && threadIdx.x == 0)
+    {
+        bexp[static_cast<int64_t>(dst_row0 / 128 + rb) * bldE + dst_kb0 + kb] = eb;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+    {
+        const int r = r_first + i;
+        if (r >= rows)
+        {
+            break;
+        }
+        const double2 *p2 = reinterpret_cast<const double2 *>(src + static_cast<int64_t>(r) * lds + col);
+        const double2 a = p2[0], b = p2[1];
+        const double v[4] = { a.x, a.y, b.x, b.y };
+        const int64_t dcol = static_cast<int64_t>(dst_kb0 + kb) * OZ_KB + lane * 4;
+        if (rdig != nullptr)
+        {
+            write_digits(v, er[i], s, rdig + static_cast<int64_t>(dst_row0 + r) * rld + dcol, rplane);
+        }
+        if (bdig != nullptr)
+        {
+            write_digits(v, eb, s, bdig + static_cast<int64_t>(dst_row0 + r) * bld + dcol, bplane);
+        }
+    }
+    pdl_launch_dependents();
+}
+
+// ---------------------------------------------------------------------------
+// GEMM
+
+constexpr int OZ_THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
+constexpr int OZ_EPI_WARPS = 8;
+constexpr int OZ_A_BYTES = 128 * 128;  // 128 rows x 128 digit bytes
+constexpr int OZ_B_BYTES = 64 * 128;   // this CTA's half of the 128 B rows
+constexpr int OZ_RA = 9;               // A ring slots (>= s + 1: the next block's first planes load early)
+constexpr int OZ_RB = 6;               // B ring slots
+constexpr int OZ_NACC = 4;             // int32 accumulators of 128 TMEM columns
+constexpr int OZ_TMEM_COLS = OZ_NACC * 128;
+constexpr int OZ_EPI_BUF = 32 * 128;  // 32 rows x 16 doubles per epilogue warp
+constexpr int OZ_SMEM_BYTES =
+    1024 + OZ_RA * OZ_A_BYTES + OZ_RB * OZ_B_BYTES + OZ_EPI_WARPS * OZ_EPI_BUF + 512;
+static_assert(OZ_SMEM_BYTES <= 232448, "shared memory of the int8 GEMM exceeds the per-CTA limit");
+static_assert(OZ_RA >= OZ_MAX_SLICES + 1, "the A ring must hold one block's planes plus one");
+// D = S32, A and B signed 8-bit, K-major, N = 128, M = 256 (CTA pair)
+constexpr uint32_t OZ_IDESC =
+    (2u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((256u >> 4) << 24);
+constexpr int OZ_GROUP_M = 8;  // row tiles per group of the non-lower tile order
+
+struct OzKernelArgs
+{
+    int M, N, nkb;
+    int a_row0, a_col0, b_row0, b_col0;
+    const int32_t *ea;
+    int ldea;
+    const int32_t *eb;
+    int ldeb;
+    double *C;
+    int64_t ldc;
+    double alpha;
+    int beta;
+    int lower;
+    double *rowsq;
+    int64_t rowsq_half;
+    DeviceStatus *status;
+    int groups;
+    int tiles_m, tiles_n, ntiles;
+};
+
+__device__ __forceinline__ void tma_load_3d_pair(void *dst, const CUtensorMap *map, uint32_t leader_bar, int x, int y,
+                                                 int z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
+        "%5}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(leader_bar), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(OZ_IDESC), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tmem_ld32_i(uint32_t taddr, int32_t *v)
+{
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+    {
+        v[j] = static_cast<int32_t>(r[j]);
+    }
+}
+
+// exact int32 -> FP64: the bit pattern 0x43300000:(v ^ 2^31) is 2^52 + 2^31 + v
+__device__ __forceinline__ double i2d(int32_t v)
+{
+    return __dsub_rn(__hiloint2double(0x43300000, v ^ static_cast<int32_t>(0x80000000u)), I2D_BIAS);
+}
+
+// pair tile t -> (m0, n0): 256-row x 128-column tiles.  Lower mode: row tile i
+// holds the 2 i + 2 column tiles that reach its last row (the final one is
+// dropped by the host when it lies right of N).
+__device__ __forceinline__ void oz_tile(int t, bool lower, int tiles_m, int tiles_n, int &m0, int &n0)
+{
+    if (!lower)
+    {
+        const int span = OZ_GROUP_M * tiles_n;
+        const int g = t / span;
+        const int first = g * OZ_GROUP_M;
+        const int gm = min(tiles_m - first, OZ_GROUP_M);
+        const int r = t - g * span;
+        m0 = (first + r % gm) * 256;
+        n0 = (r / gm) * 128;
+        return;
+    }
+    int i = static_cast<int>((sqrt(4.0 * t + 1.0) - 1.0) * 0.5);
+    while ((i + 1) * (i + 2) <= t)
+    {
+        ++i;
+    }
+    while (i > 0 && i * (i + 1) > t)
+    {
+        --i;
+    }
+    m0 = i * 256;
+    n0 = (t - i * (i + 1)) * 128;
+}
+
+__global__ void __maxnreg__(200)
+    oz_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzKernelArgs p)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t *aring = smem;
+    uint8_t *bring = aring + OZ_RA * OZ_A_BYTES;
+    uint8_t *epi = bring + OZ_RB * OZ_B_BYTES;
+    uint64_t *afull = reinterpret_cast<uint64_t *>(epi + OZ_EPI_WARPS * OZ_EPI_BUF);
+    uint64_t *aempty = afull + OZ_RA;
+    uint64_t *bfull = aempty + OZ_RA;
+    uint64_t *bempty = bfull + OZ_RB;
+    uint64_t *tfull = bempty + OZ_RB;
+    uint64_t *tempty = tfull + OZ_NACC;
+    uint64_t *drain = tempty + OZ_NACC;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const int pair = blockIdx.x >> 1;
+    const int npairs = gridDim.x >> 1;
+    const int G = p.groups;
+
+    if (threadIdx.x == 0)
+    {
+        for (int i = 0; i < OZ_RA; ++i)
+        {
+            mbar_init(&afull[i], 1);
+            mbar_init(&aempty[i], 1);
+        }
+        for (int i = 0; i < OZ_RB; ++i)
+        {
+            mbar_init(&bfull[i], 1);
+            mbar_init(&bempty[i], 1);
+        }
+        for (int u = 0; u < OZ_NACC; ++u)
+        {
+            mbar_init(&tfull[u], 1);
+            mbar_init(&tempty[u], 2 * OZ_EPI_WARPS);
+        }
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(OZ_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::);
+    }
+    tc_fence_before();
+    cluster_sync_all();  // barriers of both CTAs initialised, TMEM allocated
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    pdl_wait();  // the previous kernel's results are visible from here on
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            // ---------------- TMA producer (both CTAs) ----------------
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+            int na = 0, nb = 0;
+            bool ok = true;
+            for (int t = pair; ok && t < p.ntiles; t += npairs)
+            {
+                int m0, n0;
+                oz_tile(t, p.lower != 0, p.tiles_m, p.tiles_n, m0, n0);
+                const int arow = p.a_row0 + m0 + 128 * static_cast<int>(rank);
+                const int brow = p.b_row0 + n0 + 64 * static_cast<int>(rank);
+                for (int kb = 0; ok && kb < p.nkb; ++kb)
+                {
+                    const int xa = p.a_col0 + kb * OZ_KB, xb = p.b_col0 + kb * OZ_KB;
+                    for (int g = 0; ok && g < G; ++g)
+                    {
+                        {
+                            const int slot = na % OZ_RA;
+                            if (!mbar_wait(&aempty[slot], ((na / OZ_RA) & 1u) ^ 1u, abort_flag))
+                            {
+                                ok = false;
+                                break;
+                            }
+                            if (leader)
+                            {
+                                mbar_expect_tx(&afull[slot], 2 * OZ_A_BYTES);  // both CTAs' bytes
+                            }
+                            tma_load_3d_pair(aring + slot * OZ_A_BYTES, &tmA, map_to_rank(&afull[slot], 0), xa, arow,
+                                             g);
+                            ++na;
+                        }
+                        for (int q = g; q >= 0; --q)  // pairs (g - q, q): B plane q
+                        {
+                            const int slot = nb % OZ_RB;
+                            if (!mbar_wait(&bempty[slot], ((nb / OZ_RB) & 1u) ^ 1u, abort_flag))
+                            {
+                                ok = false;
+                                break;
+                            }
+                            if (leader)
+                            {
+                                mbar_expect_tx(&bfull[slot], 2 * OZ_B_BYTES);
+                            }
+                            tma_load_3d_pair(bring + slot * OZ_B_BYTES, &tmB, map_to_rank(&bfull[slot], 0), xb, brow,
+                                             q);
+                            ++nb;
+                        }
+                    }
+                }
+            }
+            if (*abort_flag)
+            {
+                // give copies already in flight time to land before the CTA exits
+                const unsigned long long t0 = global_ns();
+                while (global_ns() - t0 < 200000ull)
+                {
+                }
+            }
+        }
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0 && leader)
+        {
+            // ---------------- MMA issuer (leader only) ----------------
+            int na = 0, nb = 0, nu = 0;
+            bool ok = true;
+            for (int t = pair; ok && t < p.ntiles; t += npairs)
+            {
+                for (int kb = 0; ok && kb < p.nkb; ++kb)
+                {
+                    const int abase = na;
+                    for (int g = 0; ok && g < G; ++g)
+                    {
+                        const int u = nu % OZ_NACC;
+                        if (!mbar_wait(&tempty[u], ((nu / OZ_NACC) & 1u) ^ 1u, abort_flag))
+                        {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t d = tmem_base + static_cast<uint32_t>(u * 128);
+                        for (int pa = 0; pa <= g; ++pa)  // A plane pa, B plane g - pa (the producer's order)
+                        {
+                            const int ai = abase + pa;
+                            const int aslot = ai % OZ_RA;
+                            if (pa == g && !mbar_wait(&afull[aslot], (ai / OZ_RA) & 1u, abort_flag))
+                            {
+                                ok = false;
+                                break;
+                            }
+                            const int bslot = nb % OZ_RB;
+                            if (!mbar_wait(&bfull[bslot], (nb / OZ_RB) & 1u, abort_flag))
+                            {
+                                ok = false;
+                                break;
+                            }
+                            tc_fence_after();
+                            const uint64_t adesc = sw128_desc(smem_u32(aring + aslot * OZ_A_BYTES));
+                            const uint64_t bdesc = sw128_desc(smem_u32(bring + bslot * OZ_B_BYTES));
+#pragma unroll
+                            for (int kk = 0; kk < 4; ++kk)
+                            {
+                                // 32 bytes of K per instruction: advance the start address by 2 x 16 B
+                                mma_i8_pair(d, adesc + 2 * kk, bdesc + 2 * kk, (pa | kk) != 0 ? 1u : 0u);
+                            }
+                            mma_commit_pair_both(&bempty[bslot]);
+                            ++nb;
+                        }
+                        if (!ok)
+                        {
+                            break;
+                        }
+                        mma_commit_pair_both(&tfull[u]);
+                        ++nu;
+                    }
+                    if (!ok)
+                    {
+                        break;
+                    }
+                    for (int pa = 0; pa < G; ++pa)
+                    {
+                        mma_commit_pair_both(&aempty[(abase + pa) % OZ_RA]);
+                    }
+                    na += G;
+                }
+            }
+            // drain: arrives once every MMA issued above has completed
+            mma_commit_pair_local(drain);
+            mbar_wait(drain, 0u, abort_flag);
+        }
+    }
+    else
+    {
+        // ---------------- epilogue (warps 2..9 of both CTAs) ----------------
+        const int ew = warp - 2;
+        const int q = warp & 3;  // TMEM lane quarter this warp may access
+        const int h = ew >> 2;   // column half
+        uint8_t *buf = epi + ew * OZ_EPI_BUF;
+        const uint32_t buf_s = smem_u32(buf);
+        int nu = 0;
+        bool ok = true;
+        for (int t = pair; ok && t < p.ntiles; t += npairs)
+        {
+            int mp, n0;
+            oz_tile(t, p.lower != 0, p.tiles_m, p.tiles_n, mp, n0);
+            const int row0w = mp + 128 * static_cast<int>(rank) + q * 32;  // this warp's first row of C
+            const int row = row0w + lane;
+            const bool rvalid = row < p.M;
+            const int32_t *earow = p.ea + static_cast<int64_t>(p.a_row0 + (rvalid ? row : 0)) * p.ldea + p.a_col0 / OZ_KB;
+            const int32_t *ebblk = p.eb + static_cast<int64_t>((p.b_row0 + n0) / 128) * p.ldeb + p.b_col0 / OZ_KB;
+            double acc[64];
+#pragma unroll
+            for (int j = 0; j < 64; ++j)
+            {
+                acc[j] = 0.0;
+            }
+            for (int kb = 0; ok && kb < p.nkb; ++kb)
+            {
+                const int ea = earow[kb];
+                const int eb = ebblk[kb];
+                const bool bad = ea == OZ_BAD_EXP || eb == OZ_BAD_EXP;
+                for (int g = 0; g < G; ++g)
+                {
+                    const int u = nu % OZ_NACC;
+                    if (!mbar_wait(&tfull[u], (nu / OZ_NACC) & 1u, abort_flag))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t taddr = tmem_base + (static_cast<uint32_t>(q * 32) << 16) +
+                                           static_cast<uint32_t>(u * 128 + h * 64);
+                    const double sc = bad ? __longlong_as_double(0x7ff8000000000000ll) : pow2(ea + eb - 12 - 7 * g);
+                    int32_t v[32];
+                    tmem_ld32_i(taddr, v);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                    {
+                        acc[j] = fma(i2d(v[j]), sc, acc[j]);
+                    }
+                    tmem_ld32_i(taddr + 32, v);
+                    tmem_ld_wait();
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0)
+                    {
+                        mbar_arrive_cluster(map_to_rank(&tempty[u], 0));
+                    }
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                    {
+                        acc[32 + j] = fma(i2d(v[j]), sc, acc[32 + j]);
+                    }
+                    ++nu;
+                }
+            }
+            if (!ok)
+            {
+                break;
+            }
+            // ---- write alpha * acc: 4 chunks of 32 rows x 16 columns per warp ----
+            double sq = 0.0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                const int col0 = n0 + h * 64 + c * 16;
+                // warp-uniform: chunk right of C, below C, or (lower) above the diagonal for all rows
+                if (col0 >= p.N || row0w >= p.M || (p.lower && col0 > row0w + 31))
+                {
+                    continue;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                {
+                    const double x = p.alpha * acc[c * 16 + 2 * j];
+                    const double y = p.alpha * acc[c * 16 + 2 * j + 1];
+                    const uint32_t addr = buf_s + static_cast<uint32_t>(lane) * 128u +
+                                          (static_cast<uint32_t>(j ^ (lane & 7)) << 4);
+                    asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(x), "d"(y) : "memory");
+                    if (p.rowsq != nullptr && rvalid)
+                    {
+                        if (col0 + 2 * j < p.N)
+                        {
+                            sq += x * x;
+                        }
+                        if (col0 + 2 * j + 1 < p.N)
+                        {
+                            sq += y * y;
+                        }
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int it = 0; it < 8; ++it)
+                {
+                    const int r = it * 4 + (lane >> 3);
+                    const int uu = lane & 7;
+                    const int grow = row0w + r;
+                    if (grow >= p.M)
+                    {
+                        continue;
+                    }
+                    double x, y;
+                    const uint32_t addr =
+                        buf_s + static_cast<uint32_t>(r) * 128u + (static_cast<uint32_t>(uu ^ (r & 7)) << 4);
+                    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "r"(addr) : "memory");
+                    const int gc = col0 + 2 * uu;
+                    double *dst = p.C + static_cast<int64_t>(grow) * p.ldc + gc;
+                    const bool ok0 = gc < p.N && (!p.lower || gc <= grow);
+                    const bool ok1 = gc + 1 < p.N && (!p.lower || gc + 1 <= grow);
+                    if (ok0 && ok1)
+                    {
+                        double2 o = make_double2(x, y);
+                        if (p.beta)
+                        {
+                            const double2 c0 = *reinterpret_cast<const double2 *>(dst);
+                            o.x += c0.x;
+                            o.y += c0.y;
+                        }
+                        *reinterpret_cast<double2 *>(dst) = o;
+                    }
+                    else
+                    {
+                        if (ok0)
+                        {
+                            dst[0] = p.beta ? dst[0] + x : x;
+                        }
+                        if (ok1)
+                        {
+                            dst[1] = p.beta ? dst[1] + y : y;
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            if (p.rowsq != nullptr && rvalid)
+            {
+                p.rowsq[h * p.rowsq_half + row] += sq;  // single writer per word and launch
+            }
+        }
+        // the CTA's last tile is written: the next kernel in the stream may
+        // start its set-up
+        pdl_launch_dependents();
+    }
+
+    tc_fence_before();
+    cluster_sync_all();  // no CTA leaves while its peer may still signal or read it
+    if (warp == 0)
+    {
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(OZ_TMEM_COLS));
+    }
+    if (threadIdx.x == 0 && *abort_flag && p.status != nullptr)
+    {
+        atomicExch(&p.status->timeout, 1);
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once,
+                   []
+                   {
+                       void *q = nullptr;
+                       cudaDriverEntryPointQueryResult r;
+                       if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &q, 12000, cudaEnableDefault,
+                                                            &r) == cudaSuccess &&
+                           r == cudaDriverEntryPointSuccess)
+                       {
+                           fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(q);
+                       }
+                   });
+    if (fn == nullptr)
+    {
+        throw Error(4, "cuTensorMapEncodeTiled is not available from the driver");
+    }
+    return fn;
+}
+
+void encode_digits(CUtensorMap *map, int8_t *base, int rows, int cols, int64_t ld, int64_t plane, int s, int box_rows)
+{
+    cuuint64_t dims[3] = { static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows), static_cast<cuuint64_t>(s) };
+    cuuint64_t strides[2] = { static_cast<cuuint64_t>(ld), static_cast<cuuint64_t>(plane) };
+    cuuint32_t box[3] = { 128u, static_cast<cuuint32_t>(box_rows), 1u };
+    cuuint32_t estrides[3] = { 1u, 1u, 1u };
+    CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estrides,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+    {
+        throw Error(4, "cuTensorMapEncodeTiled (digit planes) failed with code " + std::to_string(static_cast<int>(r)));
+    }
+}
+
+}  // namespace
+
+void oz_make_operand(OzOperand &op, int8_t *digits, int32_t *exps, int rows, int cols, int64_t ld, int64_t plane,
+                     int ldE, int s, bool block)
+{
+    if (digits == nullptr || exps == nullptr || rows <= 0 || cols <= 0 || cols % OZ_KB != 0 || ld < cols ||
+        ld % OZ_KB != 0 || plane < static_cast<int64_t>(rows) * ld || plane % 16 != 0 || ldE < cols / OZ_KB ||
+        s < OZ_MIN_SLICES || s > OZ_MAX_SLICES || (reinterpret_cast<uintptr_t>(digits) & 127))
+    {
+        throw Error(1, "oz_make_operand: invalid digit-plane layout");
+    }
+    op.digits = digits;
+    op.exps = exps;
+    op.rows = rows;
+    op.cols = cols;
+    op.ld = ld;
+    op.plane = plane;
+    op.ldE = ldE;
+    op.s = s;
+    op.block = block;
+    encode_digits(&op.map_a, digits, rows, cols, ld, plane, s, 128);
+    encode_digits(&op.map_b, digits, rows, cols, ld, plane, s, 64);
+}
+
+void oz_split(const double *src, int64_t lds, int rows, int cols, const OzOperand *row_op, const OzOperand *blk_op,
+              int dst_row0, int dst_col0, cudaStream_t s)
+{
+    if (rows <= 0 || cols <= 0)
+    {
+        return;
+    }
+    if (cols % OZ_KB != 0 || dst_col0 % OZ_KB != 0 || (lds & 1) || (reinterpret_cast<uintptr_t>(src) & 15) ||
+        (row_op == nullptr && blk_op == nullptr))
+    {
+        throw Error(1, "oz_split: cols and dst_col0 must be multiples of 128, src 16-byte aligned with an even ld");
+    }
+    const int slices = row_op != nullptr ? row_op->s : blk_op->s;
+    for (const OzOperand *op : { row_op, blk_op })
+    {
+        if (op == nullptr)
+        {
+            continue;
+        }
+        if (op->s != slices || dst_row0 < 0 || dst_row0 + rows > op->rows || dst_col0 + cols > op->cols)
+        {
+            throw Error(1, "oz_split: destination range exceeds the slice operand");
+        }
+    }
+    if (blk_op != nullptr && dst_row0 % 128 != 0)
+    {
+        throw Error(1, "oz_split: block exponents need dst_row0 to be a multiple of 128");
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ceil_div(rows, 128), cols / OZ_KB);
+    cfg.blockDim = dim3(SPLIT_THREADS);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1] = { programmatic_launch_attr() };
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    GPRAT_CUDA_CHECK(cudaLaunchKernelEx(
+        &cfg, oz_split_kernel, src, lds, rows, row_op ? row_op->digits : static_cast<int8_t *>(nullptr),
+        row_op ? row_op->ld : int64_t(0), row_op ? row_op->plane : int64_t(0),
+        row_op ? row_op->exps : static_cast<int32_t *>(nullptr), row_op ? row_op->ldE : 0,
+        blk_op ? blk_op->digits : static_cast<int8_t *>(nullptr), blk_op ? blk_op->ld : int64_t(0),
+        blk_op ? blk_op->plane : int64_t(0), blk_op ? blk_op->exps : static_cast<int32_t *>(nullptr),
+        blk_op ? blk_op->ldE : 0, dst_row0, dst_col0 / OZ_KB, slices));
+    GPRAT_LAUNCH_CHECK();
+}
+
+void oz_gemm(const OzOperand &A, const OzOperand &B, const OzGemmArgs &a, cudaStream_t s)
+{
+    if (a.M <= 0 || a.N <= 0)
+    {
+        return;
+    }
+    if (A.block || !B.block || A.s != B.s)
+    {
+        throw Error(1, "oz_gemm: A must be a row operand and B a block operand with the same slice count");
+    }
+    const int G = a.groups == 0 ? A.s : a.groups;
+    if (G < 1 || G > A.s)
+    {
+        throw Error(1, "oz_gemm: groups must be in [1, s]");
+    }
+    if (a.K <= 0 || a.K % OZ_KB != 0 || a.a_col0 % OZ_KB != 0 || a.b_col0 % OZ_KB != 0 || a.b_row0 % 128 != 0 ||
+        a.a_row0 < 0 || a.b_row0 < 0)
+    {
+        throw Error(1, "oz_gemm: K, a_col0, b_col0 and b_row0 must be multiples of 128");
+    }
+    if (a.a_row0 + a.M > A.rows || a.b_row0 + a.N > B.rows || a.a_col0 + a.K > A.cols || a.b_col0 + a.K > B.cols)
+    {
+        throw Error(1, "oz_gemm: range exceeds an operand");
+    }
+    if (a.C == nullptr || (reinterpret_cast<uintptr_t>(a.C) & 15) || (a.ldc & 1) || a.ldc < a.N)
+    {
+        throw Error(1, "oz_gemm: C must be 16-byte aligned with an even ldc >= N");
+    }
+    if (!(a.beta == 0.0 || a.beta == 1.0))
+    {
+        throw Error(1, "oz_gemm: beta must be 0 or 1");
+    }
+    if (a.lower && a.M != a.N)
+    {
+        throw Error(1, "oz_gemm: lower mode needs M == N");
+    }
+    if (a.rowsq != nullptr && (a.lower || a.beta != 0.0 || a.rowsq_half < a.M))
+    {
+        throw Error(1, "oz_gemm: rowsq needs beta = 0, no lower mode and rowsq_half >= M");
+    }
+    OzKernelArgs k{};
+    k.M = a.M;
+    k.N = a.N;
+    k.nkb = a.K / OZ_KB;
+    k.a_row0 = a.a_row0;
+    k.a_col0 = a.a_col0;
+    k.b_row0 = a.b_row0;
+    k.b_col0 = a.b_col0;
+    k.ea = A.exps;
+    k.ldea = A.ldE;
+    k.eb = B.exps;
+    k.ldeb = B.ldE;
+    k.C = a.C;
+    k.ldc = a.ldc;
+    k.alpha = a.alpha;
+    k.beta = a.beta != 0.0 ? 1 : 0;
+    k.lower = a.lower ? 1 : 0;
+    k.rowsq = a.rowsq;
+    k.rowsq_half = a.rowsq_half;
+    k.status = a.status;
+    k.groups = G;
+    k.tiles_m = ceil_div(a.M, 256);
+    k.tiles_n = ceil_div(a.N, 128);
+    if (a.lower)
+    {
+        k.ntiles = k.tiles_m * (k.tiles_m + 1) - (2 * k.tiles_m > k.tiles_n ? 1 : 0);
+    }
+    else
+    {
+        k.ntiles = k.tiles_m * k.tiles_n;
+    }
+    const int sms = device_sm_count();
+    int npairs = std::min(k.ntiles, sms / 2);
+    if (a.max_ctas > 0)
+    {
+        npairs = std::min(npairs, std::max(1, a.max_ctas / 2));
+    }
+    const bool timed = gemm_timing_enabled();
+    if (timed)
+    {
+        gemm_timing_begin(s);
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * npairs);
+    cfg.blockDim = dim3(OZ_THREADS);
+    cfg.dynamicSmemBytes = OZ_SMEM_BYTES;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    attr[1] = programmatic_launch_attr();
+    cfg.attrs = attr;
+    cfg.numAttrs = 2;
+    ensure_smem_attr(reinterpret_cast<const void *>(oz_gemm_kernel), OZ_SMEM_BYTES);
+    GPRAT_CUDA_CHECK(cudaLaunchKernelEx(&cfg, oz_gemm_kernel, A.map_a, B.map_b, k));
+    GPRAT_LAUNCH_CHECK();
+    if (timed)
+    {
+        // int8 tensor-core operations issued (the pipe this kernel is bound by)
+        const double mn = a.lower ? 0.5 * static_cast<double>(a.M) * (a.M + 1) : static_cast<double>(a.M) * a.N;
+        gemm_timing_end(s, 2.0 * mn * a.K * (G * (G + 1) / 2));
+    }
+}
+
+}  // namespace gprat_cu

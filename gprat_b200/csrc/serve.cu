@@ -451,7 +451,10 @@ void fitter_loop(gprat_cu_server *sv)
         Request *r = sv->pending_fit.front();
         // admission: a new model's resident bytes must fit next to the others
         const int64_t n = static_cast<int64_t>(r->n_tiles) * r->T;
-        const int64_t need = n * (n + 8) * 8 * (sv->precision == GPRAT_CU_PREC_FP64 ? 1 : 2);
+        // (FP64 factor; the TF32/BF16 modes add a working copy, the int8 mode two digit-plane sets of 6 bytes)
+        const int64_t need = n * (n + 8) * (sv->precision == GPRAT_CU_PREC_FP64        ? 8
+                                            : sv->precision == GPRAT_CU_PREC_FP64_INT8 ? 20
+                                                                                        : 16);
         if (sv->used + need > sv->budget)
         {
             bool inflight = false;
@@ -549,7 +552,7 @@ int gprat_cu_server_create(int device, int64_t memory_budget_bytes, int precisio
         {
             need(out != nullptr, "server pointer must not be NULL");
             need(precision == GPRAT_CU_PREC_FP64 || precision == GPRAT_CU_PREC_MIXED_TF32 ||
-                     precision == GPRAT_CU_PREC_MIXED_BF16,
+                     precision == GPRAT_CU_PREC_MIXED_BF16 || precision == GPRAT_CU_PREC_FP64_INT8,
                  "unknown precision mode");
             int count = 0;
             if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)

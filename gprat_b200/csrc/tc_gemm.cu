@@ -24,6 +24,7 @@
 // TMA copies are given time to land, the MMA issuer drains its own MMAs, the
 // TMEM is freed and the status word's timeout flag is set.
 #include "tc_gemm.cuh"
+#include "tcgen05_ptx.cuh"
 
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -35,13 +36,14 @@ namespace gprat_cu
 namespace
 {
 
+using namespace tcx;
+
 constexpr int TM = 128;
 constexpr int TN = 128;                // N of the narrow tile (row sums of squares need N <= TN)
 constexpr int TILE_BYTES = 128 * 128;  // one 128-row x 128-byte operand tile (one TMA box)
 constexpr int NUM_THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
 constexpr int EPI_WARPS = 8;
 constexpr int EPI_BUF_BYTES = 32 * 128;  // one 32 x 32 FP32 sub-tile (TMA box, 128-byte swizzle)
-constexpr unsigned long long WAIT_NS = 2000000000ull;  // bounded waits: 2 s
 
 // Tile shape: 128 x TNV (TNV = 128 or 256).  The wide tile halves the A
 // traffic per flop and lowers the shared-memory bandwidth the MMA and the
@@ -55,70 +57,6 @@ struct TileCfg
     static constexpr int EPI_COLS = TNV / 2;   // columns per epilogue warp
     static constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + EPI_WARPS * EPI_BUF_BYTES + 256;
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait for the phase with the given parity; false if it gave up
-// (or another role already aborted).
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag)
-{
-    const unsigned long long t0 = global_ns();
-    for (uint32_t i = 0;; ++i)
-    {
-        if (mbar_try_wait(bar, parity))
-        {
-            return true;
-        }
-        if (*abort_flag)
-        {
-            return false;
-        }
-        if ((i & 255u) == 255u && global_ns() - t0 > WAIT_NS)
-        {
-            *abort_flag = 1;
-            return false;
-        }
-    }
-}
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y)
 {
@@ -143,28 +81,6 @@ __device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap *map, const 
                      reinterpret_cast<uint64_t>(map)),
                  "r"(smem_u32(src)), "r"(x), "r"(y)
                  : "memory");
-}
-
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// K-major operand tile with 128-byte swizzle: rows of 128 B, 8-row groups
-// 1024 B apart (stride byte offset), descriptor version 1 (sm_100).
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr)
-{
-    uint64_t d = 0;
-    d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
-    d |= static_cast<uint64_t>(1) << 16;             // leading byte offset (unused for swizzled K-major)
-    d |= static_cast<uint64_t>(1024 >> 4) << 32;     // stride byte offset
-    d |= static_cast<uint64_t>(1) << 46;             // descriptor version
-    d |= static_cast<uint64_t>(2) << 61;             // SWIZZLE_128B
-    return d;
 }
 
 // Instruction descriptor: D = F32, A/B format (1 = BF16, 2 = TF32), both
@@ -220,7 +136,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v)
     }
 }
 
-__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Full (non-lower) tile index t -> (row tile, column tile) in groups of
 // GROUP_M row tiles: a group sweeps its columns together, so the tiles in
@@ -596,31 +511,6 @@ constexpr int PAIR_TN = 256;
 constexpr int PAIR_TMEM_COLS = 2 * PAIR_TN;
 constexpr int PAIR_SMEM_BYTES = 1024 + PAIR_STAGES * PAIR_STAGE_BYTES + EPI_WARPS * EPI_BUF_BYTES + 256;
 
-__device__ __forceinline__ uint32_t cluster_rank()
-{
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-
-// shared::cluster address of the same shared variable in CTA `rank`
-__device__ __forceinline__ uint32_t map_to_rank(const void *p, uint32_t rank)
-{
-    uint32_t out;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(smem_u32(p)), "r"(rank));
-    return out;
-}
-
-__device__ __forceinline__ void cluster_sync_all()
-{
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr)
-{
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
-}
-
 __device__ __forceinline__ void tma_load_2d_pair(void *dst, const CUtensorMap *map, uint32_t leader_bar, int x, int y)
 {
     asm volatile(
@@ -648,22 +538,6 @@ __device__ __forceinline__ void mma_issue_pair(uint32_t tmem_d, uint64_t adesc, 
             "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
             "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
     }
-}
-
-// arrives on the barrier at the same offset in both CTAs of the pair
-__device__ __forceinline__ void mma_commit_pair_both(uint64_t *bar)
-{
-    asm volatile(
-        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
-            smem_u32(bar)),
-        "h"(static_cast<uint16_t>(3))
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_commit_pair_local(uint64_t *bar)
-{
-    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
 }
 
 // pair tile t -> (m0, n0) in units of 256 (lower: square tiles at or below the diagonal)

@@ -1,7 +1,10 @@
 // Kernel-level test entry points of the C ABI (gprat_cu_test_*): run one
-// kernel on host-provided data so that tests can compare it in isolation.
+// kernel on host-provided data so that tests can compare it in isolation
+// (tcgen05 TF32/BF16 GEMM, fused triangular solves, the int8 digit split and
+// the int8-emulated FP64 GEMM).
 #include "common.cuh"
 #include "gprat_cu.h"
+#include "ozaki.cuh"
 #include "tc_gemm.cuh"
 
 #include <algorithm>
@@ -234,6 +237,141 @@ extern "C" int gprat_cu_test_trsv(int kind, int n, const double *L, const double
         if (hst.timeout != 0)
         {
             throw Error(GPRAT_CU_ERR_TIMEOUT, "triangular solve: a bounded wait timed out");
+        }
+        set_last_error("");
+        return GPRAT_CU_OK;
+    }
+    catch (const Error &e)
+    {
+        set_last_error(e.what());
+        return e.code;
+    }
+    catch (const std::exception &e)
+    {
+        set_last_error(e.what());
+        return GPRAT_CU_ERR_INVALID_ARG;
+    }
+}
+
+namespace
+{
+
+// Digit planes + exponents of one slice operand on the device.
+struct OzBuf
+{
+    Buf dig, exps;
+    OzOperand op;
+    OzBuf(int rows, int cols, int s, bool block)
+        : dig(static_cast<size_t>(s) * round_up(rows, 128) * cols + 128),
+          exps(static_cast<size_t>(block ? ceil_div(rows, 128) : rows) * (cols / OZ_KB) * sizeof(int32_t) + 16)
+    {
+        const int64_t plane = static_cast<int64_t>(round_up(rows, 128)) * cols;
+        oz_make_operand(op, static_cast<int8_t *>(dig.p), static_cast<int32_t *>(exps.p), rows, cols, cols, plane,
+                        cols / OZ_KB, s, block);
+    }
+};
+
+}  // namespace
+
+extern "C" int gprat_cu_test_oz_split(int rows, int cols, const double *src, int s, int block, int8_t *digits,
+                                      int32_t *exps)
+{
+    try
+    {
+        if (src == nullptr || digits == nullptr || exps == nullptr || rows <= 0 || cols <= 0 || cols % OZ_KB != 0 ||
+            s < OZ_MIN_SLICES || s > OZ_MAX_SLICES)
+        {
+            throw Error(GPRAT_CU_ERR_INVALID_ARG, "gprat_cu_test_oz_split: invalid arguments");
+        }
+        Buf dsrc(static_cast<size_t>(rows) * cols * sizeof(double));
+        GPRAT_CUDA_CHECK(cudaMemcpy(dsrc.p, src, static_cast<size_t>(rows) * cols * sizeof(double),
+                                    cudaMemcpyHostToDevice));
+        OzBuf o(rows, cols, s, block != 0);
+        cudaStream_t st = nullptr;
+        oz_split(static_cast<const double *>(dsrc.p), cols, rows, cols, block ? nullptr : &o.op,
+                 block ? &o.op : nullptr, 0, 0, st);
+        GPRAT_CUDA_CHECK(cudaStreamSynchronize(st));
+        for (int p = 0; p < s; ++p)
+        {
+            GPRAT_CUDA_CHECK(cudaMemcpy(digits + static_cast<size_t>(p) * rows * cols,
+                                        static_cast<int8_t *>(o.dig.p) + p * o.op.plane,
+                                        static_cast<size_t>(rows) * cols, cudaMemcpyDeviceToHost));
+        }
+        const size_t ne = static_cast<size_t>(block ? ceil_div(rows, 128) : rows) * (cols / OZ_KB);
+        GPRAT_CUDA_CHECK(cudaMemcpy(exps, o.exps.p, ne * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        set_last_error("");
+        return GPRAT_CU_OK;
+    }
+    catch (const Error &e)
+    {
+        set_last_error(e.what());
+        return e.code;
+    }
+    catch (const std::exception &e)
+    {
+        set_last_error(e.what());
+        return GPRAT_CU_ERR_INVALID_ARG;
+    }
+}
+
+extern "C" int gprat_cu_test_oz_gemm(int M, int N, int K, const double *A, const double *B, double *C, double alpha,
+                                     double beta, int lower, int s, int groups, double *rowsq, int max_ctas)
+{
+    try
+    {
+        if (A == nullptr || B == nullptr || C == nullptr || M <= 0 || N <= 0 || K <= 0 || K % OZ_KB != 0 ||
+            s < OZ_MIN_SLICES || s > OZ_MAX_SLICES || groups < 0 || groups > s || max_ctas < 0)
+        {
+            throw Error(GPRAT_CU_ERR_INVALID_ARG, "gprat_cu_test_oz_gemm: invalid arguments");
+        }
+        cudaStream_t st = nullptr;
+        const int64_t lc = round_up(N, 2);
+        Buf dA(static_cast<size_t>(M) * K * 8), dB(static_cast<size_t>(N) * K * 8), dC(static_cast<size_t>(M) * lc * 8);
+        GPRAT_CUDA_CHECK(cudaMemcpy(dA.p, A, static_cast<size_t>(M) * K * 8, cudaMemcpyHostToDevice));
+        GPRAT_CUDA_CHECK(cudaMemcpy(dB.p, B, static_cast<size_t>(N) * K * 8, cudaMemcpyHostToDevice));
+        GPRAT_CUDA_CHECK(cudaMemcpy2D(dC.p, lc * 8, C, N * 8, N * 8, M, cudaMemcpyHostToDevice));
+        OzBuf oa(M, K, s, false), ob(N, K, s, true);
+        oz_split(static_cast<const double *>(dA.p), K, M, K, &oa.op, nullptr, 0, 0, st);
+        oz_split(static_cast<const double *>(dB.p), K, N, K, nullptr, &ob.op, 0, 0, st);
+        Buf dStatus(sizeof(DeviceStatus));
+        GPRAT_CUDA_CHECK(cudaMemset(dStatus.p, 0, sizeof(DeviceStatus)));
+        Buf dRow(2 * static_cast<size_t>(M) * sizeof(double));
+        if (rowsq != nullptr)
+        {
+            GPRAT_CUDA_CHECK(cudaMemset(dRow.p, 0, 2 * static_cast<size_t>(M) * sizeof(double)));
+            GPRAT_CUDA_CHECK(cudaMemcpy(dRow.p, rowsq, M * sizeof(double), cudaMemcpyHostToDevice));
+        }
+        OzGemmArgs g{};
+        g.M = M;
+        g.N = N;
+        g.K = K;
+        g.C = static_cast<double *>(dC.p);
+        g.ldc = lc;
+        g.alpha = alpha;
+        g.beta = beta;
+        g.lower = lower != 0;
+        g.rowsq = rowsq != nullptr ? static_cast<double *>(dRow.p) : nullptr;
+        g.rowsq_half = M;
+        g.status = static_cast<DeviceStatus *>(dStatus.p);
+        g.max_ctas = max_ctas;
+        g.groups = groups;
+        oz_gemm(oa.op, ob.op, g, st);
+        GPRAT_CUDA_CHECK(cudaStreamSynchronize(st));
+        DeviceStatus hs{};
+        GPRAT_CUDA_CHECK(cudaMemcpy(&hs, dStatus.p, sizeof(hs), cudaMemcpyDeviceToHost));
+        if (hs.timeout != 0)
+        {
+            throw Error(GPRAT_CU_ERR_TIMEOUT, "int8 GEMM: a bounded wait timed out");
+        }
+        GPRAT_CUDA_CHECK(cudaMemcpy2D(C, N * 8, dC.p, lc * 8, N * 8, M, cudaMemcpyDeviceToHost));
+        if (rowsq != nullptr)
+        {
+            std::vector<double> halves(2 * static_cast<size_t>(M));
+            GPRAT_CUDA_CHECK(cudaMemcpy(halves.data(), dRow.p, halves.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int i = 0; i < M; ++i)
+            {
+                rowsq[i] = halves[i] + halves[M + i];
+            }
         }
         set_last_error("");
         return GPRAT_CU_OK;

@@ -50,6 +50,10 @@ extern "C" {
 #define GPRAT_CU_PREC_FP64 0       /* all FP64 (DMMA tensor cores) */
 #define GPRAT_CU_PREC_MIXED_TF32 1 /* FP32 storage, TF32 tcgen05 trailing updates, FP64 diagonal */
 #define GPRAT_CU_PREC_MIXED_BF16 2 /* FP32 storage, BF16 tcgen05 trailing updates, FP64 diagonal */
+/* FP64 storage; every product of the factorisation and of the variance solve
+ * emulated on the int8 tensor cores (Ozaki scheme, s digit planes, see
+ * gprat_cu_gp_set_int8_slices); FP64 diagonal blocks and alpha solves. */
+#define GPRAT_CU_PREC_FP64_INT8 3
 
 typedef struct gprat_cu_gp gprat_cu_gp;
 
@@ -80,8 +84,19 @@ int gprat_cu_gp_create(int device,
 
 int gprat_cu_gp_destroy(gprat_cu_gp *gp);
 
-/* Selects GPRAT_CU_PREC_* for subsequent calls (default FP64). */
+/* Selects GPRAT_CU_PREC_* for subsequent calls (default FP64).  The
+ * tensor-core modes (TF32, BF16, FP64_INT8) need n_tiles * n_tile_size to be
+ * a multiple of 128. */
 int gprat_cu_gp_set_precision(gprat_cu_gp *gp, int precision);
+
+/*
+ * Digit planes of the int8-emulated FP64 products (GPRAT_CU_PREC_FP64_INT8),
+ * 3 <= slices <= 8, default 6.  Each operand keeps 6 + 7 (slices - 1) bits
+ * relative to the largest entry of its 128-column block; a product costs
+ * slices * (slices + 1) / 2 int8 tensor-core passes.  No counterpart in the
+ * reference (whose GPU path is FP64 cuBLAS/cuSOLVER only).
+ */
+int gprat_cu_gp_set_int8_slices(gprat_cu_gp *gp, int slices);
 
 /*
  * Tiled Cholesky factor (gprat::GP::cholesky, core/src/gprat_c.cpp:336-361;
@@ -290,6 +305,42 @@ int gprat_cu_test_tc_gemm(int kind,
  * from b.  max_ctas > 0 bounds the grid.
  */
 int gprat_cu_test_trsv(int kind, int n, const double *L, const double *b, double *x_fwd, double *x_bwd, int max_ctas);
+
+/*
+ * Kernel-level test entry (no counterpart in the reference): splits the
+ * host matrix src (rows x cols, row-major FP64, cols a multiple of 128) into
+ * s int8 digit planes on the current device, as the int8-emulated FP64
+ * products do:  src[r][c] ~= 2^(e - 6) * sum_{p<s} D_p[r][c] * 2^(-7 p),
+ * one exponent e per row and 128-column block (block = 0) or per 128 x 128
+ * block (block != 0).  digits: s * rows * cols bytes (plane-major);
+ * exps: rows * (cols / 128) (or ceil(rows / 128) * (cols / 128)) ints.
+ * 3 <= s <= 8.
+ */
+int gprat_cu_test_oz_split(int rows, int cols, const double *src, int s, int block, int8_t *digits, int32_t *exps);
+
+/*
+ * Kernel-level test entry (no counterpart in the reference): the FP64 GEMM
+ * emulated on the int8 tensor cores (tcgen05.mma kind::i8, Ozaki scheme),
+ * C = beta * C + alpha * A B^T with host buffers A (M x K), B (N x K),
+ * C (M x N; read when beta = 1), all row-major FP64 with K a multiple of 128.
+ * A is split with row exponents, B with block exponents, into s digit
+ * planes; groups (0 = s) digit groups are kept.  lower != 0: M == N and only
+ * C[i][j], i >= j, is written.  rowsq (optional, beta = 0):
+ * rowsq[i] += sum_j C_new[i][j]^2.  max_ctas > 0 bounds the grid.
+ */
+int gprat_cu_test_oz_gemm(int M,
+                          int N,
+                          int K,
+                          const double *A,
+                          const double *B,
+                          double *C,
+                          double alpha,
+                          double beta,
+                          int lower,
+                          int s,
+                          int groups,
+                          double *rowsq,
+                          int max_ctas);
 
 /*
  * Serving (no counterpart in the reference, whose every predict call

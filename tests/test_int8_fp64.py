@@ -1,0 +1,124 @@
+"""The FP64-accurate pipeline on the int8 tensor cores (PREC_FP64_INT8: every
+product of the factorisation and of the variance solve emulated with int8
+digit planes, Ozaki scheme) against the FP64 numpy oracle.
+
+Bar (the mixed-precision target of this path): predictive mean and variance
+within 1e-8 relative of the FP64 oracle, per test point; the NLML within
+1e-10.  Cases: the d=8 and the d=64 hyper-parameters of the benchmark
+configurations at n = 2048 and 4096, with 6 digit planes (and 5 for d=64,
+the slice count the n=32768 benchmark uses).
+"""
+import numpy as np
+import pytest
+
+from oracle import gprat_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MEAN_TOL = 1e-8
+VAR_TOL = 1e-8
+LOSS_TOL = 1e-10
+
+CASES = {
+    # name: n, m, d, T, hyper
+    "d8_n2048": (2048, 2048, 8, 256, (1.0, 1.0, 0.1)),
+    "d8_n4096": (4096, 2048, 8, 512, (1.0, 1.0, 0.1)),
+    "d64_n2048": (2048, 512, 64, 256, (4.0, 1.0, 0.01)),
+    "d64_n4096": (4096, 2048, 64, 512, (4.0, 1.0, 0.01)),
+}
+
+
+@pytest.fixture(scope="module")
+def capi():
+    from gprat_b200 import capi as c
+
+    assert c.device_count() >= 1
+    return c
+
+
+_cache = {}
+
+
+def problem(name):
+    if name not in _cache:
+        n, m, d, T, h = CASES[name]
+        x, y, xt = O.synthetic(n, m, d)
+        o = O.OracleGP(x, y, n // T, T, d, h)
+        om, ov = o.predict_with_uncertainty(xt, 1, m)
+        _cache[name] = dict(n=n, m=m, d=d, T=T, h=h, x=x, y=y, xt=xt, om=om, ov=ov, loss=o.calculate_loss())
+    return _cache[name]
+
+
+@pytest.mark.parametrize("name,slices", [("d8_n2048", 6), ("d8_n4096", 6), ("d64_n2048", 6), ("d64_n4096", 6),
+                                         ("d64_n4096", 5)])
+def test_predict_with_uncertainty(capi, name, slices):
+    p = problem(name)
+    gp = capi.CudaGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"])
+    gp.set_precision(capi.PREC_FP64_INT8)
+    gp.set_int8_slices(slices)
+    mean, var = gp.predict_with_uncertainty(p["h"], p["xt"], 1, p["m"])
+    mean_err = np.max(np.abs(mean - p["om"])) / np.max(np.abs(p["om"]))
+    var_err = np.max(np.abs(var - p["ov"]) / p["ov"])
+    loss = gp.compute_loss(p["h"])
+    loss_err = abs(loss - p["loss"]) / abs(p["loss"])
+    print(f"{name} s={slices}: mean {mean_err:.2e} var {var_err:.2e} loss {loss_err:.2e}")
+    assert mean_err <= MEAN_TOL
+    assert var_err <= VAR_TOL
+    assert loss_err <= LOSS_TOL
+    gp.close()
+
+
+def test_other_entry_points(capi):
+    """predict (mean only), predict_with_full_cov, a small test set (the
+    panel-ordered variance solve) and the device-resident entry point, which
+    runs the same overlapped schedule as predict_with_uncertainty."""
+    import torch
+
+    p = problem("d8_n2048")
+    gp = capi.CudaGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"])
+    gp.set_precision(capi.PREC_FP64_INT8)
+    mean = gp.predict(p["h"], p["xt"], 1, p["m"])
+    assert np.max(np.abs(mean - p["om"])) / np.max(np.abs(p["om"])) <= MEAN_TOL
+    fm, fv = gp.predict_with_full_cov(p["h"], p["xt"], 1, p["m"])
+    assert np.max(np.abs(fv - p["ov"]) / p["ov"]) <= VAR_TOL
+    m_small = 300
+    sm, sv = gp.predict_with_uncertainty(p["h"], p["xt"][:m_small + p["d"] - 1], 1, m_small)
+    assert np.max(np.abs(sv - p["ov"][:m_small]) / p["ov"][:m_small]) <= VAR_TOL
+    assert np.max(np.abs(sm - p["om"][:m_small])) / np.max(np.abs(p["om"])) <= MEAN_TOL
+    hm, hv = gp.predict_with_uncertainty(p["h"], p["xt"], 1, p["m"])
+    dev = torch.device("cuda", 0)
+    dxt = torch.tensor(p["xt"], device=dev)
+    dm = torch.empty(p["m"], dtype=torch.float64, device=dev)
+    dv = torch.empty(p["m"], dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    gp.fit_predict_device(p["h"], dxt.data_ptr(), dxt.numel(), p["m"], dm.data_ptr(), dv.data_ptr(),
+                          stream.cuda_stream)
+    torch.cuda.synchronize()
+    gp.check_status()
+    # the same pipeline, deterministic: identical results through both entry points
+    assert np.array_equal(dm.cpu().numpy(), hm)
+    assert np.array_equal(dv.cpu().numpy(), hv)
+    gp.close()
+
+
+def test_not_positive_definite(capi):
+    """A covariance that is not positive definite (negative noise) raises, and
+    the handle then works again."""
+    p = problem("d8_n2048")
+    gp = capi.CudaGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"])
+    gp.set_precision(capi.PREC_FP64_INT8)
+    with pytest.raises(capi.NotPositiveDefiniteError):
+        gp.predict_with_uncertainty((1.0, 1.0, -5.0), p["xt"], 1, 256)
+    mean, var = gp.predict_with_uncertainty(p["h"], p["xt"], 1, p["m"])
+    assert np.max(np.abs(var - p["ov"]) / p["ov"]) <= VAR_TOL
+    gp.close()
+
+
+def test_slices_rejected(capi):
+    p = problem("d8_n2048")
+    gp = capi.CudaGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"])
+    with pytest.raises(capi.GpratCudaError):
+        gp.set_int8_slices(2)
+    with pytest.raises(capi.GpratCudaError):
+        gp.set_int8_slices(9)
+    gp.close()

@@ -1,0 +1,168 @@
+"""Int8-emulated FP64 products (Ozaki scheme): the device digit split and the
+tcgen05 kind::i8 GEMM against a numpy restatement of the same scheme.
+
+Every int32 group product is exact and the kernel accumulates the groups in
+FP64 in a fixed order (128-column block, then digit group), so the numpy
+restatement below reproduces the kernel's result bit for bit; a second check
+bounds the distance to the plain FP64 product by the truncation error of s
+digits.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+KB = 128
+
+
+def np_exponents(X, block):
+    """One exponent e per row (or 128-row block) and 128-column block with
+    max|x| < 2^e (frexp's exponent); all-zero domains get -2000."""
+    R, C = X.shape
+    m = np.abs(X).reshape(R, C // KB, KB).max(axis=2)
+    if block:
+        rb = (R + 127) // 128
+        mp = np.zeros((rb * 128, C // KB))
+        mp[:R] = m
+        m = mp.reshape(rb, 128, C // KB).max(axis=1)
+    e = np.frexp(m)[1].astype(np.int64)
+    return np.where(m > 0, e, -2000)
+
+
+def np_split(X, s, block):
+    R, C = X.shape
+    E = np_exponents(X, block)
+    Er = np.repeat(E, 128, axis=0)[:R] if block else E
+    Ee = np.repeat(Er, KB, axis=1)
+    t = X * np.ldexp(1.0, (6 - Ee).clip(-1022, 1023))
+    t[Ee == -2000] = 0.0
+    D = []
+    for _ in range(s):
+        d = np.rint(t)
+        D.append(d)
+        t = (t - d) * 128.0
+    return np.array(D), E
+
+
+def np_oz_gemm(A, B, C, alpha, beta, s, groups=0, lower=False):
+    """The kernel's arithmetic: per 128-column block k and group g an exact
+    integer product, scaled by 2^(eA + eB - 12 - 7g) and added in FP64."""
+    G = groups or s
+    DA, EA = np_split(A, s, False)
+    DB, EB = np_split(B, s, True)
+    M, N = A.shape[0], B.shape[0]
+    acc = np.zeros((M, N))
+    ebcol = np.repeat(EB, 128, axis=0)[:N]  # per B row (= C column), per block
+    for k in range(A.shape[1] // KB):
+        sl = slice(k * KB, (k + 1) * KB)
+        for g in range(G):
+            P = np.zeros((M, N))
+            for p in range(g + 1):
+                P += DA[p][:, sl] @ DB[g - p][:, sl].T
+            e = EA[:, k][:, None] + ebcol[:, k][None, :] - 12 - 7 * g
+            acc += P * np.ldexp(1.0, e.clip(-1022, 1023))
+    out = alpha * acc
+    if beta != 0.0:
+        out = C + out
+    if lower:
+        keep = np.tril(np.ones((M, N), dtype=bool))
+        out = np.where(keep, out, C)
+    return out
+
+
+@pytest.fixture(scope="module")
+def capi():
+    from gprat_b200 import capi as c
+
+    return c
+
+
+def graded(rng, rows, cols):
+    """Rows of widely different magnitudes (the per-row exponents matter)."""
+    X = rng.standard_normal((rows, cols))
+    X *= np.exp2(rng.integers(-20, 4, size=(rows, 1)))
+    X[:, :KB] *= np.exp2(rng.integers(-6, 6, size=(rows, 1)))  # the first column block differs
+    return X
+
+
+@pytest.mark.parametrize("block", [False, True])
+@pytest.mark.parametrize("s", [3, 6, 8])
+def test_split_matches_numpy(capi, block, s):
+    rng = np.random.default_rng(11)
+    X = graded(rng, 300, 256)
+    X[7] = 0.0            # an all-zero row
+    X[200:210, KB:] = 0.0  # zero in one column block only
+    D, E = capi.test_oz_split(X, s, block)
+    Dn, En = np_split(X, s, block)
+    assert np.array_equal(E, En)
+    assert np.array_equal(D.astype(np.float64), Dn)
+    assert np.abs(D).max() <= 64
+    # reconstruction: error below half a unit of the last digit
+    Er = np.repeat(En, 128, axis=0)[:300] if block else En
+    Ee = np.repeat(Er, KB, axis=1)
+    rec = sum(Dn[p] * np.ldexp(1.0, -7 * p) for p in range(s)) * np.ldexp(1.0, (Ee - 6).clip(-1022, 1023))
+    rec[Ee == -2000] = 0.0
+    bound = np.ldexp(1.0, Ee - 6 - 7 * (s - 1) - 1)
+    assert np.all(np.abs(rec - X) <= bound)
+
+
+@pytest.mark.parametrize("M,N,K,beta,lower,s,groups,max_ctas", [
+    (300, 200, 384, 0.0, False, 6, 0, 0),
+    (300, 200, 384, 1.0, False, 5, 0, 0),
+    (384, 384, 256, 1.0, True, 6, 0, 0),
+    (640, 640, 128, 1.0, True, 4, 0, 0),
+    (1024, 1024, 1024, 1.0, False, 6, 0, 8),   # persistent: 4 pairs loop over 32 tiles
+    (512, 128, 256, 0.0, False, 7, 5, 0),      # fewer groups than digits
+    (128, 72, 128, 0.0, False, 8, 0, 0),       # ragged N, a single pair tile
+])
+def test_gemm_bit_exact(capi, M, N, K, beta, lower, s, groups, max_ctas):
+    rng = np.random.default_rng(M + N + K + s)
+    A = graded(rng, M, K)
+    B = graded(rng, N, K)
+    C = rng.standard_normal((M, N))
+    if lower:
+        B = A.copy()
+    out = C.copy()
+    capi.test_oz_gemm(A, B, out, -1.0, beta, s, groups, lower, max_ctas=max_ctas)
+    ref = np_oz_gemm(A, B, C, -1.0, beta, s, groups, lower)
+    assert np.array_equal(out, ref), f"max |diff| {np.max(np.abs(out - ref)):.3e}"
+    # distance to the plain FP64 product: truncation of s digits, relative to |A| |B|^T
+    exact = (C if beta else 0.0) - A @ B.T
+    if lower:
+        exact = np.where(np.tril(np.ones((M, N), dtype=bool)), exact, C)
+    scale = np.abs(A).max(axis=1)[:, None] * np.abs(B).max(axis=1)[None, :] * K
+    G = groups or s
+    assert np.all(np.abs(out - exact) <= scale * 2.0 ** (-(7 * G - 9)) + 1e-300)
+
+
+def test_gemm_rowsq(capi):
+    rng = np.random.default_rng(5)
+    M, N, K = 700, 128, 256
+    A, B = graded(rng, M, K), graded(rng, N, K)
+    C = np.zeros((M, N))
+    rs = rng.standard_normal(M) ** 2
+    rs0 = rs.copy()
+    capi.test_oz_gemm(A, B, C, 1.0, 0.0, 6, rowsq=rs)
+    ref = np_oz_gemm(A, B, np.zeros((M, N)), 1.0, 0.0, 6)
+    assert np.array_equal(C, ref)
+    np.testing.assert_allclose(rs, rs0 + np.sum(ref * ref, axis=1), rtol=1e-14)
+
+
+def test_gemm_nan_propagates(capi):
+    rng = np.random.default_rng(6)
+    A, B = rng.standard_normal((256, 256)), rng.standard_normal((128, 256))
+    A[3, 200] = np.nan
+    C = np.zeros((256, 128))
+    capi.test_oz_gemm(A, B, C, 1.0, 0.0, 5)
+    assert np.all(np.isnan(C[3]))
+    assert np.all(np.isfinite(np.delete(C, 3, axis=0)))
+
+
+def test_gemm_rejects_bad_shapes(capi):
+    A = np.zeros((128, 100))
+    B = np.zeros((128, 100))
+    C = np.zeros((128, 128))
+    with pytest.raises(capi.GpratCudaError):
+        capi.test_oz_gemm(A, B, C, 1.0, 0.0, 6)  # K not a multiple of 128
+    with pytest.raises(capi.GpratCudaError):
+        capi.test_oz_gemm(np.zeros((128, 128)), np.zeros((128, 128)), C, 1.0, 0.0, 9)  # too many digits
