@@ -158,12 +158,13 @@ void factor_oz(gprat_cu_gp *gp, cudaStream_t s, const std::vector<std::pair<int,
             }
             double *linv = gp->Linv.ptr + static_cast<int64_t>(k) * NB * NB;
             potrf_diag(kat(gp, r0, r0), ld, NB, r0, linv, NB, st, side);
+            // every block's inverse, the last one included: the variance solve's last leaf uses it
+            oz_split(linv, NB, NB, NB, nullptr, &ops.INV, k * NB, 0, side);
             const int rows = n - r0 - NB;
             if (rows <= 0)
             {
                 continue;
             }
-            oz_split(linv, NB, NB, NB, nullptr, &ops.INV, k * NB, 0, side);
             oz_split(kat(gp, r0 + NB, r0), ld, rows, NB, &ops.P, nullptr, 0, 0, side);
             oz_gemm(ops.P, ops.INV,
                     oz_args(rows, NB, NB, 0, 0, k * NB, 0, kat(gp, r0 + NB, r0), ld, 1.0, 0.0, false, st), side);

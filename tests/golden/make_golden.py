@@ -1,7 +1,9 @@
 """Generates the golden fixtures under tests/golden/ (run in a container that
-has the reference tree and the compiled reference, oracle/_ref):
+has the reference tree and the compiled reference, oracle/_ref).  The
+reference tree is $GPRAT_REFERENCE, else the directory `reference` beside
+this repository:
 
-    make -C oracle REF=/root/reference && python tests/golden/make_golden.py
+    make -C oracle && python tests/golden/make_golden.py
 
 1. data_1024_n128.json: the reference's own known-answer test
    (test/src/output_correctness.cpp:60-247): the first 128 values of
@@ -16,6 +18,12 @@ has the reference tree and the compiled reference, oracle/_ref):
    initial (lengthscale, vertical_lengthscale, noise) = (0.5, 2.0, 0.5),
    50 Adam steps at lr = 0.1: the reference's loss and parameters after every
    step and its gradient at steps 0, 10, 20, 30, 40.
+4. ref_large.npz (`--large`, tens of minutes on 8 cores): the benchmark
+   configurations at full size, C1 = n_train 16384, n_test 4096, d 8,
+   32 x 32 tiles of 512, (1.0, 1.0, 0.1) and C2 = n_train 32768, n_test 8192,
+   d 64, 32 x 32 tiles of 1024, (4.0, 1.0, 0.01): predict_with_uncertainty's
+   mean and variance, calculate_loss, and of cholesky() the sum and the sum
+   of squares of every tile plus three 32 x 32 corners.
 """
 from __future__ import annotations
 
@@ -32,7 +40,7 @@ sys.path.insert(0, ROOT)
 from oracle import gprat_oracle as O  # noqa: E402
 from oracle import ref  # noqa: E402
 
-REF = os.environ.get("GPRAT_REFERENCE", "/root/reference")
+REF = os.environ.get("GPRAT_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
 
 
 def known_answer():
@@ -109,10 +117,57 @@ def case_c3():
                         losses=np.array(losses), params=np.array(params), grads=np.array(grads))
 
 
+LARGE = {
+    # tag: n, m, d, T, hyper
+    "c1": (16384, 4096, 8, 512, (1.0, 1.0, 0.1)),
+    "c2": (32768, 8192, 64, 1024, (4.0, 1.0, 0.01)),
+}
+
+
+def case_large(tag, store):
+    import time
+
+    n, m, d, T, hyper = LARGE[tag]
+    x, y, xt = O.synthetic(n, m, d)
+    nt = n // T
+    mt, mts = ref.compute_test_tiles(m, nt, T)
+    gp = ref.RefGP(x, y, nt, T, d, hyper)
+    t0 = time.time()
+    mean, var = gp.predict_with_uncertainty(xt, mt, mts)
+    t1 = time.time()
+    loss = gp.calculate_loss()
+    t2 = time.time()
+    tiles = gp.cholesky()
+    t3 = time.time()
+    print(f"{tag}: predict_with_uncertainty {t1 - t0:.1f} s, calculate_loss {t2 - t1:.1f} s, cholesky {t3 - t2:.1f} s",
+          flush=True)
+    sums = np.array([t.sum() if t is not None else 0.0 for t in tiles])
+    sumsq = np.array([np.dot(t, t) if t is not None else 0.0 for t in tiles])
+    last = tiles[nt * nt - 1].reshape(T, T)
+    store.update({
+        f"{tag}_cfg": np.array([n, m, d, T, mt, mts], dtype=np.int64),
+        f"{tag}_hyper": np.array(hyper),
+        f"{tag}_mean": mean, f"{tag}_var": var, f"{tag}_loss": np.array([loss]),
+        f"{tag}_tile_sum": sums, f"{tag}_tile_sumsq": sumsq,
+        f"{tag}_corner_00": tiles[0].reshape(T, T)[:32, :32].copy(),
+        f"{tag}_corner_last": last[-32:, -32:].copy(),
+        f"{tag}_corner_low": tiles[(nt - 1) * nt].reshape(T, T)[:32, :32].copy(),
+        f"{tag}_seconds": np.array([t1 - t0, t2 - t1, t3 - t2]),
+    })
+    del tiles
+
+
 def main():
     ref.start()
     if "--c3" in sys.argv:
         case_c3()
+        return
+    if "--large" in sys.argv:
+        path = os.path.join(HERE, "ref_large.npz")
+        store = dict(np.load(path)) if os.path.exists(path) else {}
+        for tag in [a for a in sys.argv[sys.argv.index("--large") + 1:] if a in LARGE] or list(LARGE):
+            case_large(tag, store)
+            np.savez_compressed(path, **store)
         return
     known_answer()
     store = {}

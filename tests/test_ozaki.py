@@ -130,7 +130,10 @@ def test_gemm_bit_exact(capi, M, N, K, beta, lower, s, groups, max_ctas):
     exact = (C if beta else 0.0) - A @ B.T
     if lower:
         exact = np.where(np.tril(np.ones((M, N), dtype=bool)), exact, C)
-    scale = np.abs(A).max(axis=1)[:, None] * np.abs(B).max(axis=1)[None, :] * K
+    # A has row exponents, B block exponents (the maximum over each 128-row block of B)
+    bmax = np.abs(B).max(axis=1)
+    bblk = np.array([bmax[(j // 128) * 128:(j // 128 + 1) * 128].max() for j in range(N)])
+    scale = np.abs(A).max(axis=1)[:, None] * bblk[None, :] * K
     G = groups or s
     assert np.all(np.abs(out - exact) <= scale * 2.0 ** (-(7 * G - 9)) + 1e-300)
 
