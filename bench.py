@@ -44,8 +44,8 @@ WORKLOADS = {
     "c1": dict(n=16384, m=4096, d=8, T=512, hyper=(1.0, 1.0, 0.1)),
 }
 
-# Bounded CPU sample of the same workload: same d, hyper-parameters and
-# n_test/n_train ratio; time scales with n^3 (n^3/3 Cholesky + n^2 m solve).
+# Per-call CPU and GPU timings of the API calls (cholesky, predict,
+# calculate_loss, optimize_step) are taken at this smaller training size.
 CPU_SAMPLE_N = 8192
 
 
@@ -233,31 +233,52 @@ def measure_fp64_gemm_peak(torch, device) -> float:
     return best
 
 
-def cpu_reference_sample(wl, reps: int):
-    """The reference's own CPU path (compiled from source, oracle/_ref) on a
-    bounded sample: n=8192 with the workload's d, hyper-parameters and
-    n_test/n_train ratio.  Returns (seconds per rep, scale factor to the
-    full workload, description, threads)."""
+def measure_int8_peak(torch, device) -> float:
+    """cuBLASLt int8 GEMM throughput (torch._int_mm, int8 x int8 -> int32,
+    8192^3, best of 5), tera-ops/s."""
+    a = torch.randint(-64, 64, (8192, 8192), dtype=torch.int8, device=device)
+    b = torch.randint(-64, 64, (8192, 8192), dtype=torch.int8, device=device)
+    torch._int_mm(a, b)
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch._int_mm(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (s.elapsed_time(e) / 1e3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def cpu_reference_full(wl, reps: int):
+    """The reference's own CPU path (compiled from source, oracle/_ref) at the
+    FULL workload on all host cores: `reps` timed predict_with_uncertainty
+    calls (assembly + Cholesky + alpha solves + mean + variance), after one
+    small untimed call that starts the task pool and pages the libraries in.
+    Returns (seconds of each rep, description, threads)."""
     from oracle import ref
 
-    n, d = CPU_SAMPLE_N, wl["d"]
-    m = wl["m"] * n // wl["n"]
-    T = 512
+    n, m, d, T = wl["n"], wl["m"], wl["d"], wl["T"]
     threads = os.cpu_count() or 1
     ref.start(threads)
+    xw, yw, xtw = synthetic(1024, 256, d)
+    ref.RefGP(xw, yw, 8, 128, d, wl["hyper"]).predict_with_uncertainty(xtw, 2, 128)
     x, y, xt = synthetic(n, m, d)
-    gp = ref.RefGP(x, y, n // T, T, d, wl["hyper"])
+    nt = n // T
+    mt, mts = ref.compute_test_tiles(m, nt, T)
+    gp = ref.RefGP(x, y, nt, T, d, wl["hyper"])
     times = []
     for _ in range(reps):
         t0 = time.perf_counter()
-        gp.predict_with_uncertainty(xt, m // T, T)
+        gp.predict_with_uncertainty(xt, mt, mts)
         times.append(time.perf_counter() - t0)
-    scale = algorithmic_flops(wl["n"], wl["m"]) / algorithmic_flops(n, m)
-    desc = (f"reference CPU predict_with_uncertainty (assembly+Cholesky+solves+mean+var), n_train={n}, "
-            f"n_test={m}, d={d}, {n // T}x{n // T} tiles of {T}; median of {reps}; scaled x{scale:.0f} by "
-            f"algorithmic flops to n_train={wl['n']}, n_test={wl['m']}; HPX replaced by std::thread shim, "
-            f"OpenBLAS 0.3.30 single-threaded per task")
-    return statistics.median(times), scale, desc, threads
+    desc = (f"reference CPU predict_with_uncertainty (assembly+Cholesky+solves+mean+var) at the full workload "
+            f"n_train={n}, n_test={m}, d={d}, {nt}x{nt} tiles of {T}; {reps} timed call(s) after one small "
+            f"untimed warm-up call (n_train=1024); HPX replaced by a std::thread shim, OpenBLAS 0.3.30 "
+            f"single-threaded per task, {threads} threads")
+    return times, desc, threads
 
 
 def cpu_reference_calls(wl, reps: int = 3):
@@ -361,19 +382,25 @@ def cusolver_fp64_comparator(torch, device, wl):
                     "solve_triangular for the variance; same inputs; best of 2"}
 
 
+# Full-size calls the reference arm times (one C2 call is about 30 s on 16
+# host cores, so the requested --steps are not all run at full size).
+REF_FULL_REPS = 2
+
+
 def run_reference(args, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    for _ in range(args.warmup):
-        pass  # warm-up happens inside cpu_reference_sample's first rep
-    sample_s, scale, desc, threads = cpu_reference_sample(wl, max(args.steps, 1))
-    value = sample_s * scale
+    reps = min(max(args.steps, 1), REF_FULL_REPS)
+    times, desc, threads = cpu_reference_full(wl, reps)
+    value = float(np.mean(times))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "steps": reps, "warmup": 1, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": value * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_of(wl),
+        "seconds_per_call": times,
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference", "sample": desc},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -388,7 +415,9 @@ def config_of(wl):
             "parallelism": "replicas"}
 
 
-PRECISIONS = {"fp64": 0, "mixed-tf32": 1, "mixed-bf16": 2}
+PRECISIONS = {"fp64": 0, "mixed-tf32": 1, "mixed-bf16": 2, "fp64-int8": 3}
+# modes timed beside the headline one (besides FP64, which every run times)
+ARM_ORDER = ("fp64-int8", "mixed-tf32", "mixed-bf16")
 
 # DRAM traffic of one representative launch of the dominant kernel, from an
 # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum); the live
@@ -419,7 +448,8 @@ SERVE_REQUESTS = 200
 SERVE_RATE = 40.0  # requests per second
 
 
-def time_device_steps(torch, gp, hyper, dxt, m, dmean, dvar, stream, steps, warmup, barrier, local):
+def time_device_steps(torch, gp, hyper, dxt, m, dmean, dvar, stream, steps, warmup, barrier, local,
+                      instrumented=True):
     """Device-timed fit+predict steps (CUDA events on the launching stream).
 
     Two timed regions of `steps` steps each: the first one plain (its time is
@@ -449,6 +479,8 @@ def time_device_steps(torch, gp, hyper, dxt, m, dmean, dvar, stream, steps, warm
         barrier()
     gp.check_status()
     elapsed = start.elapsed_time(end)
+    if not instrumented:
+        return elapsed, {"launches": 0, "gemm_launches": 0, "gemm_ms": 0.0, "gemm_flops": 0.0}, clocks.summary()
     # instrumented region: one step first fills the library's event pool
     capi.stats_enable_timing(True)
     step()
@@ -562,6 +594,8 @@ def run_ours(args, wl):
     x, y, xt = synthetic(n, m, d)
     gp = capi.CudaGP(x, y, n // T, T, d, device=local)
     gp.set_precision(PRECISIONS[args.precision])
+    if args.slices:
+        gp.set_int8_slices(args.slices)
 
     dxt = torch.tensor(xt, device=device)
     dmean = torch.empty(m, dtype=torch.float64, device=device)
@@ -599,30 +633,45 @@ def run_ours(args, wl):
     loss = gp.compute_loss(hyper)
     pcg_iters = gp.pcg_iterations()
 
-    # the plain FP64 path on the same inputs (timed the same way), and the
-    # mixed results' error against it
+    # the other precision modes on the same inputs, timed the same way, and
+    # every mode's error against the plain FP64 path
     fp64 = None
-    if args.precision != "fp64" and not args.skip_fp64:
-        gp.set_precision(capi.PREC_FP64)
-        m64 = torch.empty_like(dmean)
-        v64 = torch.empty_like(dvar)
-        el64, st64, clk64 = time_device_steps(torch, gp, hyper, dxt, m, m64, v64, stream, args.steps, args.warmup,
-                                              barrier, local)
-        ms64 = max_over_ranks(el64, dist if world > 1 else None, device) / args.steps
-        mean64, var64 = m64.cpu().numpy(), v64.cpu().numpy()
-        loss64 = gp.compute_loss(hyper)
-        fp64 = {
-            "value": aggregate_seconds(ms64, world), "ms_per_step": ms64,
-            "gemm_tflops": st64["gemm_flops"] / (st64["gemm_ms"] / 1e3) / 1e12 if st64["gemm_ms"] > 0 else None,
-            "clocks": clk64,
-            "speedup_of_mixed": ms64 / ms_per_step,
-            "mixed_error_vs_fp64": {
-                "mean_max_rel": float(np.max(np.abs(mean_h - mean64)) / np.max(np.abs(mean64))),
-                "var_max_rel": float(np.max(np.abs(var_h - var64) / var64)),
-                "loss_rel": float(abs(loss - loss64) / abs(loss64)),
-            },
-        }
+    arms = {}
+    if not args.skip_fp64:
+        results = {}
+        others = ["fp64"] + ([a for a in ARM_ORDER if a != args.precision] if not args.skip_arms else [])
+        for prec in others:
+            if prec == args.precision:
+                continue
+            gp.set_precision(PRECISIONS[prec])
+            ma, va = torch.empty_like(dmean), torch.empty_like(dvar)
+            el, st, ck = time_device_steps(torch, gp, hyper, dxt, m, ma, va, stream, args.steps, args.warmup,
+                                           barrier, local, instrumented=(prec == "fp64"))
+            msa = max_over_ranks(el, dist if world > 1 else None, device) / args.steps
+            results[prec] = dict(mean=ma.cpu().numpy(), var=va.cpu().numpy(), loss=gp.compute_loss(hyper), ms=msa,
+                                 clocks=ck, stats=st)
         gp.set_precision(PRECISIONS[args.precision])
+        ref64 = results["fp64"]
+
+        def error_vs_fp64(mean_a, var_a, loss_a):
+            return {
+                "mean_max_rel": float(np.max(np.abs(mean_a - ref64["mean"])) / np.max(np.abs(ref64["mean"]))),
+                "var_max_rel": float(np.max(np.abs(var_a - ref64["var"]) / ref64["var"])),
+                "loss_rel": float(abs(loss_a - ref64["loss"]) / abs(ref64["loss"])),
+            }
+
+        st64 = ref64["stats"]
+        fp64 = {
+            "value": aggregate_seconds(ref64["ms"], world), "ms_per_step": ref64["ms"],
+            "gemm_tflops": st64["gemm_flops"] / (st64["gemm_ms"] / 1e3) / 1e12 if st64["gemm_ms"] > 0 else None,
+            "clocks": ref64["clocks"],
+            "speedup_of_mixed": ref64["ms"] / ms_per_step,
+            "mixed_error_vs_fp64": error_vs_fp64(mean_h, var_h, loss),
+        }
+        for prec, r in results.items():
+            if prec != "fp64":
+                arms[prec] = {"ms_per_step": r["ms"], "speedup_over_fp64": ref64["ms"] / r["ms"],
+                              "error_vs_fp64": error_vs_fp64(r["mean"], r["var"], r["loss"]), "clocks": r["clocks"]}
 
     if rank != 0:
         if world > 1:
@@ -642,6 +691,12 @@ def run_ours(args, wl):
                   "trailing updates, variance solve)")
         peak_source = ("cuBLAS TF32 GEMM (torch.matmul fp32 8192^3 with allow_tf32, best of 5) measured in this "
                        "run; MEASURED_PEAKS.json holds only the bf16 figure")
+    elif args.precision == "fp64-int8":
+        peak = measure_int8_peak(torch, device)
+        kernel = ("oz_gemm_kernel (tcgen05.mma.cta_group::2 kind::i8, int32 groups in TMEM, FP64 accumulation in the "
+                  "epilogue: every product of the factorisation and of the variance solve)")
+        peak_source = ("cuBLASLt int8 GEMM (torch._int_mm 8192^3, best of 5) measured in this run; "
+                       "MEASURED_PEAKS.json holds no int8 figure")
     else:
         peak = peaks.get("bf16_tflops") or measure_gemm_peak(torch, device, torch.bfloat16)
         kernel = "tc_gemm_kernel<BF16> (tcgen05.mma kind::f16 with bf16 operands)"
@@ -649,8 +704,8 @@ def run_ours(args, wl):
     gemm_tflops = stats["gemm_flops"] / (stats["gemm_ms"] / 1e3) / 1e12 if stats["gemm_ms"] > 0 else None
     step_flops = algorithmic_flops(n, m)
     if world == 1 and not args.skip_cpu_baseline:
-        sample_s, scale, desc, threads = cpu_reference_sample(wl, 3)
-        cpu = {"value": sample_s * scale, "unit": "s", "cores": threads, "kind": "reference", "sample": desc,
+        times, desc, threads = cpu_reference_full(wl, 1)
+        cpu = {"value": times[0], "unit": "s", "cores": threads, "kind": "reference", "sample": desc,
                "calls_at_sample": cpu_reference_calls(wl),
                "gpu_calls_at_sample": {"fp64": gpu_calls(wl, capi.PREC_FP64),
                                        args.precision: gpu_calls(wl, PRECISIONS[args.precision])}}
@@ -699,6 +754,7 @@ def run_ours(args, wl):
         "phases_ms": phases,
         "clocks": clk,
         "fp64": fp64,
+        "arms": arms,
         "fp64_library_comparator": comparator,
         "serving": serve,
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
@@ -719,10 +775,12 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
     ap.add_argument("--precision", choices=sorted(PRECISIONS), default="mixed-tf32")
+    ap.add_argument("--slices", type=int, default=0, help="int8 digit planes of the fp64-int8 mode (0 = default)")
     ap.add_argument("--skip-cpu-baseline", action="store_true",
                     help="omit the CPU reference sample (cpu_baseline becomes null)")
     ap.add_argument("--skip-fp64", action="store_true", help="omit the FP64 comparison arm")
     ap.add_argument("--skip-serving", action="store_true", help="omit the serving stream")
+    ap.add_argument("--skip-arms", action="store_true", help="omit the other precision modes (FP64 still runs)")
     ap.add_argument("--profile", action="store_true",
                     help="device steps only (no CPU sample, e2e loop or peak measurement): for ncu captures")
     args = ap.parse_args()

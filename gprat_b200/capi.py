@@ -84,6 +84,7 @@ def _load() -> ctypes.CDLL:
     _vp, _i64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)
     lib.gprat_cu_steps_enable.argtypes = [ctypes.c_int]
     lib.gprat_cu_test_trsv.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int]
+    lib.gprat_cu_test_set_wait_budget.argtypes = [_i64]
     _i8p, _i32p = ctypes.POINTER(ctypes.c_int8), ctypes.POINTER(ctypes.c_int32)
     lib.gprat_cu_test_oz_split.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, _i8p, _i32p]
     lib.gprat_cu_test_oz_gemm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double,
@@ -108,6 +109,8 @@ def _load() -> ctypes.CDLL:
     lib.gprat_cu_multiserver_stats.argtypes = lib.gprat_cu_server_stats.argtypes
     lib.gprat_cu_multiserver_replica_completed.argtypes = [_vp, ctypes.c_int, _i64p]
     lib.gprat_cu_multiserver_set_replication.argtypes = [_vp, ctypes.c_int]
+    lib.gprat_cu_multiserver_resident_bytes.argtypes = [_vp, ctypes.c_int, _i64p]
+    lib.gprat_cu_test_multiserver_fail_copy.argtypes = [_vp, ctypes.c_int]
     return lib
 
 
@@ -205,6 +208,12 @@ def test_trsv(kind: int, L: np.ndarray, b: np.ndarray, max_ctas: int = 0) -> Tup
     xf, xb = np.empty(n), np.empty(n)
     check(lib.gprat_cu_test_trsv(int(kind), n, _p(L), _p(b), _p(xf), _p(xb), int(max_ctas)))
     return xf, xb
+
+
+def test_set_wait_budget(polls: int) -> None:
+    """Poll budget of the fused triangular solves' waits on the current device
+    (negative: the default).  Tests use 0 to make a wait give up."""
+    check(lib.gprat_cu_test_set_wait_budget(int(polls)))
 
 
 def test_oz_split(src: np.ndarray, s: int, block: bool) -> Tuple[np.ndarray, np.ndarray]:

@@ -239,6 +239,9 @@ void trsv_fused_forward_f32(const float *L, int64_t ld, const float *Linv, int n
                             double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
 void trsv_fused_backward_f32(const float *L, int64_t ld, const float *Linv, int n, double *x, int *flags,
                              double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
+// Poll budget of the single-launch solves' waits on the current device
+// (polls < 0: the default, about 0.5-1 s).
+void set_trsv_wait_budget(long long polls);
 // Same with an FP32 factor (mixed precision); FP64 right-hand side and arithmetic.
 void trsv_forward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s);
 void trsv_backward_f32(const float *L, int64_t ldl, const double *Linv, int nb, int n, double *rhs, cudaStream_t s);

@@ -25,6 +25,8 @@ void set_last_error(const std::string &message);
 int server_add_model_copy(gprat_cu_server *dst, gprat_cu_server *src, int src_model, const double *train_in,
                           int64_t n_in, const double *train_out, int64_t n_out, int n_tiles, int n_tile_size,
                           int n_regressors, int *model_id);
+int server_release_model(gprat_cu_server *sv, int model_id);
+int64_t server_resident_bytes(gprat_cu_server *sv);
 }
 
 using namespace gprat_cu;
@@ -58,6 +60,7 @@ struct gprat_cu_multiserver
     std::vector<double> latencies_ms;
     int64_t next_id = 1;
     int replication = GPRAT_CU_REPLICATE_COPY;
+    int fail_copy_replica = -1;  // test hook: the next copy to this replica reports a failure
 };
 
 namespace
@@ -144,6 +147,11 @@ void copy_to_replicas(gprat_cu_multiserver *ms, int id0, const double *x, int64_
 {
     ids.assign(ms->servers.size(), -1);
     ids[0] = id0;
+    int fail = -1;
+    {
+        std::lock_guard<std::mutex> lk(ms->mtx);
+        std::swap(fail, ms->fail_copy_replica);
+    }
     on_every_replica(ms,
                      [&](int r)
                      {
@@ -151,9 +159,28 @@ void copy_to_replicas(gprat_cu_multiserver *ms, int id0, const double *x, int64_
                          {
                              return static_cast<int>(GPRAT_CU_OK);
                          }
+                         if (r == fail)
+                         {
+                             set_last_error("copy to the replica failed (injected by the test hook)");
+                             return static_cast<int>(GPRAT_CU_ERR_OOM);
+                         }
                          return server_add_model_copy(ms->servers[r], ms->servers[0], id0, x, nx, y, ny, n_tiles, T,
                                                       d, &ids[r]);
                      });
+}
+
+// A replicated fit that failed somewhere: the replicas' models that did
+// come into being (ids[r] >= 0) are freed, so no unreachable copy stays
+// resident.
+void release_replicas(gprat_cu_multiserver *ms, const std::vector<int> &ids)
+{
+    for (size_t r = 0; r < ids.size() && r < ms->servers.size(); ++r)
+    {
+        if (ids[r] >= 0)
+        {
+            server_release_model(ms->servers[r], ids[r]);
+        }
+    }
 }
 
 // Lets each replica's device read every other replica's memory directly
@@ -260,22 +287,30 @@ int gprat_cu_multiserver_add_model(gprat_cu_multiserver *ms, const double *train
         {
             require_ms(ms != nullptr && model_id != nullptr, "arguments must not be NULL");
             std::vector<int> ids(ms->servers.size(), -1);
-            if (ms->replication == GPRAT_CU_REPLICATE_COPY)
+            try
             {
-                int id0 = -1;
-                check_rc(gprat_cu_server_add_model(ms->servers[0], train_in, n_in, train_out, n_out, n_tiles,
-                                                   n_tile_size, n_regressors, hyper, &id0));
-                copy_to_replicas(ms, id0, train_in, n_in, train_out, n_out, n_tiles, n_tile_size, n_regressors, ids);
+                if (ms->replication == GPRAT_CU_REPLICATE_COPY)
+                {
+                    check_rc(gprat_cu_server_add_model(ms->servers[0], train_in, n_in, train_out, n_out, n_tiles,
+                                                       n_tile_size, n_regressors, hyper, &ids[0]));
+                    copy_to_replicas(ms, ids[0], train_in, n_in, train_out, n_out, n_tiles, n_tile_size,
+                                     n_regressors, ids);
+                }
+                else
+                {
+                    on_every_replica(ms,
+                                     [&](int r)
+                                     {
+                                         return gprat_cu_server_add_model(ms->servers[r], train_in, n_in, train_out,
+                                                                          n_out, n_tiles, n_tile_size, n_regressors,
+                                                                          hyper, &ids[r]);
+                                     });
+                }
             }
-            else
+            catch (...)
             {
-                on_every_replica(ms,
-                                 [&](int r)
-                                 {
-                                     return gprat_cu_server_add_model(ms->servers[r], train_in, n_in, train_out,
-                                                                      n_out, n_tiles, n_tile_size, n_regressors,
-                                                                      hyper, &ids[r]);
-                                 });
+                release_replicas(ms, ids);  // no replica keeps a model that has no global id
+                throw;
             }
             std::lock_guard<std::mutex> lk(ms->mtx);
             ms->model_ids.push_back(ids);
@@ -353,12 +388,14 @@ int gprat_cu_multiserver_submit_fit(gprat_cu_multiserver *ms, const double *trai
                                                           n_tile_size, n_regressors, hyper, &p.local_ids[r]);
                 if (rc != GPRAT_CU_OK)
                 {
-                    // the replicas that accepted the fit finish it; their copies are dropped
+                    // the replicas that accepted the fit finish it; their models are freed
                     const std::string m = gprat_cu_last_error();
+                    std::vector<int> done(r, -1);
                     for (size_t q = 0; q < r; ++q)
                     {
-                        gprat_cu_server_wait(ms->servers[q], p.local_ids[q], nullptr, nullptr, nullptr, nullptr);
+                        gprat_cu_server_wait(ms->servers[q], p.local_ids[q], nullptr, nullptr, &done[q], nullptr);
                     }
+                    release_replicas(ms, done);
                     throw Error(rc, "replica " + std::to_string(r) + ": " + m);
                 }
             }
@@ -411,19 +448,35 @@ int gprat_cu_multiserver_wait(gprat_cu_multiserver *ms, int64_t request_id, doub
                 // fitted on replica 0; the copies to the others count in the latency
                 check_rc(gprat_cu_server_wait(ms->servers[0], p.local_ids[0], nullptr, nullptr, &ids[0], &worst));
                 const auto t0 = std::chrono::steady_clock::now();
-                copy_to_replicas(ms, ids[0], p.x.data(), static_cast<int64_t>(p.x.size()), p.y.data(),
-                                 static_cast<int64_t>(p.y.size()), p.n_tiles, p.T, p.d, ids);
+                try
+                {
+                    copy_to_replicas(ms, ids[0], p.x.data(), static_cast<int64_t>(p.x.size()), p.y.data(),
+                                     static_cast<int64_t>(p.y.size()), p.n_tiles, p.T, p.d, ids);
+                }
+                catch (...)
+                {
+                    release_replicas(ms, ids);  // the original on replica 0 and the copies that succeeded
+                    throw;
+                }
                 worst += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
             }
             else
             {
                 std::vector<double> lats(ms->servers.size(), 0.0);
-                on_every_replica(ms,
-                                 [&](int r)
-                                 {
-                                     return gprat_cu_server_wait(ms->servers[r], p.local_ids[r], nullptr, nullptr,
-                                                                 &ids[r], &lats[r]);
-                                 });
+                try
+                {
+                    on_every_replica(ms,
+                                     [&](int r)
+                                     {
+                                         return gprat_cu_server_wait(ms->servers[r], p.local_ids[r], nullptr, nullptr,
+                                                                     &ids[r], &lats[r]);
+                                     });
+                }
+                catch (...)
+                {
+                    release_replicas(ms, ids);  // the replicas whose fit succeeded
+                    throw;
+                }
                 for (double l : lats)
                 {
                     worst = std::max(worst, l);
@@ -511,6 +564,30 @@ int gprat_cu_multiserver_set_replication(gprat_cu_multiserver *ms, int mode)
                        "replication mode must be GPRAT_CU_REPLICATE_COPY or GPRAT_CU_REPLICATE_REFIT");
             std::lock_guard<std::mutex> lk(ms->mtx);
             ms->replication = mode;
+        });
+}
+
+int gprat_cu_multiserver_resident_bytes(gprat_cu_multiserver *ms, int replica, int64_t *bytes)
+{
+    return guarded_ms(
+        [&]
+        {
+            require_ms(ms != nullptr && bytes != nullptr, "arguments must not be NULL");
+            require_ms(replica >= 0 && replica < static_cast<int>(ms->servers.size()), "unknown replica");
+            *bytes = server_resident_bytes(ms->servers[replica]);
+        });
+}
+
+int gprat_cu_test_multiserver_fail_copy(gprat_cu_multiserver *ms, int replica)
+{
+    return guarded_ms(
+        [&]
+        {
+            require_ms(ms != nullptr, "multi-server must not be NULL");
+            require_ms(replica >= 1 && replica < static_cast<int>(ms->servers.size()),
+                       "the injected failure needs a replica other than the first");
+            std::lock_guard<std::mutex> lk(ms->mtx);
+            ms->fail_copy_replica = replica;
         });
 }
 

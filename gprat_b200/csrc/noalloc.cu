@@ -21,7 +21,14 @@
 //     the GPU (different streams or threads, same device) race on it.
 //   * The first call on a device resolves the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current).
-//     Make that first call before any stream capture.
+//     Make that first call before any stream capture.  With CUDA's lazy
+//     module loading (the default) that first call may also load the
+//     library's device code and so reserve the array: a caller that must
+//     never allocate makes one warm-up call outside its critical region.
+//     The address is kept for the life of the process, so cudaDeviceReset
+//     on a device after its first call is not supported.
+//   * Every call copies the status word to the host and synchronises the
+//     stream it was given before it returns.
 #include "common.cuh"
 #include "gprat_cu.h"
 
@@ -43,6 +50,7 @@ constexpr int64_t OFF_PARAMS = OFF_ALPHA + NOALLOC_MAX_N;                    // 
 constexpr int64_t OFF_STATUS = OFF_PARAMS + 32;                              // DeviceStatus
 constexpr int64_t SCRATCH_DOUBLES = OFF_STATUS + 32;
 static_assert(sizeof(DeviceParams) <= 32 * sizeof(double), "parameter block does not fit its slot");
+static_assert(sizeof(DeviceStatus) <= 32 * sizeof(double), "status word does not fit its slot");
 
 // The scratch.  In host code this name is only a host-side stand-in, not a
 // device address: host code must use the address from cudaGetSymbolAddress.

@@ -256,20 +256,17 @@ __device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t adesc, uin
         "l"(adesc), "l"(bdesc), "r"(OZ_IDESC), "r"(accumulate));
 }
 
-__device__ __forceinline__ void tmem_ld32_i(uint32_t taddr, int32_t *v)
+__device__ __forceinline__ void tmem_ld16_i(uint32_t taddr, int32_t *v)
 {
-    uint32_t r[32];
+    uint32_t r[16];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
+    for (int j = 0; j < 16; ++j)
     {
         v[j] = static_cast<int32_t>(r[j]);
     }
@@ -310,7 +307,7 @@ __device__ __forceinline__ void oz_tile(int t, bool lower, int tiles_m, int tile
     n0 = (t - i * (i + 1)) * 128;
 }
 
-__global__ void __maxnreg__(200)
+__global__ void __launch_bounds__(OZ_THREADS, 1)
     oz_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzKernelArgs p)
 {
     extern __shared__ uint8_t smem_raw[];
@@ -547,26 +544,28 @@ __global__ void __maxnreg__(200)
                     const uint32_t taddr = tmem_base + (static_cast<uint32_t>(q * 32) << 16) +
                                            static_cast<uint32_t>(u * 128 + h * 64);
                     const double sc = bad ? __longlong_as_double(0x7ff8000000000000ll) : pow2(ea + eb - 12 - 7 * g);
-                    int32_t v[32];
-                    tmem_ld32_i(taddr, v);
-                    tmem_ld_wait();
+                    // 16 columns at a time (the 64 FP64 accumulators already take 128 registers)
 #pragma unroll
-                    for (int j = 0; j < 32; ++j)
+                    for (int c = 0; c < 4; ++c)
                     {
-                        acc[j] = fma(i2d(v[j]), sc, acc[j]);
-                    }
-                    tmem_ld32_i(taddr + 32, v);
-                    tmem_ld_wait();
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0)
-                    {
-                        mbar_arrive_cluster(map_to_rank(&tempty[u], 0));
-                    }
+                        int32_t v[16];
+                        tmem_ld16_i(taddr + c * 16, v);
+                        tmem_ld_wait();
+                        if (c == 3)
+                        {
+                            // the accumulator is read: the MMA warp may reuse it
+                            tc_fence_before();
+                            __syncwarp();
+                            if (lane == 0)
+                            {
+                                mbar_arrive_cluster(map_to_rank(&tempty[u], 0));
+                            }
+                        }
 #pragma unroll
-                    for (int j = 0; j < 32; ++j)
-                    {
-                        acc[32 + j] = fma(i2d(v[j]), sc, acc[32 + j]);
+                        for (int j = 0; j < 16; ++j)
+                        {
+                            acc[c * 16 + j] = fma(i2d(v[j]), sc, acc[c * 16 + j]);
+                        }
                     }
                     ++nu;
                 }

@@ -109,6 +109,7 @@ struct Model
     PinnedBuf h_in, h_out;
     cudaEvent_t done_ev = nullptr;
     bool busy = false;
+    bool released = false;  // device state freed (server_release_model); the id stays unused
     std::vector<Request *> inflight;
     int64_t inflight_bytes = 0;
     ~Model()
@@ -665,6 +666,49 @@ int server_add_model_copy(gprat_cu_server *dst, gprat_cu_server *src, int src_mo
             *model_id = static_cast<int>(dst->models.size()) - 1;
         });
 }
+
+// Frees a model that no request refers to and that has no batch in flight
+// (replica serving drops the copies of a fit that failed on another replica):
+// its device state goes back to the device and to the budget, and its id is
+// never reused.
+int server_release_model(gprat_cu_server *sv, int model_id)
+{
+    return guarded_sv(
+        [&]
+        {
+            need(sv != nullptr, "server must not be NULL");
+            Model *md = nullptr;
+            {
+                std::lock_guard<std::mutex> lk(sv->mtx);
+                need(model_id >= 0 && model_id < static_cast<int>(sv->models.size()), "unknown model id");
+                md = sv->models[model_id].get();
+                need(!md->released, "model already released");
+                need(!md->busy, "model has a batch in flight");
+                for (const Request *r : sv->pending)
+                {
+                    need(r->model != model_id, "model has pending requests");
+                }
+                md->released = true;  // the scheduler never touches it again
+                sv->used -= md->resident;
+                md->resident = 0;
+            }
+            GPRAT_CUDA_CHECK(cudaSetDevice(sv->device));
+            gprat_cu_gp *gp = md->gp;
+            md->gp = nullptr;
+            gprat_cu_gp_destroy(gp);
+            md->d_series.release();
+            md->d_mean.release();
+            md->d_var.release();
+            md->d_offsets.release();
+        });
+}
+
+// Bytes the server's resident models hold (its admission count).
+int64_t server_resident_bytes(gprat_cu_server *sv)
+{
+    std::lock_guard<std::mutex> lk(sv->mtx);
+    return sv->used;
+}
 }  // namespace gprat_cu
 
 extern "C" {
@@ -683,6 +727,7 @@ int gprat_cu_server_submit_predict(gprat_cu_server *sv, int model_id, const doub
             r->model = model_id;
             std::lock_guard<std::mutex> lk(sv->mtx);
             need(model_id >= 0 && model_id < static_cast<int>(sv->models.size()), "unknown model id");
+            need(!sv->models[model_id]->released, "model was released");
             const int d = sv->models[model_id]->d;
             need(n_test_in >= static_cast<int64_t>(m) + d - 1, "test series too short for the sliding window");
             r->series.assign(test_in, test_in + (static_cast<int64_t>(m) + d - 1));

@@ -387,3 +387,18 @@ extern "C" int gprat_cu_test_oz_gemm(int M, int N, int K, const double *A, const
         return GPRAT_CU_ERR_INVALID_ARG;
     }
 }
+
+extern "C" int gprat_cu_test_set_wait_budget(int64_t polls)
+{
+    try
+    {
+        set_trsv_wait_budget(polls);
+        set_last_error("");
+        return GPRAT_CU_OK;
+    }
+    catch (const Error &e)
+    {
+        set_last_error(e.what());
+        return e.code;
+    }
+}

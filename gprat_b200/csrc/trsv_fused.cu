@@ -34,6 +34,9 @@ namespace
 constexpr int FT = 256;  // threads per CTA (8 warps)
 constexpr int FB = 128;  // block size
 constexpr long long SPIN_LIMIT = 1ll << 24;  // with 32 ns sleeps: about 0.5-1 s
+// The poll budget the solves use on this device (SPIN_LIMIT unless a test
+// shrank it with gprat_cu_test_set_wait_budget).
+__device__ long long g_spin_limit = SPIN_LIMIT;
 constexpr long long SENTINEL = -1ll;          // 0xFFFF...FF
 
 // Packed lower triangle of a 128 x 128 FP64 block: row r holds columns
@@ -84,6 +87,7 @@ template <int N>
 __device__ __forceinline__ void await_x(const double *const (&p)[N], double (&v)[N], bool urgent, DeviceStatus *st)
 {
     long long spins = 0;
+    const long long limit = g_spin_limit;
     for (;;)
     {
         bool missing = false;
@@ -97,7 +101,7 @@ __device__ __forceinline__ void await_x(const double *const (&p)[N], double (&v)
         {
             return;
         }
-        if (++spins > SPIN_LIMIT)
+        if (++spins > limit)
         {
             if (st != nullptr)
             {
@@ -127,7 +131,7 @@ __device__ __forceinline__ void await_x(const double *const (&p)[N], double (&v)
                     if (!waited && __double_as_longlong(v[t]) == SENTINEL)
                     {
                         long long inner = 0;
-                        while (__double_as_longlong(load_relaxed(p[t])) == SENTINEL && ++inner < SPIN_LIMIT)
+                        while (__double_as_longlong(load_relaxed(p[t])) == SENTINEL && ++inner < limit)
                         {
                             __nanosleep(256);
                         }
@@ -951,6 +955,15 @@ void trsv_fused_backward_f32(const float *L, int64_t ld, const float *Linv, int 
     trsv_bwd_f32_kernel<<<grid_for(nblk, max_ctas), FT, SMEM_F32_BWD, s>>>(L, ld, Linv, n, nblk, scratch, x, flags,
                                                                         st);
     GPRAT_LAUNCH_CHECK();
+}
+
+// Sets the poll budget of the solves' waits on the current device; polls < 0
+// restores the default.  Test use: a budget of 0 makes a wait on an unsolved
+// block give up at once (the status word's timeout flag), with no hang.
+void set_trsv_wait_budget(long long polls)
+{
+    const long long v = polls < 0 ? SPIN_LIMIT : polls;
+    GPRAT_CUDA_CHECK(cudaMemcpyToSymbol(g_spin_limit, &v, sizeof(v)));
 }
 
 }  // namespace gprat_cu

@@ -159,3 +159,16 @@ class MultiServer(Server):
             capi.check(capi.lib.gprat_cu_multiserver_replica_completed(self._h, r, ctypes.byref(c)))
             out.append(c.value)
         return out
+
+    def resident_bytes(self) -> list:
+        """Device bytes the resident models hold, per replica."""
+        out = []
+        for r in range(self.n_replicas):
+            c = ctypes.c_int64()
+            capi.check(capi.lib.gprat_cu_multiserver_resident_bytes(self._h, r, ctypes.byref(c)))
+            out.append(c.value)
+        return out
+
+    def fail_next_copy(self, replica: int) -> None:
+        """Test hook: the next copy of a fitted model to `replica` fails (on the host)."""
+        capi.check(capi.lib.gprat_cu_test_multiserver_fail_copy(self._h, int(replica)))

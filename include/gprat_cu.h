@@ -225,6 +225,11 @@ int gprat_cu_gp_pcg_iterations(gprat_cu_gp *gp, int *iterations);
  * call and keeps the last call's contents: calls that overlap on the GPU
  * race.  The first call on a device resolves the array's device address
  * (cudaGetSymbolAddress, once per device); make it before any stream capture.
+ * With CUDA's lazy module loading that first call may also load the
+ * library's device code and reserve the array, so a caller that must never
+ * allocate makes one warm-up call outside its critical region; the address
+ * is kept for the life of the process (cudaDeviceReset of that device
+ * afterwards is not supported).
  */
 int gprat_cu_compute_loss_noalloc(int device,
                                   const double *d_train_in,
@@ -305,6 +310,16 @@ int gprat_cu_test_tc_gemm(int kind,
  * from b.  max_ctas > 0 bounds the grid.
  */
 int gprat_cu_test_trsv(int kind, int n, const double *L, const double *b, double *x_fwd, double *x_bwd, int max_ctas);
+
+/*
+ * Test entry (no counterpart in the reference, which bounds no wait): the
+ * number of polls after which a wait of the single-launch triangular solves
+ * on an unsolved row block gives up, on the current device; the call then
+ * returns GPRAT_CU_ERR_TIMEOUT.  polls < 0 restores the default (about
+ * 0.5-1 s of polling).  The waits only re-read global memory, so a budget of
+ * 0 ends them at once and nothing is left in flight.
+ */
+int gprat_cu_test_set_wait_budget(int64_t polls);
 
 /*
  * Kernel-level test entry (no counterpart in the reference): splits the
@@ -475,6 +490,14 @@ int gprat_cu_multiserver_stats(gprat_cu_multiserver *server,
                                int64_t *completed,
                                int64_t *batches);
 int gprat_cu_multiserver_replica_completed(gprat_cu_multiserver *server, int replica, int64_t *completed);
+/* Bytes of device memory the resident models of one replica hold (the
+ * replica's admission count).  A replicated fit or add that fails on one
+ * replica frees the models it made on the others, so they do not stay
+ * resident without a global id. */
+int gprat_cu_multiserver_resident_bytes(gprat_cu_multiserver *server, int replica, int64_t *bytes);
+/* Test entry: the next copy of a fitted model to `replica` (>= 1) reports
+ * GPRAT_CU_ERR_OOM instead of copying (a failure made on the host). */
+int gprat_cu_test_multiserver_fail_copy(gprat_cu_multiserver *server, int replica);
 #define GPRAT_CU_REPLICATE_COPY 0
 #define GPRAT_CU_REPLICATE_REFIT 1
 int gprat_cu_multiserver_set_replication(gprat_cu_multiserver *server, int mode);

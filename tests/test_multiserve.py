@@ -117,3 +117,36 @@ def test_multiserver_invalid_requests(serving):
         mean, var, _, _ = ms.wait(ms.submit_predict(mid, np.linspace(-1, 1, 40), 33))
         assert mean.shape == (33,) and np.all(var > 0)
         assert ms.replica_completed() in ([1, 0], [0, 1])
+
+
+def test_failed_copy_frees_every_replica(serving):
+    """A replicated fit whose copy to one replica fails (an error made on the
+    host by the test hook) fails the request and leaves nothing resident
+    without a global id: the fitted original on the first replica is freed
+    too.  The same holds for a synchronous add.  The server keeps serving, and
+    its results match the oracle."""
+    capi, S = serving
+    fx, fy, _ = O.synthetic(1024, 16, 8, seeds=(81, 82, 83))
+    hyper = (1.0, 1.0, 0.1)
+    series = np.random.default_rng(8).uniform(-1, 1, 50 + 7)
+    with S.MultiServer([0, 0], memory_budget_bytes=BUDGET, precision=capi.PREC_FP64,
+                       replication=capi.REPLICATE_COPY) as ms:
+        before = ms.resident_bytes()
+        ms.fail_next_copy(1)
+        with pytest.raises(capi.GpratCudaError) as err:
+            ms.wait(ms.submit_fit(fx, fy, 8, 128, 8, hyper))
+        assert err.value.code == capi.ERR_OOM
+        assert ms.resident_bytes() == before
+        ms.fail_next_copy(1)
+        with pytest.raises(capi.GpratCudaError):
+            ms.add_model(fx, fy, 8, 128, 8, hyper)
+        assert ms.resident_bytes() == before
+        _, _, gid, _ = ms.wait(ms.submit_fit(fx, fy, 8, 128, 8, hyper))
+        assert all(b > a for a, b in zip(before, ms.resident_bytes()))
+        results = [ms.wait(ms.submit_predict(gid, series, 50)) for _ in range(4)]
+        assert min(ms.replica_completed()) > 0
+    om, ov = O.OracleGP(fx, fy, 8, 128, 8, hyper).predict_with_uncertainty(series, 1, 50)
+    for mean, var, got, _ in results:
+        assert got == gid
+        assert np.max(np.abs(mean - om)) <= 1e-10 * max(1.0, np.max(np.abs(om)))
+        assert np.max(np.abs(var - ov) / ov) <= 1e-10
