@@ -13,23 +13,27 @@
 // oz_gemm_kernel: persistent, warp-specialised CTA pair (cluster of 2, 320
 // threads each), one 256 x 128 output tile per pair at a time:
 //   warp 0, one lane (both CTAs): TMA producer.  For each 128-column block k
-//     and group g it loads A digit plane g (this CTA's 128 rows, 16 KB) into
-//     a ring of OZ_RA slots, then the B digit planes g - p, p = 0..g (this
-//     CTA's 64 rows, 8 KB) into a ring of OZ_RB slots.  The A planes of a
-//     block stay resident until its last group, so each A tile crosses from
-//     L2 once per block and each B tile once per pair (p, g - p).
+//     and group g it loads digit plane g of A (this CTA's 128 rows, 16 KB)
+//     and of B (this CTA's 64 rows, 8 KB) into rings of OZ_RA and OZ_RB
+//     slots.  A block's planes stay resident until its last group, so every
+//     digit tile crosses from L2 once per block; the spare slots let the next
+//     block's first planes load while the current block's last groups run.
 //   warp 1, one lane (leader): MMA issuer.  Group g of block k is one unit:
 //     for p = 0..g, four tcgen05.mma.cta_group::2.kind::i8 (M 256, N 128,
 //     K 32) of A_p against B_{g-p} into one int32 accumulator in tensor
 //     memory (four accumulators of 128 columns rotate); tcgen05.commit frees
-//     B slots, the accumulator, and after the block's last group its A slots.
+//     the accumulator, and after the block's last group its A and B slots.
 //   warps 2..9 (both CTAs): epilogue.  Two warps per TMEM lane quarter, 64
-//     columns each; every unit is read with tcgen05.ld, converted exactly to
-//     FP64 (2^52 + 2^31 bias trick) and added with its scale
-//     2^(eA + eB - 12 - 7 g) into 64 FP64 registers per thread.  After the
-//     tile's last unit, alpha * acc is staged per warp in shared memory
-//     (16-byte XOR swizzle) and written to C with coalesced 16-byte accesses
-//     (beta = 1 adds to C).
+//     columns each; units are read with tcgen05.ld in pairs of groups
+//     (g, g + 1) and combined exactly in int32 as 128 P_g + P_{g+1}
+//     (|P_g| <= 7 * 2^19), converted exactly to FP64 (2^52 + 2^31 bias
+//     trick) and added with the pair's scale 2^(eA + eB - 12 - 7 (g + 1))
+//     into 64 FP64 registers per thread (a last unpaired group as 128 P_g at
+//     the same scale).  The next block's exponents are loaded while a block
+//     is read.  After the tile's last unit, alpha * acc is staged per warp in
+//     shared memory, 8 columns at a time (16-byte XOR swizzle), and written
+//     to C with coalesced 16-byte accesses (beta = 1 adds to C; those C
+//     values are loaded before the staging).
 // Every mbarrier wait is bounded (tcgen05_ptx.cuh); a wait that gives up
 // raises the CTA's abort flag, the roles leave their loops, TMA copies in
 // flight get 200 us to land, the MMA issuer drains, TMEM is freed and the
@@ -204,15 +208,16 @@ constexpr int OZ_THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
 constexpr int OZ_EPI_WARPS = 8;
 constexpr int OZ_A_BYTES = 128 * 128;  // 128 rows x 128 digit bytes
 constexpr int OZ_B_BYTES = 64 * 128;   // this CTA's half of the 128 B rows
-constexpr int OZ_RA = 9;               // A ring slots (>= s + 1: the next block's first planes load early)
-constexpr int OZ_RB = 6;               // B ring slots
+constexpr int OZ_RA = 8;               // A ring slots (>= s + 1: the next block's first planes load early)
+constexpr int OZ_RB = 9;               // B ring slots (the same, one plane of B each)
 constexpr int OZ_NACC = 4;             // int32 accumulators of 128 TMEM columns
 constexpr int OZ_TMEM_COLS = OZ_NACC * 128;
-constexpr int OZ_EPI_BUF = 32 * 128;  // 32 rows x 16 doubles per epilogue warp
+constexpr int OZ_EPI_BUF = 32 * 64;   // 32 rows x 8 doubles per epilogue warp
 constexpr int OZ_SMEM_BYTES =
     1024 + OZ_RA * OZ_A_BYTES + OZ_RB * OZ_B_BYTES + OZ_EPI_WARPS * OZ_EPI_BUF + 512;
 static_assert(OZ_SMEM_BYTES <= 232448, "shared memory of the int8 GEMM exceeds the per-CTA limit");
-static_assert(OZ_RA >= OZ_MAX_SLICES + 1, "the A ring must hold one block's planes plus one");
+static_assert(OZ_RA >= OZ_MAX_SLICES + 1 && OZ_RB >= OZ_MAX_SLICES + 1,
+              "the rings must hold one block's planes plus one");
 // D = S32, A and B signed 8-bit, K-major, N = 128, M = 256 (CTA pair)
 constexpr uint32_t OZ_IDESC =
     (2u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((256u >> 4) << 24);
@@ -256,17 +261,14 @@ __device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t adesc, uin
         "l"(adesc), "l"(bdesc), "r"(OZ_IDESC), "r"(accumulate));
 }
 
-__device__ __forceinline__ void tmem_ld16_i(uint32_t taddr, int32_t *v)
+__device__ __forceinline__ void tmem_ld8_i(uint32_t taddr, int32_t *v)
 {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
 #pragma unroll
-    for (int j = 0; j < 16; ++j)
+    for (int j = 0; j < 8; ++j)
     {
         v[j] = static_cast<int32_t>(r[j]);
     }
@@ -401,7 +403,6 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                                              g);
                             ++na;
                         }
-                        for (int q = g; q >= 0; --q)  // pairs (g - q, q): B plane q
                         {
                             const int slot = nb % OZ_RB;
                             if (!mbar_wait(&bempty[slot], ((nb / OZ_RB) & 1u) ^ 1u, abort_flag))
@@ -414,7 +415,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                                 mbar_expect_tx(&bfull[slot], 2 * OZ_B_BYTES);
                             }
                             tma_load_3d_pair(bring + slot * OZ_B_BYTES, &tmB, map_to_rank(&bfull[slot], 0), xb, brow,
-                                             q);
+                                             g);
                             ++nb;
                         }
                     }
@@ -441,47 +442,32 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             {
                 for (int kb = 0; ok && kb < p.nkb; ++kb)
                 {
-                    const int abase = na;
+                    const int abase = na, bbase = nb;
                     for (int g = 0; ok && g < G; ++g)
                     {
                         const int u = nu % OZ_NACC;
-                        if (!mbar_wait(&tempty[u], ((nu / OZ_NACC) & 1u) ^ 1u, abort_flag))
+                        // group g needs planes A_g and B_g next (planes below g arrived for earlier groups)
+                        const int ai = abase + g, bi = bbase + g;
+                        if (!mbar_wait(&tempty[u], ((nu / OZ_NACC) & 1u) ^ 1u, abort_flag) ||
+                            !mbar_wait(&afull[ai % OZ_RA], (ai / OZ_RA) & 1u, abort_flag) ||
+                            !mbar_wait(&bfull[bi % OZ_RB], (bi / OZ_RB) & 1u, abort_flag))
                         {
                             ok = false;
                             break;
                         }
                         tc_fence_after();
                         const uint32_t d = tmem_base + static_cast<uint32_t>(u * 128);
-                        for (int pa = 0; pa <= g; ++pa)  // A plane pa, B plane g - pa (the producer's order)
+                        for (int pa = 0; pa <= g; ++pa)  // A plane pa against B plane g - pa
                         {
-                            const int ai = abase + pa;
-                            const int aslot = ai % OZ_RA;
-                            if (pa == g && !mbar_wait(&afull[aslot], (ai / OZ_RA) & 1u, abort_flag))
-                            {
-                                ok = false;
-                                break;
-                            }
-                            const int bslot = nb % OZ_RB;
-                            if (!mbar_wait(&bfull[bslot], (nb / OZ_RB) & 1u, abort_flag))
-                            {
-                                ok = false;
-                                break;
-                            }
-                            tc_fence_after();
-                            const uint64_t adesc = sw128_desc(smem_u32(aring + aslot * OZ_A_BYTES));
-                            const uint64_t bdesc = sw128_desc(smem_u32(bring + bslot * OZ_B_BYTES));
+                            const uint64_t adesc = sw128_desc(smem_u32(aring + ((abase + pa) % OZ_RA) * OZ_A_BYTES));
+                            const uint64_t bdesc =
+                                sw128_desc(smem_u32(bring + ((bbase + g - pa) % OZ_RB) * OZ_B_BYTES));
 #pragma unroll
                             for (int kk = 0; kk < 4; ++kk)
                             {
                                 // 32 bytes of K per instruction: advance the start address by 2 x 16 B
                                 mma_i8_pair(d, adesc + 2 * kk, bdesc + 2 * kk, (pa | kk) != 0 ? 1u : 0u);
                             }
-                            mma_commit_pair_both(&bempty[bslot]);
-                            ++nb;
-                        }
-                        if (!ok)
-                        {
-                            break;
                         }
                         mma_commit_pair_both(&tfull[u]);
                         ++nu;
@@ -490,11 +476,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     {
                         break;
                     }
+                    // the block's planes are free once its last group's MMAs complete
                     for (int pa = 0; pa < G; ++pa)
                     {
                         mma_commit_pair_both(&aempty[(abase + pa) % OZ_RA]);
+                        mma_commit_pair_both(&bempty[(bbase + pa) % OZ_RB]);
                     }
                     na += G;
+                    nb += G;
                 }
             }
             // drain: arrives once every MMA issued above has completed
@@ -509,7 +498,6 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const int q = warp & 3;  // TMEM lane quarter this warp may access
         const int h = ew >> 2;   // column half
         uint8_t *buf = epi + ew * OZ_EPI_BUF;
-        const uint32_t buf_s = smem_u32(buf);
         int nu = 0;
         bool ok = true;
         for (int t = pair; ok && t < p.ntiles; t += npairs)
@@ -527,73 +515,111 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             {
                 acc[j] = 0.0;
             }
+            int ea_next = earow[0], eb_next = ebblk[0];
             for (int kb = 0; ok && kb < p.nkb; ++kb)
             {
-                const int ea = earow[kb];
-                const int eb = ebblk[kb];
-                const bool bad = ea == OZ_BAD_EXP || eb == OZ_BAD_EXP;
-                for (int g = 0; g < G; ++g)
+                const int ea = ea_next;
+                const int eb = eb_next;
+                if (kb + 1 < p.nkb)
                 {
-                    const int u = nu % OZ_NACC;
-                    if (!mbar_wait(&tfull[u], (nu / OZ_NACC) & 1u, abort_flag))
+                    // the next block's exponents load while this block's groups are read
+                    ea_next = earow[kb + 1];
+                    eb_next = ebblk[kb + 1];
+                }
+                const bool bad = ea == OZ_BAD_EXP || eb == OZ_BAD_EXP;
+                // groups in pairs (g, g + 1): 128 P_g + P_{g+1} is exact in int32
+                // (|P_g| <= 7 * 2^19), so one conversion and one FMA serve both
+                for (int g = 0; g < G; g += 2)
+                {
+                    const bool two = g + 1 < G;
+                    const int u0 = nu % OZ_NACC;
+                    const int u1 = (nu + 1) % OZ_NACC;
+                    if (!mbar_wait(&tfull[u0], (nu / OZ_NACC) & 1u, abort_flag) ||
+                        (two && !mbar_wait(&tfull[u1], ((nu + 1) / OZ_NACC) & 1u, abort_flag)))
                     {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t taddr = tmem_base + (static_cast<uint32_t>(q * 32) << 16) +
-                                           static_cast<uint32_t>(u * 128 + h * 64);
-                    const double sc = bad ? __longlong_as_double(0x7ff8000000000000ll) : pow2(ea + eb - 12 - 7 * g);
-                    // 16 columns at a time (the 64 FP64 accumulators already take 128 registers)
+                    const uint32_t lane_base = tmem_base + (static_cast<uint32_t>(q * 32) << 16) +
+                                               static_cast<uint32_t>(h * 64);
+                    const uint32_t t0 = lane_base + static_cast<uint32_t>(u0 * 128);
+                    const uint32_t t1 = lane_base + static_cast<uint32_t>(u1 * 128);
+                    // a last unpaired group counts as 128 P_g + 0 at the pair's scale (the same value)
+                    const double sc = bad ? __longlong_as_double(0x7ff8000000000000ll) : pow2(ea + eb - 12 - 7 * (g + 1));
+                    // 8 columns of each group at a time (10 warps on 4 sub-partitions leave
+                    // 168 registers a thread; the 64 FP64 accumulators take 128)
 #pragma unroll
-                    for (int c = 0; c < 4; ++c)
+                    for (int c = 0; c < 8; ++c)
                     {
-                        int32_t v[16];
-                        tmem_ld16_i(taddr + c * 16, v);
-                        tmem_ld_wait();
-                        if (c == 3)
+                        int32_t v[8], w[8];
+                        tmem_ld8_i(t0 + c * 8, v);
+                        if (two)
                         {
-                            // the accumulator is read: the MMA warp may reuse it
+                            tmem_ld8_i(t1 + c * 8, w);
+                        }
+                        else
+                        {
+#pragma unroll
+                            for (int j = 0; j < 8; ++j)
+                            {
+                                w[j] = 0;
+                            }
+                        }
+                        tmem_ld_wait();
+                        if (c == 7)
+                        {
+                            // both accumulators are read: the MMA warp may reuse them
                             tc_fence_before();
                             __syncwarp();
                             if (lane == 0)
                             {
-                                mbar_arrive_cluster(map_to_rank(&tempty[u], 0));
+                                mbar_arrive_remote(map_to_rank(&tempty[u0], 0));
+                                if (two)
+                                {
+                                    mbar_arrive_remote(map_to_rank(&tempty[u1], 0));
+                                }
                             }
                         }
 #pragma unroll
-                        for (int j = 0; j < 16; ++j)
+                        for (int j = 0; j < 8; ++j)
                         {
-                            acc[c * 16 + j] = fma(i2d(v[j]), sc, acc[c * 16 + j]);
+                            acc[c * 8 + j] = fma(i2d(v[j] * 128 + w[j]), sc, acc[c * 8 + j]);
                         }
                     }
-                    ++nu;
+                    nu += two ? 2 : 1;
                 }
             }
             if (!ok)
             {
                 break;
             }
-            // ---- write alpha * acc: 4 chunks of 32 rows x 16 columns per warp ----
+            // ---- write alpha * acc: 8 chunks of 32 rows x 8 columns per warp ----
+            // A lane holds one row; the chunk is transposed through shared memory
+            // (16-byte units swizzled by (row >> 1) & 3, conflict-free both ways)
+            // so that 4 lanes write 64 contiguous bytes of one row.  With beta = 1
+            // the chunk's C values are loaded before the staging, so their
+            // latency overlaps it.
             double sq = 0.0;
+            double2 *buf2 = reinterpret_cast<double2 *>(buf);
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+            for (int c = 0; c < 8; ++c)
             {
-                const int col0 = n0 + h * 64 + c * 16;
+                const int col0 = n0 + h * 64 + c * 8;
                 // warp-uniform: chunk right of C, below C, or (lower) above the diagonal for all rows
                 if (col0 >= p.N || row0w >= p.M || (p.lower && col0 > row0w + 31))
                 {
                     continue;
                 }
+                const int uu = lane & 3;
+                const int gc = col0 + 2 * uu;
                 __syncwarp();
 #pragma unroll
-                for (int j = 0; j < 8; ++j)
+                for (int j = 0; j < 4; ++j)
                 {
-                    const double x = p.alpha * acc[c * 16 + 2 * j];
-                    const double y = p.alpha * acc[c * 16 + 2 * j + 1];
-                    const uint32_t addr = buf_s + static_cast<uint32_t>(lane) * 128u +
-                                          (static_cast<uint32_t>(j ^ (lane & 7)) << 4);
-                    asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(x), "d"(y) : "memory");
+                    const double x = p.alpha * acc[c * 8 + 2 * j];
+                    const double y = p.alpha * acc[c * 8 + 2 * j + 1];
+                    buf2[lane * 4 + (j ^ ((lane >> 1) & 3))] = make_double2(x, y);
                     if (p.rowsq != nullptr && rvalid)
                     {
                         if (col0 + 2 * j < p.N)
@@ -608,26 +634,21 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 }
                 __syncwarp();
 #pragma unroll
-                for (int it = 0; it < 8; ++it)
+                for (int it = 0; it < 4; ++it)
                 {
-                    const int r = it * 4 + (lane >> 3);
-                    const int uu = lane & 7;
+                    const int r = it * 8 + (lane >> 2);
                     const int grow = row0w + r;
                     if (grow >= p.M)
                     {
                         continue;
                     }
-                    double x, y;
-                    const uint32_t addr =
-                        buf_s + static_cast<uint32_t>(r) * 128u + (static_cast<uint32_t>(uu ^ (r & 7)) << 4);
-                    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "r"(addr) : "memory");
-                    const int gc = col0 + 2 * uu;
+                    const double2 v = buf2[r * 4 + (uu ^ ((r >> 1) & 3))];
                     double *dst = p.C + static_cast<int64_t>(grow) * p.ldc + gc;
                     const bool ok0 = gc < p.N && (!p.lower || gc <= grow);
                     const bool ok1 = gc + 1 < p.N && (!p.lower || gc + 1 <= grow);
                     if (ok0 && ok1)
                     {
-                        double2 o = make_double2(x, y);
+                        double2 o = v;
                         if (p.beta)
                         {
                             const double2 c0 = *reinterpret_cast<const double2 *>(dst);
@@ -636,16 +657,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                         }
                         *reinterpret_cast<double2 *>(dst) = o;
                     }
-                    else
+                    else if (ok0)
                     {
-                        if (ok0)
-                        {
-                            dst[0] = p.beta ? dst[0] + x : x;
-                        }
-                        if (ok1)
-                        {
-                            dst[1] = p.beta ? dst[1] + y : y;
-                        }
+                        dst[0] = p.beta ? dst[0] + v.x : v.x;
                     }
                 }
             }

@@ -16,9 +16,10 @@
 //     2^(eA + eB - 12) * sum_{g < G} 2^(-7 g) * P_g,
 //     P_g = sum_{p + q = g} D^A_p (D^B_q)^T          (exact in int32)
 // and the G = s groups of one block form one unit of int32 accumulation in
-// tensor memory (tcgen05.mma kind::i8); the epilogue converts each unit
-// exactly to FP64 and accumulates it with its scale, so the only roundings
-// are the digit truncation and FP64 additions.
+// tensor memory (tcgen05.mma kind::i8) each; the epilogue combines two
+// groups exactly in int32 (128 P_g + P_{g+1}), converts the sum exactly to
+// FP64 and accumulates it with its scale, so the only roundings are the
+// digit truncation and FP64 additions.
 #pragma once
 
 #include "common.cuh"
@@ -30,7 +31,7 @@ namespace gprat_cu
 
 constexpr int OZ_KB = 128;  // columns per exponent block = digit bytes per TMA box row
 constexpr int OZ_MIN_SLICES = 3;
-constexpr int OZ_MAX_SLICES = 8;
+constexpr int OZ_MAX_SLICES = 7;
 
 struct OzOperand
 {

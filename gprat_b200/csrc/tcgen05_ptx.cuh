@@ -130,6 +130,14 @@ __device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr)
     asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
 }
 
+// arrive on a barrier of either CTA of the pair with the default
+// (release, CTA scope) semantics; ordering of tensor-memory reads against a
+// later MMA comes from tcgen05.fence::before_thread_sync before it
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr)
+{
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
 // arrives on the barrier at the same offset in both CTAs of the pair once
 // every tcgen05 operation this thread issued before has completed
 __device__ __forceinline__ void mma_commit_pair_both(uint64_t *bar)

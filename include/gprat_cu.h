@@ -91,7 +91,7 @@ int gprat_cu_gp_set_precision(gprat_cu_gp *gp, int precision);
 
 /*
  * Digit planes of the int8-emulated FP64 products (GPRAT_CU_PREC_FP64_INT8),
- * 3 <= slices <= 8, default 6.  Each operand keeps 6 + 7 (slices - 1) bits
+ * 3 <= slices <= 7, default 6.  Each operand keeps 6 + 7 (slices - 1) bits
  * relative to the largest entry of its 128-column block; a product costs
  * slices * (slices + 1) / 2 int8 tensor-core passes.  No counterpart in the
  * reference (whose GPU path is FP64 cuBLAS/cuSOLVER only).
@@ -329,7 +329,7 @@ int gprat_cu_test_set_wait_budget(int64_t polls);
  * one exponent e per row and 128-column block (block = 0) or per 128 x 128
  * block (block != 0).  digits: s * rows * cols bytes (plane-major);
  * exps: rows * (cols / 128) (or ceil(rows / 128) * (cols / 128)) ints.
- * 3 <= s <= 8.
+ * 3 <= s <= 7.
  */
 int gprat_cu_test_oz_split(int rows, int cols, const double *src, int s, int block, int8_t *digits, int32_t *exps);
 

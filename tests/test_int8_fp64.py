@@ -120,5 +120,5 @@ def test_slices_rejected(capi):
     with pytest.raises(capi.GpratCudaError):
         gp.set_int8_slices(2)
     with pytest.raises(capi.GpratCudaError):
-        gp.set_int8_slices(9)
+        gp.set_int8_slices(8)
     gp.close()

@@ -143,7 +143,9 @@ def test_failed_copy_frees_every_replica(serving):
         assert ms.resident_bytes() == before
         _, _, gid, _ = ms.wait(ms.submit_fit(fx, fy, 8, 128, 8, hyper))
         assert all(b > a for a, b in zip(before, ms.resident_bytes()))
-        results = [ms.wait(ms.submit_predict(gid, series, 50)) for _ in range(4)]
+        # submitted together, so the outstanding-points routing spreads them over both replicas
+        tickets = [ms.submit_predict(gid, series, 50) for _ in range(4)]
+        results = [ms.wait(t) for t in tickets]
         assert min(ms.replica_completed()) > 0
     om, ov = O.OracleGP(fx, fy, 8, 128, 8, hyper).predict_with_uncertainty(series, 1, 50)
     for mean, var, got, _ in results:
