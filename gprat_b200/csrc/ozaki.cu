@@ -10,21 +10,24 @@
 // t <- (t - d) * 128 is exact, so D_0 .. D_{s-1} are the leading s balanced
 // base-128 digits of x * 2^(6 - e).
 //
-// oz_gemm_kernel: persistent, warp-specialised CTA pair (cluster of 2, 320
+// oz_gemm_kernel: persistent, warp-specialised CTA pair (cluster of 2, 384
 // threads each), one 256 x 128 output tile per pair at a time:
 //   warp 0, one lane (both CTAs): TMA producer.  For each 128-column block k
 //     and group g it loads digit plane g of A (this CTA's 128 rows, 16 KB)
-//     and of B (this CTA's 64 rows, 8 KB) into rings of OZ_RA and OZ_RB
-//     slots.  A block's planes stay resident until its last group, so every
-//     digit tile crosses from L2 once per block; the spare slots let the next
-//     block's first planes load while the current block's last groups run.
+//     and of B (this CTA's 64 rows, 8 KB) into one slot of a ring of
+//     OZ_RING, both counted by the slot's one barrier.  A block's planes stay
+//     resident until its last group, so every digit tile crosses from L2
+//     once per block; the spare slots let the next block's first planes load
+//     while the current block's last groups run.
 //   warp 1, one lane (leader): MMA issuer.  Group g of block k is one unit:
 //     for p = 0..g, four tcgen05.mma.cta_group::2.kind::i8 (M 256, N 128,
 //     K 32) of A_p against B_{g-p} into one int32 accumulator in tensor
 //     memory (four accumulators of 128 columns rotate); tcgen05.commit frees
-//     the accumulator, and after the block's last group its A and B slots.
-//   warps 2..9 (both CTAs): epilogue.  Two warps per TMEM lane quarter, 64
-//     columns each; units are read with tcgen05.ld in pairs of groups
+//     the accumulator, and after the block's last group its slots.  The
+//     issuing thread waits as little as it can (see the issuer below).
+//   warps 4..11 (both CTAs): epilogue.  Two warps per TMEM lane quarter, 64
+//     columns each (224 registers after setmaxnreg); units are read with
+//     double-buffered tcgen05.ld, 16 columns at a time, in pairs of groups
 //     (g, g + 1) and combined exactly in int32 as 128 P_g + P_{g+1}
 //     (|P_g| <= 7 * 2^19), converted exactly to FP64 (2^52 + 2^31 bias
 //     trick) and added with the pair's scale 2^(eA + eB - 12 - 7 (g + 1))
@@ -204,20 +207,26 @@ __global__ void __launch_bounds__(SPLIT_THREADS) oz_split_kernel(const double *_
 // ---------------------------------------------------------------------------
 // GEMM
 
-constexpr int OZ_THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
+// warpgroup 0: warp 0 TMA, warp 1 MMA (warps 2, 3 idle); warpgroups 1 and 2
+// (warps 4..11): epilogue.  The kernel launches with 168 registers a thread;
+// warpgroup 0 gives registers up (setmaxnreg) so that each epilogue thread
+// holds 224: 128 * 56 + 256 * 224 = 384 * 168.
+constexpr int OZ_THREADS = 384;
+constexpr int OZ_REGS_PRODUCER = 56;
+constexpr int OZ_REGS_EPILOGUE = 224;
+static_assert(128 * OZ_REGS_PRODUCER + 256 * OZ_REGS_EPILOGUE <= OZ_THREADS * 168,
+              "the register split exceeds the registers the block launches with");
 constexpr int OZ_EPI_WARPS = 8;
 constexpr int OZ_A_BYTES = 128 * 128;  // 128 rows x 128 digit bytes
 constexpr int OZ_B_BYTES = 64 * 128;   // this CTA's half of the 128 B rows
-constexpr int OZ_RA = 8;               // A ring slots (>= s + 1: the next block's first planes load early)
-constexpr int OZ_RB = 9;               // B ring slots (the same, one plane of B each)
+constexpr int OZ_RING = 8;  // slots of one A and one B digit plane (>= s + 1: the next block's first planes load early)
 constexpr int OZ_NACC = 4;             // int32 accumulators of 128 TMEM columns
 constexpr int OZ_TMEM_COLS = OZ_NACC * 128;
 constexpr int OZ_EPI_BUF = 32 * 64;   // 32 rows x 8 doubles per epilogue warp
 constexpr int OZ_SMEM_BYTES =
-    1024 + OZ_RA * OZ_A_BYTES + OZ_RB * OZ_B_BYTES + OZ_EPI_WARPS * OZ_EPI_BUF + 512;
+    1024 + OZ_RING * (OZ_A_BYTES + OZ_B_BYTES) + OZ_EPI_WARPS * OZ_EPI_BUF + 512;
 static_assert(OZ_SMEM_BYTES <= 232448, "shared memory of the int8 GEMM exceeds the per-CTA limit");
-static_assert(OZ_RA >= OZ_MAX_SLICES + 1 && OZ_RB >= OZ_MAX_SLICES + 1,
-              "the rings must hold one block's planes plus one");
+static_assert(OZ_RING >= OZ_MAX_SLICES + 1, "the ring must hold one block's planes plus one");
 // D = S32, A and B signed 8-bit, K-major, N = 128, M = 256 (CTA pair)
 constexpr uint32_t OZ_IDESC =
     (2u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((256u >> 4) << 24);
@@ -261,16 +270,31 @@ __device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t adesc, uin
         "l"(adesc), "l"(bdesc), "r"(OZ_IDESC), "r"(accumulate));
 }
 
-__device__ __forceinline__ void tmem_ld8_i(uint32_t taddr, int32_t *v)
+__device__ __forceinline__ void tmem_ld16_i(uint32_t taddr, int32_t *v)
 {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
+    for (int j = 0; j < 16; ++j)
     {
         v[j] = static_cast<int32_t>(r[j]);
+    }
+}
+
+// Ties registers written by tcgen05.ld to the point after tcgen05.wait::ld:
+// an empty volatile asm that reads and writes each one, so that no use is
+// scheduled before the wait.
+__device__ __forceinline__ void regs_loaded(int32_t (&v)[16])
+{
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+    {
+        asm volatile("" : "+r"(v[j]));
     }
 }
 
@@ -315,13 +339,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t *aring = smem;
-    uint8_t *bring = aring + OZ_RA * OZ_A_BYTES;
-    uint8_t *epi = bring + OZ_RB * OZ_B_BYTES;
-    uint64_t *afull = reinterpret_cast<uint64_t *>(epi + OZ_EPI_WARPS * OZ_EPI_BUF);
-    uint64_t *aempty = afull + OZ_RA;
-    uint64_t *bfull = aempty + OZ_RA;
-    uint64_t *bempty = bfull + OZ_RB;
-    uint64_t *tfull = bempty + OZ_RB;
+    uint8_t *bring = aring + OZ_RING * OZ_A_BYTES;
+    uint8_t *epi = bring + OZ_RING * OZ_B_BYTES;
+    uint64_t *full = reinterpret_cast<uint64_t *>(epi + OZ_EPI_WARPS * OZ_EPI_BUF);
+    uint64_t *empty = full + OZ_RING;
+    uint64_t *tfull = empty + OZ_RING;
     uint64_t *tempty = tfull + OZ_NACC;
     uint64_t *drain = tempty + OZ_NACC;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
@@ -337,15 +359,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 
     if (threadIdx.x == 0)
     {
-        for (int i = 0; i < OZ_RA; ++i)
+        for (int i = 0; i < OZ_RING; ++i)
         {
-            mbar_init(&afull[i], 1);
-            mbar_init(&aempty[i], 1);
-        }
-        for (int i = 0; i < OZ_RB; ++i)
-        {
-            mbar_init(&bfull[i], 1);
-            mbar_init(&bempty[i], 1);
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
         }
         for (int u = 0; u < OZ_NACC; ++u)
         {
@@ -367,7 +384,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     pdl_wait();  // the previous kernel's results are visible from here on
-
+    if (warp < 4)
+    {
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(OZ_REGS_PRODUCER));
+    }
     if (warp == 0)
     {
         if (lane == 0)
@@ -375,7 +395,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             // ---------------- TMA producer (both CTAs) ----------------
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
             asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
-            int na = 0, nb = 0;
+            int n = 0;  // digit-plane pairs loaded
             bool ok = true;
             for (int t = pair; ok && t < p.ntiles; t += npairs)
             {
@@ -388,36 +408,21 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     const int xa = p.a_col0 + kb * OZ_KB, xb = p.b_col0 + kb * OZ_KB;
                     for (int g = 0; ok && g < G; ++g)
                     {
+                        // slot n % OZ_RING takes A_g and B_g; one barrier counts both
+                        const int slot = n % OZ_RING;
+                        if (!mbar_wait(&empty[slot], ((n / OZ_RING) & 1u) ^ 1u, abort_flag))
                         {
-                            const int slot = na % OZ_RA;
-                            if (!mbar_wait(&aempty[slot], ((na / OZ_RA) & 1u) ^ 1u, abort_flag))
-                            {
-                                ok = false;
-                                break;
-                            }
-                            if (leader)
-                            {
-                                mbar_expect_tx(&afull[slot], 2 * OZ_A_BYTES);  // both CTAs' bytes
-                            }
-                            tma_load_3d_pair(aring + slot * OZ_A_BYTES, &tmA, map_to_rank(&afull[slot], 0), xa, arow,
-                                             g);
-                            ++na;
+                            ok = false;
+                            break;
                         }
+                        if (leader)
                         {
-                            const int slot = nb % OZ_RB;
-                            if (!mbar_wait(&bempty[slot], ((nb / OZ_RB) & 1u) ^ 1u, abort_flag))
-                            {
-                                ok = false;
-                                break;
-                            }
-                            if (leader)
-                            {
-                                mbar_expect_tx(&bfull[slot], 2 * OZ_B_BYTES);
-                            }
-                            tma_load_3d_pair(bring + slot * OZ_B_BYTES, &tmB, map_to_rank(&bfull[slot], 0), xb, brow,
-                                             g);
-                            ++nb;
+                            mbar_expect_tx(&full[slot], 2 * (OZ_A_BYTES + OZ_B_BYTES));  // both CTAs' bytes
                         }
+                        const uint32_t bar = map_to_rank(&full[slot], 0);
+                        tma_load_3d_pair(aring + slot * OZ_A_BYTES, &tmA, bar, xa, arow, g);
+                        tma_load_3d_pair(bring + slot * OZ_B_BYTES, &tmB, bar, xb, brow, g);
+                        ++n;
                     }
                 }
             }
@@ -436,38 +441,56 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         if (lane == 0 && leader)
         {
             // ---------------- MMA issuer (leader only) ----------------
-            int na = 0, nb = 0, nu = 0;
+            // The issuing thread runs in step with the tensor core (an MMA issue
+            // returns about when the previous one completes), and an mbarrier
+            // wait in this thread leaves the tensor core idle for a while even
+            // when the phase has already completed.  So the thread waits as
+            // little as it can: one barrier per digit-plane slot (A_g and B_g
+            // together), and an accumulator wait only for a group whose
+            // accumulator was last read as the first of an epilogue pair (the
+            // epilogue frees both accumulators of a pair after reading both).
+            // Descriptors advance from the ring bases (a slot is OZ_A_BYTES / 16
+            // or OZ_B_BYTES / 16 units of the descriptor's address field).
+            const uint64_t adesc0 = sw128_desc(smem_u32(aring));
+            const uint64_t bdesc0 = sw128_desc(smem_u32(bring));
+            int n = 0, nu = 0;
+            unsigned pair_first = 0;  // bit u: the group last in accumulator u opened an epilogue pass
             bool ok = true;
             for (int t = pair; ok && t < p.ntiles; t += npairs)
             {
                 for (int kb = 0; ok && kb < p.nkb; ++kb)
                 {
-                    const int abase = na, bbase = nb;
+                    const int s0 = n % OZ_RING;  // slot of this block's plane 0
                     for (int g = 0; ok && g < G; ++g)
                     {
                         const int u = nu % OZ_NACC;
-                        // group g needs planes A_g and B_g next (planes below g arrived for earlier groups)
-                        const int ai = abase + g, bi = bbase + g;
-                        if (!mbar_wait(&tempty[u], ((nu / OZ_NACC) & 1u) ^ 1u, abort_flag) ||
-                            !mbar_wait(&afull[ai % OZ_RA], (ai / OZ_RA) & 1u, abort_flag) ||
-                            !mbar_wait(&bfull[bi % OZ_RB], (bi / OZ_RB) & 1u, abort_flag))
+                        const int ni = n + g;
+                        if ((nu >= OZ_NACC && ((pair_first >> u) & 1u) &&
+                             !mbar_wait(&tempty[u], ((nu / OZ_NACC) & 1u) ^ 1u, abort_flag)) ||
+                            !mbar_wait(&full[ni % OZ_RING], (ni / OZ_RING) & 1u, abort_flag))
                         {
                             ok = false;
                             break;
                         }
                         tc_fence_after();
+                        // groups (0, 1), (2, 3), ... of a block form the epilogue's passes
+                        pair_first = (g % 2 == 0) ? (pair_first | (1u << u)) : (pair_first & ~(1u << u));
                         const uint32_t d = tmem_base + static_cast<uint32_t>(u * 128);
+                        int aslot = s0;  // slot of A_pa
+                        int bslot = s0 + g;  // slot of B_{g-pa}
+                        bslot -= bslot >= OZ_RING ? OZ_RING : 0;
                         for (int pa = 0; pa <= g; ++pa)  // A plane pa against B plane g - pa
                         {
-                            const uint64_t adesc = sw128_desc(smem_u32(aring + ((abase + pa) % OZ_RA) * OZ_A_BYTES));
-                            const uint64_t bdesc =
-                                sw128_desc(smem_u32(bring + ((bbase + g - pa) % OZ_RB) * OZ_B_BYTES));
+                            const uint64_t adesc = adesc0 + static_cast<uint64_t>(aslot * (OZ_A_BYTES >> 4));
+                            const uint64_t bdesc = bdesc0 + static_cast<uint64_t>(bslot * (OZ_B_BYTES >> 4));
 #pragma unroll
                             for (int kk = 0; kk < 4; ++kk)
                             {
                                 // 32 bytes of K per instruction: advance the start address by 2 x 16 B
                                 mma_i8_pair(d, adesc + 2 * kk, bdesc + 2 * kk, (pa | kk) != 0 ? 1u : 0u);
                             }
+                            aslot = aslot + 1 == OZ_RING ? 0 : aslot + 1;
+                            bslot = bslot == 0 ? OZ_RING - 1 : bslot - 1;
                         }
                         mma_commit_pair_both(&tfull[u]);
                         ++nu;
@@ -476,14 +499,13 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     {
                         break;
                     }
-                    // the block's planes are free once its last group's MMAs complete
+                    // the block's slots are free once its last group's MMAs complete
                     for (int pa = 0; pa < G; ++pa)
                     {
-                        mma_commit_pair_both(&aempty[(abase + pa) % OZ_RA]);
-                        mma_commit_pair_both(&bempty[(bbase + pa) % OZ_RB]);
+                        const int sl = s0 + pa;
+                        mma_commit_pair_both(&empty[sl >= OZ_RING ? sl - OZ_RING : sl]);
                     }
-                    na += G;
-                    nb += G;
+                    n += G;
                 }
             }
             // drain: arrives once every MMA issued above has completed
@@ -491,10 +513,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             mbar_wait(drain, 0u, abort_flag);
         }
     }
-    else
+    else if (warp >= 4)
     {
-        // ---------------- epilogue (warps 2..9 of both CTAs) ----------------
-        const int ew = warp - 2;
+        // ---------------- epilogue (warps 4..11 of both CTAs) ----------------
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(OZ_REGS_EPILOGUE));
+        const int ew = warp - 4;
         const int q = warp & 3;  // TMEM lane quarter this warp may access
         const int h = ew >> 2;   // column half
         uint8_t *buf = epi + ew * OZ_EPI_BUF;
@@ -547,27 +570,30 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     const uint32_t t1 = lane_base + static_cast<uint32_t>(u1 * 128);
                     // a last unpaired group counts as 128 P_g + 0 at the pair's scale (the same value)
                     const double sc = bad ? __longlong_as_double(0x7ff8000000000000ll) : pow2(ea + eb - 12 - 7 * (g + 1));
-                    // 8 columns of each group at a time (10 warps on 4 sub-partitions leave
-                    // 168 registers a thread; the 64 FP64 accumulators take 128)
-#pragma unroll
-                    for (int c = 0; c < 8; ++c)
+                    // 16 columns of each group at a time, double-buffered: the next
+                    // chunk's tensor-memory loads are in flight while this chunk converts
+                    auto chunk = [&](int32_t(&v)[16], int32_t(&w)[16], int32_t(&vn)[16], int32_t(&wn)[16], int c)
                     {
-                        int32_t v[8], w[8];
-                        tmem_ld8_i(t0 + c * 8, v);
-                        if (two)
+                        tmem_ld_wait();
+                        regs_loaded(v);
+                        regs_loaded(w);
+                        if (c < 3)
                         {
-                            tmem_ld8_i(t1 + c * 8, w);
-                        }
-                        else
-                        {
-#pragma unroll
-                            for (int j = 0; j < 8; ++j)
+                            tmem_ld16_i(t0 + (c + 1) * 16, vn);
+                            if (two)
                             {
-                                w[j] = 0;
+                                tmem_ld16_i(t1 + (c + 1) * 16, wn);
+                            }
+                            else
+                            {
+#pragma unroll
+                                for (int k = 0; k < 16; ++k)
+                                {
+                                    wn[k] = 0;
+                                }
                             }
                         }
-                        tmem_ld_wait();
-                        if (c == 7)
+                        else
                         {
                             // both accumulators are read: the MMA warp may reuse them
                             tc_fence_before();
@@ -582,11 +608,29 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                             }
                         }
 #pragma unroll
-                        for (int j = 0; j < 8; ++j)
+                        for (int k = 0; k < 16; ++k)
                         {
-                            acc[c * 8 + j] = fma(i2d(v[j] * 128 + w[j]), sc, acc[c * 8 + j]);
+                            acc[c * 16 + k] = fma(i2d(v[k] * 128 + w[k]), sc, acc[c * 16 + k]);
+                        }
+                    };
+                    int32_t va[16], wa[16], vb[16], wb[16];
+                    tmem_ld16_i(t0, va);
+                    if (two)
+                    {
+                        tmem_ld16_i(t1, wa);
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int k = 0; k < 16; ++k)
+                        {
+                            wa[k] = 0;
                         }
                     }
+                    chunk(va, wa, vb, wb, 0);
+                    chunk(vb, wb, va, wa, 1);
+                    chunk(va, wa, vb, wb, 2);
+                    chunk(vb, wb, va, wa, 3);
                     nu += two ? 2 : 1;
                 }
             }

@@ -56,10 +56,31 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
+// non-blocking test of the phase with the given parity
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // Bounded wait for the phase with the given parity; false if it gave up
 // (or another role already aborted).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag)
 {
+    // fast path: a phase that has already completed costs one non-blocking
+    // test (cheaper for a thread that issues tensor-core MMAs than a
+    // try_wait); the timer is read only once the wait has to spin
+    if (mbar_test_wait(bar, parity))
+    {
+        return true;
+    }
     const unsigned long long t0 = global_ns();
     for (uint32_t i = 0;; ++i)
     {
