@@ -19,12 +19,13 @@
 //     resident until its last group, so every digit tile crosses from L2
 //     once per block; the spare slots let the next block's first planes load
 //     while the current block's last groups run.
-//   warp 1, one lane (leader): MMA issuer.  Group g of block k is one unit:
+//   warps 1 and 2, one lane each (leader): MMA issuers, taking alternate
+//     groups so that one thread's barrier waits do not idle the tensor core
+//     (the issuer below says why).  Group g of block k is one unit:
 //     for p = 0..g, four tcgen05.mma.cta_group::2.kind::i8 (M 256, N 128,
 //     K 32) of A_p against B_{g-p} into one int32 accumulator in tensor
 //     memory (four accumulators of 128 columns rotate); tcgen05.commit frees
-//     the accumulator, and after the block's last group its slots.  The
-//     issuing thread waits as little as it can (see the issuer below).
+//     the accumulator, and after the block (from both issuers) its slots.
 //   warps 4..11 (both CTAs): epilogue.  Two warps per TMEM lane quarter, 64
 //     columns each (224 registers after setmaxnreg); units are read with
 //     double-buffered tcgen05.ld, 16 columns at a time, in pairs of groups
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS) oz_split_kernel(const double *_
 // ---------------------------------------------------------------------------
 // GEMM
 
-// warpgroup 0: warp 0 TMA, warp 1 MMA (warps 2, 3 idle); warpgroups 1 and 2
+// warpgroup 0: warp 0 TMA, warps 1 and 2 MMA (warp 3 idle); warpgroups 1 and 2
 // (warps 4..11): epilogue.  The kernel launches with 168 registers a thread;
 // warpgroup 0 gives registers up (setmaxnreg) so that each epilogue thread
 // holds 224: 128 * 56 + 256 * 224 = 384 * 168.
@@ -362,14 +363,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         for (int i = 0; i < OZ_RING; ++i)
         {
             mbar_init(&full[i], 1);
-            mbar_init(&empty[i], 1);
+            mbar_init(&empty[i], 2);  // one commit from each MMA issuer
         }
         for (int u = 0; u < OZ_NACC; ++u)
         {
             mbar_init(&tfull[u], 1);
             mbar_init(&tempty[u], 2 * OZ_EPI_WARPS);
         }
-        mbar_init(drain, 1);
+        mbar_init(drain, 2);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -436,47 +437,60 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             }
         }
     }
-    else if (warp == 1)
+    else if (warp == 1 || warp == 2)
     {
         if (lane == 0 && leader)
         {
-            // ---------------- MMA issuer (leader only) ----------------
-            // The issuing thread runs in step with the tensor core (an MMA issue
-            // returns about when the previous one completes), and an mbarrier
-            // wait in this thread leaves the tensor core idle for a while even
-            // when the phase has already completed.  So the thread waits as
-            // little as it can: one barrier per digit-plane slot (A_g and B_g
-            // together), and an accumulator wait only for a group whose
-            // accumulator was last read as the first of an epilogue pair (the
-            // epilogue frees both accumulators of a pair after reading both).
-            // Descriptors advance from the ring bases (a slot is OZ_A_BYTES / 16
-            // or OZ_B_BYTES / 16 units of the descriptor's address field).
+            // ---------------- MMA issuers (leader only, two threads) ----------------
+            // An issuing thread runs in step with the tensor core (an MMA issue
+            // returns about when the previous one completes), and a barrier
+            // test in that thread costs a shared-memory round trip, which is
+            // slow while the tensor core streams its operands; the tensor core
+            // would sit idle for it.  Two threads (warps 1 and 2) therefore
+            // issue: groups of even global index from one, odd from the other
+            // (so each owns two of the four accumulators), and while one waits
+            // the other's MMAs keep the tensor core busy.  Before a group a
+            // thread waits for its accumulator and for the digit planes of
+            // the block it has not seen yet; after the block both threads
+            // commit to each slot's empty barrier (count 2).  Descriptors
+            // advance from the ring bases (a slot is OZ_A_BYTES / 16 or
+            // OZ_B_BYTES / 16 units of the descriptor's address field).
+            const int me = warp - 1;
             const uint64_t adesc0 = sw128_desc(smem_u32(aring));
             const uint64_t bdesc0 = sw128_desc(smem_u32(bring));
             int n = 0, nu = 0;
-            unsigned pair_first = 0;  // bit u: the group last in accumulator u opened an epilogue pass
             bool ok = true;
             for (int t = pair; ok && t < p.ntiles; t += npairs)
             {
                 for (int kb = 0; ok && kb < p.nkb; ++kb)
                 {
                     const int s0 = n % OZ_RING;  // slot of this block's plane 0
-                    for (int g = 0; ok && g < G; ++g)
+                    int seen = -1;               // planes of this block this thread has waited for
+                    for (int g = 0; ok && g < G; ++g, ++nu)
                     {
+                        if ((nu & 1) != me)
+                        {
+                            continue;
+                        }
                         const int u = nu % OZ_NACC;
-                        const int ni = n + g;
-                        if ((nu >= OZ_NACC && ((pair_first >> u) & 1u) &&
-                             !mbar_wait(&tempty[u], ((nu / OZ_NACC) & 1u) ^ 1u, abort_flag)) ||
-                            !mbar_wait(&full[ni % OZ_RING], (ni / OZ_RING) & 1u, abort_flag))
+                        if (nu >= OZ_NACC && !mbar_wait(&tempty[u], ((nu / OZ_NACC) & 1u) ^ 1u, abort_flag))
                         {
                             ok = false;
                             break;
                         }
+                        for (int pl = seen + 1; ok && pl <= g; ++pl)
+                        {
+                            const int ni = n + pl;
+                            ok = mbar_wait(&full[ni % OZ_RING], (ni / OZ_RING) & 1u, abort_flag);
+                        }
+                        if (!ok)
+                        {
+                            break;
+                        }
+                        seen = g;
                         tc_fence_after();
-                        // groups (0, 1), (2, 3), ... of a block form the epilogue's passes
-                        pair_first = (g % 2 == 0) ? (pair_first | (1u << u)) : (pair_first & ~(1u << u));
                         const uint32_t d = tmem_base + static_cast<uint32_t>(u * 128);
-                        int aslot = s0;  // slot of A_pa
+                        int aslot = s0;      // slot of A_pa
                         int bslot = s0 + g;  // slot of B_{g-pa}
                         bslot -= bslot >= OZ_RING ? OZ_RING : 0;
                         for (int pa = 0; pa <= g; ++pa)  // A plane pa against B plane g - pa
@@ -493,13 +507,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                             bslot = bslot == 0 ? OZ_RING - 1 : bslot - 1;
                         }
                         mma_commit_pair_both(&tfull[u]);
-                        ++nu;
                     }
                     if (!ok)
                     {
                         break;
                     }
-                    // the block's slots are free once its last group's MMAs complete
+                    // a slot is free once both threads' MMAs of this block complete
                     for (int pa = 0; pa < G; ++pa)
                     {
                         const int sl = s0 + pa;
@@ -508,7 +521,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     n += G;
                 }
             }
-            // drain: arrives once every MMA issued above has completed
+            // drain (count 2): completes once every MMA both threads issued has completed
             mma_commit_pair_local(drain);
             mbar_wait(drain, 0u, abort_flag);
         }
