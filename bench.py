@@ -6,12 +6,14 @@ lengthscale=4.0, vertical_lengthscale=1.0, noise_variance=0.01, seeded
 synthetic series (x ~ N(0,1), y_i = sum_j sin(X_ij)/8 + N(0, 0.01^2)).
 One step = SE assembly of K + Cholesky + alpha solves + predictive mean
 (cross covariance . alpha) + per-point variance (K* L^-T row sums).  The
-default precision is mixed-tf32 (TF32 tensor-core trailing updates, FP64
-diagonal blocks and FP64-refined alpha); the same run also times the plain
-FP64 path on the same inputs ("fp64"), reports the mixed results' error
-against it, and runs the serving stream ("serving": four resident models,
-Poisson requests, p50/p99 latency).  K alone is 8.6 GB (> L2), so no L2 flush
-is needed between steps.
+default precision is fp64-int8: every product of the factorisation and of
+the variance solve emulated in FP64 on the int8 tensor cores (5 digit
+planes), FP64 diagonal blocks and triangular solves.  The same run times the
+plain FP64 path on the same inputs ("fp64") and reports the headline mode's
+error against it, times the other modes ("arms": 4 digit planes, TF32,
+BF16) with their errors, and runs the serving stream ("serving": four
+resident models, Poisson requests, p50/p99 latency).  K alone is 8.6 GB
+(> L2), so no L2 flush is needed between steps.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -311,7 +313,45 @@ def cpu_reference_calls(wl, reps: int = 3):
     }
 
 
-def gpu_calls(wl, precision: int, reps: int = 3):
+# Hyper-parameter optimisation at its own configuration (the adjoint path):
+# n_train=8192, d=8, initial (lengthscale, vertical lengthscale, noise) =
+# (0.5, 2.0, 0.5), 50 Adam steps at lr=0.1, beta1=0.9, beta2=0.999, FP64.
+C3 = dict(n=8192, d=8, T=512, theta0=(0.5, 2.0, 0.5), steps=50, adam=(0.1, 0.9, 0.999, 1e-8))
+
+
+def c3_optimize(reference: bool):
+    """The 50 Adam steps timed whole: this library's gprat_cu_optimize (one
+    call, every step on the GPU) and, if `reference`, the reference's own
+    CPU optimize (compiled from source, oracle/_ref) on all host cores."""
+    from gprat_b200 import capi
+
+    c = C3
+    x, y, _ = synthetic(c["n"], 16, c["d"])
+    gp = capi.CudaGP(x, y, c["n"] // c["T"], c["T"], c["d"])
+    params = np.array(list(c["theta0"]) + [0.0] * 6)
+    gp.optimize(params.copy(), list(c["adam"]), [1, 1, 1], 1)  # untimed: pages the kernels in
+    t0 = time.perf_counter()
+    losses, final = gp.optimize(params.copy(), list(c["adam"]), [1, 1, 1], c["steps"])
+    ours = time.perf_counter() - t0
+    gp.close()
+    out = {"config": "n_train=8192 n_regressors=8 theta0=(0.5, 2.0, 0.5), 50 Adam steps lr=0.1 b1=0.9 b2=0.999",
+           "ours_s": ours, "ours_final_loss": float(losses[-1]), "ours_final_theta": [float(v) for v in final[:3]]}
+    if reference:
+        from oracle import ref
+
+        threads = os.cpu_count() or 1
+        ref.start(threads)
+        g = ref.RefGP(x, y, c["n"] // c["T"], c["T"], c["d"], c["theta0"])
+        lr, b1, b2, eps = c["adam"]
+        t0 = time.perf_counter()
+        rl = g.optimize(lr, b1, b2, eps, c["steps"])
+        out.update({"reference_s": time.perf_counter() - t0, "reference_cores": threads,
+                    "reference_final_loss": float(rl[-1]),
+                    "final_loss_rel_diff": abs(float(losses[-1]) - float(rl[-1])) / abs(float(rl[-1]))})
+    return out
+
+
+def gpu_calls(wl, mode, reps: int = 3):
     """The same calls through this library's C ABI (host buffers, synchronous),
     at the same sample size as cpu_reference_calls."""
     from gprat_b200 import capi
@@ -320,7 +360,12 @@ def gpu_calls(wl, precision: int, reps: int = 3):
     m = wl["m"] * n // wl["n"]
     x, y, xt = synthetic(n, m, d)
     gp = capi.CudaGP(x, y, n // T, T, d)
-    gp.set_precision(precision)
+    if isinstance(mode, str):
+        set_mode(gp, mode)
+        precision = PRECISIONS[mode][0]
+    else:
+        precision = mode
+        gp.set_precision(precision)
     h = wl["hyper"]
     params = np.array(list(h) + [0.0] * 6)
 
@@ -415,9 +460,21 @@ def config_of(wl):
             "parallelism": "replicas"}
 
 
-PRECISIONS = {"fp64": 0, "mixed-tf32": 1, "mixed-bf16": 2, "fp64-int8": 3}
+# name: (GPRAT_CU_PREC_*, int8 digit planes or 0 for the library default)
+PRECISIONS = {"fp64": (0, 0), "mixed-tf32": (1, 0), "mixed-bf16": (2, 0), "fp64-int8": (3, 0),
+              "fp64-int8-4": (3, 4), "fp64-int8-6": (3, 6)}
 # modes timed beside the headline one (besides FP64, which every run times)
-ARM_ORDER = ("fp64-int8", "mixed-tf32", "mixed-bf16")
+ARM_ORDER = ("fp64-int8", "fp64-int8-4", "mixed-tf32", "mixed-bf16")
+
+
+DEFAULT_SLICES = 5  # the library's default digit-plane count
+
+
+def set_mode(gp, name, slices_override=0):
+    prec, slices = PRECISIONS[name]
+    gp.set_precision(prec)
+    if prec == 3:
+        gp.set_int8_slices(slices_override or slices or DEFAULT_SLICES)
 
 # DRAM traffic of one representative launch of the dominant kernel, from an
 # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum); the live
@@ -593,9 +650,7 @@ def run_ours(args, wl):
     n, m, d, T, hyper = wl["n"], wl["m"], wl["d"], wl["T"], wl["hyper"]
     x, y, xt = synthetic(n, m, d)
     gp = capi.CudaGP(x, y, n // T, T, d, device=local)
-    gp.set_precision(PRECISIONS[args.precision])
-    if args.slices:
-        gp.set_int8_slices(args.slices)
+    set_mode(gp, args.precision, args.slices)
 
     dxt = torch.tensor(xt, device=device)
     dmean = torch.empty(m, dtype=torch.float64, device=device)
@@ -643,14 +698,14 @@ def run_ours(args, wl):
         for prec in others:
             if prec == args.precision:
                 continue
-            gp.set_precision(PRECISIONS[prec])
+            set_mode(gp, prec)
             ma, va = torch.empty_like(dmean), torch.empty_like(dvar)
             el, st, ck = time_device_steps(torch, gp, hyper, dxt, m, ma, va, stream, args.steps, args.warmup,
                                            barrier, local, instrumented=(prec == "fp64"))
             msa = max_over_ranks(el, dist if world > 1 else None, device) / args.steps
             results[prec] = dict(mean=ma.cpu().numpy(), var=va.cpu().numpy(), loss=gp.compute_loss(hyper), ms=msa,
                                  clocks=ck, stats=st)
-        gp.set_precision(PRECISIONS[args.precision])
+        set_mode(gp, args.precision, args.slices)
         ref64 = results["fp64"]
 
         def error_vs_fp64(mean_a, var_a, loss_a):
@@ -680,35 +735,51 @@ def run_ours(args, wl):
         return
 
     peaks = measured_peaks()
+    sustained = peaks.get("bf16_tflops_sustained")
+    extra_peaks = {}
     if args.precision == "fp64":
         peak = measure_fp64_gemm_peak(torch, device)
         kernel = "dgemm_kernel (FP64 DMMA m16n8k8: Cholesky panel/trailing updates + variance solve)"
         peak_source = ("cuBLAS DGEMM (torch.matmul fp64 8192^3, best of 5) measured in this run; "
                        "MEASURED_PEAKS.json holds no FP64 figure")
-    elif args.precision == "mixed-tf32":
-        peak = measure_gemm_peak(torch, device, torch.float32)
-        kernel = ("tc_gemm_kernel<TF32> (tcgen05.mma kind::tf32, TMA-staged, TMEM accumulators: panel solves, "
-                  "trailing updates, variance solve)")
-        peak_source = ("cuBLAS TF32 GEMM (torch.matmul fp32 8192^3 with allow_tf32, best of 5) measured in this "
-                       "run; MEASURED_PEAKS.json holds only the bf16 figure")
-    elif args.precision == "fp64-int8":
-        peak = measure_int8_peak(torch, device)
+    elif args.precision.startswith("fp64-int8"):
+        # int8 tensor-core operations run at twice the bf16 rate on B200, so the
+        # measured dense bf16 figure (sustained: the GEMMs run inside a
+        # half-second step) doubled is this kernel's denominator
+        in_run = measure_int8_peak(torch, device)
+        peak = 2.0 * sustained if sustained else in_run
         kernel = ("oz_gemm_kernel (tcgen05.mma.cta_group::2 kind::i8, int32 groups in TMEM, FP64 accumulation in the "
                   "epilogue: every product of the factorisation and of the variance solve)")
-        peak_source = ("cuBLASLt int8 GEMM (torch._int_mm 8192^3, best of 5) measured in this run; "
-                       "MEASURED_PEAKS.json holds no int8 figure")
+        peak_source = ("2 x MEASURED_PEAKS.json bf16_tflops_sustained (of measured; int8 runs at twice the bf16 "
+                       "rate)" if sustained else "cuBLASLt int8 GEMM measured in this run (MEASURED_PEAKS.json absent)")
+        extra_peaks = {"cublaslt_int8_in_run": in_run,
+                       "frac_of_cublaslt_int8_in_run": None}
+    elif args.precision == "mixed-tf32":
+        peak = sustained or measure_gemm_peak(torch, device, torch.bfloat16)
+        kernel = ("tc_gemm_kernel<TF32> (tcgen05.mma kind::tf32, TMA-staged, TMEM accumulators: panel solves, "
+                  "trailing updates, variance solve)")
+        peak_source = ("MEASURED_PEAKS.json bf16_tflops_sustained (of measured); TF32 runs at half that rate"
+                       if sustained else "cuBLAS bf16 measured in this run (MEASURED_PEAKS.json absent)")
+        extra_peaks = {"tf32_half_rate": peak / 2.0, "frac_of_tf32_half_rate": None}
     else:
-        peak = peaks.get("bf16_tflops") or measure_gemm_peak(torch, device, torch.bfloat16)
+        peak = sustained or measure_gemm_peak(torch, device, torch.bfloat16)
         kernel = "tc_gemm_kernel<BF16> (tcgen05.mma kind::f16 with bf16 operands)"
-        peak_source = "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks.get("bf16_tflops") else "cuBLAS bf16 in-run"
+        peak_source = ("MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if sustained
+                       else "cuBLAS bf16 measured in this run (MEASURED_PEAKS.json absent)")
     gemm_tflops = stats["gemm_flops"] / (stats["gemm_ms"] / 1e3) / 1e12 if stats["gemm_ms"] > 0 else None
+    if gemm_tflops and "cublaslt_int8_in_run" in extra_peaks:
+        extra_peaks["frac_of_cublaslt_int8_in_run"] = gemm_tflops / extra_peaks["cublaslt_int8_in_run"]
+    if gemm_tflops and "tf32_half_rate" in extra_peaks:
+        extra_peaks["frac_of_tf32_half_rate"] = gemm_tflops / extra_peaks["tf32_half_rate"]
     step_flops = algorithmic_flops(n, m)
     if world == 1 and not args.skip_cpu_baseline:
         times, desc, threads = cpu_reference_full(wl, 1)
         cpu = {"value": times[0], "unit": "s", "cores": threads, "kind": "reference", "sample": desc,
                "calls_at_sample": cpu_reference_calls(wl),
                "gpu_calls_at_sample": {"fp64": gpu_calls(wl, capi.PREC_FP64),
-                                       args.precision: gpu_calls(wl, PRECISIONS[args.precision])}}
+                                       args.precision: gpu_calls(wl, args.precision)}}
+        if not args.skip_c3:
+            cpu["c3_optimize"] = c3_optimize(reference=True)
     else:
         cpu = None
     comparator = None
@@ -716,7 +787,7 @@ def run_ours(args, wl):
         comparator = cusolver_fp64_comparator(torch, device, wl)
     serve = None
     if world == 1 and not args.skip_serving:
-        serve = {args.precision: serving_bench(PRECISIONS[args.precision])}
+        serve = {args.precision: serving_bench(PRECISIONS[args.precision][0])}
         if args.precision != "fp64" and not args.skip_fp64:
             serve["fp64"] = serving_bench(capi.PREC_FP64)
     line = {
@@ -740,8 +811,9 @@ def run_ours(args, wl):
             "achieved": gemm_tflops,
             "peak": peak,
             "peak_source": peak_source,
-            "unit": "TFLOP/s",
+            "unit": "TOP/s (int8)" if args.precision.startswith("fp64-int8") else "TFLOP/s",
             "frac": (gemm_tflops / peak) if gemm_tflops else None,
+            **extra_peaks,
             "traffic": None,
             "traffic_sample": TRAFFIC_SAMPLE.get(args.precision),
             "gemm_share_of_step": (stats["gemm_ms"] / args.steps) / ms_per_step,
@@ -774,12 +846,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
-    ap.add_argument("--precision", choices=sorted(PRECISIONS), default="mixed-tf32")
+    ap.add_argument("--precision", choices=sorted(PRECISIONS), default="fp64-int8")
     ap.add_argument("--slices", type=int, default=0, help="int8 digit planes of the fp64-int8 mode (0 = default)")
     ap.add_argument("--skip-cpu-baseline", action="store_true",
                     help="omit the CPU reference sample (cpu_baseline becomes null)")
     ap.add_argument("--skip-fp64", action="store_true", help="omit the FP64 comparison arm")
     ap.add_argument("--skip-serving", action="store_true", help="omit the serving stream")
+    ap.add_argument("--skip-c3", action="store_true", help="omit the 50-step optimisation timing (ours and reference)")
     ap.add_argument("--skip-arms", action="store_true", help="omit the other precision modes (FP64 still runs)")
     ap.add_argument("--profile", action="store_true",
                     help="device steps only (no CPU sample, e2e loop or peak measurement): for ncu captures")

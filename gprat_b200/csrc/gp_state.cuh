@@ -113,7 +113,7 @@ struct gprat_cu_gp
     // role), of the diagonal-block inverses (B role), of one unsolved panel
     // block (A role, scratch), of the solved rows of W and of one unsolved W
     // block (A role); the cross covariance kept in FP64 for the mean
-    int oz_slices = 6;
+    int oz_slices = 5;
     gprat_cu::DevBuf<int8_t> oz_lr, oz_lb, oz_inv, oz_p, oz_w, oz_wp;
     gprat_cu::DevBuf<int32_t> oz_lr_e, oz_lb_e, oz_inv_e, oz_p_e, oz_w_e, oz_wp_e;
     gprat_cu::DevBuf<double> Kx;

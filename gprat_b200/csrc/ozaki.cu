@@ -6,9 +6,10 @@
 // row maxima (and the block maximum), pass 2 re-reads the block (L1/L2) and
 // writes s digit planes, 4 bytes per lane and plane (128-byte rows).  Digits
 // are peeled with the 1.5 * 2^52 rounding trick: y = t + 1.5 * 2^52 rounds t
-// to the nearest integer d (ties to even), d is the low word of y, and
-// t <- (t - d) * 128 is exact, so D_0 .. D_{s-1} are the leading s balanced
-// base-128 digits of x * 2^(6 - e).
+// to the nearest integer d (ties to even), d is the low word of y, then
+// t <- (t - d) * 254 (t - d is exact; the product rounds only once the
+// remainder has used up the 53 bits), so D_0 .. D_{s-1} are the leading s
+// balanced base-254 digits of x * 2^(6 - e): |D_0| <= 64, |D_p| <= 127.
 //
 // oz_gemm_kernel: persistent, warp-specialised CTA pair (cluster of 2, 384
 // threads each), one 256 x 128 output tile per pair at a time:
@@ -29,11 +30,11 @@
 //   warps 4..11 (both CTAs): epilogue.  Two warps per TMEM lane quarter, 64
 //     columns each (224 registers after setmaxnreg); units are read with
 //     double-buffered tcgen05.ld, 16 columns at a time, in pairs of groups
-//     (g, g + 1) and combined exactly in int32 as 128 P_g + P_{g+1}
-//     (|P_g| <= 7 * 2^19), converted exactly to FP64 (2^52 + 2^31 bias
-//     trick) and added with the pair's scale 2^(eA + eB - 12 - 7 (g + 1))
-//     into 64 FP64 registers per thread (a last unpaired group as 128 P_g at
-//     the same scale).  The next block's exponents are loaded while a block
+//     (g, g + 1) and combined exactly in int32 as 254 P_g + P_{g+1} (at
+//     most 2,112,012,032), converted exactly to FP64 (2^52 + 2^31 bias
+//     trick) and added by one FMA with the pair's scale
+//     2^(eA + eB - 12) / 254^(g + 1) into 64 FP64 registers per thread (a
+//     last unpaired group as 254 P_g at the same scale).  The next block's exponents are loaded while a block
 //     is read.  After the tile's last unit, alpha * acc is staged per warp in
 //     shared memory, 8 columns at a time (16-byte XOR swizzle), and written
 //     to C with coalesced 16-byte accesses (beta = 1 adds to C; those C
@@ -104,7 +105,7 @@ __device__ __forceinline__ void write_digits(const double v[4], int e, int s, in
             const double y = __dadd_rn(t[i], RND);
             const int d = __double2loint(y);
             const double r = __dsub_rn(y, RND);
-            t[i] = __dmul_rn(__dsub_rn(t[i], r), 128.0);
+            t[i] = __dmul_rn(__dsub_rn(t[i], r), OZ_BASE);
             word |= (static_cast<uint32_t>(d) & 0xffu) << (8 * i);
         }
         *reinterpret_cast<uint32_t *>(out + p * plane) = word;
@@ -251,6 +252,7 @@ struct OzKernelArgs
     DeviceStatus *status;
     int groups;
     int tiles_m, tiles_n, ntiles;
+    double wpow[OZ_MAX_SLICES + 1];  // wpow[j] = 1 / OZ_BASE^j
 };
 
 __device__ __forceinline__ void tma_load_3d_pair(void *dst, const CUtensorMap *map, uint32_t leader_bar, int x, int y,
@@ -563,8 +565,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     eb_next = ebblk[kb + 1];
                 }
                 const bool bad = ea == OZ_BAD_EXP || eb == OZ_BAD_EXP;
-                // groups in pairs (g, g + 1): 128 P_g + P_{g+1} is exact in int32
-                // (|P_g| <= 7 * 2^19), so one conversion and one FMA serve both
+                // groups in pairs (g, g + 1): OZ_BASE P_g + P_{g+1} is exact in int32
+                // (at most 2,112,012,032 for the pair (4, 5), the largest), so one
+                // conversion and one FMA serve both
                 for (int g = 0; g < G; g += 2)
                 {
                     const bool two = g + 1 < G;
@@ -581,8 +584,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                                                static_cast<uint32_t>(h * 64);
                     const uint32_t t0 = lane_base + static_cast<uint32_t>(u0 * 128);
                     const uint32_t t1 = lane_base + static_cast<uint32_t>(u1 * 128);
-                    // a last unpaired group counts as 128 P_g + 0 at the pair's scale (the same value)
-                    const double sc = bad ? __longlong_as_double(0x7ff8000000000000ll) : pow2(ea + eb - 12 - 7 * (g + 1));
+                    // a last unpaired group counts as OZ_BASE P_g + 0 at the pair's scale
+                    const double sc = bad ? __longlong_as_double(0x7ff8000000000000ll)
+                                          : pow2(ea + eb - 12) * p.wpow[g + 1];
                     // 16 columns of each group at a time, double-buffered: the next
                     // chunk's tensor-memory loads are in flight while this chunk converts
                     auto chunk = [&](int32_t(&v)[16], int32_t(&w)[16], int32_t(&vn)[16], int32_t(&wn)[16], int c)
@@ -623,7 +627,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 #pragma unroll
                         for (int k = 0; k < 16; ++k)
                         {
-                            acc[c * 16 + k] = fma(i2d(v[k] * 128 + w[k]), sc, acc[c * 16 + k]);
+                            acc[c * 16 + k] = fma(i2d(v[k] * OZ_IBASE + w[k]), sc, acc[c * 16 + k]);
                         }
                     };
                     int32_t va[16], wa[16], vb[16], wb[16];
@@ -913,6 +917,12 @@ void oz_gemm(const OzOperand &A, const OzOperand &B, const OzGemmArgs &a, cudaSt
     k.rowsq_half = a.rowsq_half;
     k.status = a.status;
     k.groups = G;
+    double pw = 1.0;
+    for (int j = 0; j <= OZ_MAX_SLICES; ++j)
+    {
+        k.wpow[j] = 1.0 / pw;  // OZ_BASE^j is exact up to j = 6
+        pw *= OZ_BASE;
+    }
     k.tiles_m = ceil_div(a.M, 256);
     k.tiles_n = ceil_div(a.N, 128);
     if (a.lower)

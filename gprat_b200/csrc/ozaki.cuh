@@ -6,20 +6,23 @@
 // in the integer form of H. Ootomo, K. Ozaki, R. Yokota, "DGEMM on integer
 // matrix multiplication unit", IJHPCA 38 (2024).
 //
-// A row-major FP64 matrix X is held as s int8 digit planes D_0..D_{s-1} and
-// power-of-two scales ("slices"):
-//     X[r][c] ~= 2^(e - 6) * sum_{p < s} D_p[r][c] * 2^(-7 p),   |D_p| <= 64,
+// A row-major FP64 matrix X is held as s int8 digit planes D_0..D_{s-1}
+// and power-of-two scales ("slices"):
+//     X[r][c] ~= 2^(e - 6) * sum_{p < s} D_p[r][c] * 254^(-p),
+//     |D_0| <= 64, |D_p| <= 127 (p >= 1),
 // with one exponent e per row and 128-column block ("row" operand) or per
 // 128 x 128 block ("block" operand); |X| < 2^e over the exponent's domain,
-// so the representation keeps 6 + 7 (s - 1) bits relative to that maximum.
+// so the representation keeps 6 + 7.99 (s - 1) bits relative to that
+// maximum (base 254 is the largest whose balanced digits fit int8).
 // A product C = A B^T over one 128-column block k is then
-//     2^(eA + eB - 12) * sum_{g < G} 2^(-7 g) * P_g,
+//     2^(eA + eB - 12) * sum_{g < G} 254^(-g) * P_g,
 //     P_g = sum_{p + q = g} D^A_p (D^B_q)^T          (exact in int32)
 // and the G = s groups of one block form one unit of int32 accumulation in
 // tensor memory (tcgen05.mma kind::i8) each; the epilogue combines two
-// groups exactly in int32 (128 P_g + P_{g+1}), converts the sum exactly to
-// FP64 and accumulates it with its scale, so the only roundings are the
-// digit truncation and FP64 additions.
+// groups exactly in int32 (254 P_g + P_{g+1}, at most 2,112,012,032 for
+// the largest pair (4, 5)), converts the sum exactly to FP64 and adds it
+// with its scale by one FMA, so the roundings are the digit truncation, the
+// scale 254^-(g+1) and FP64 additions.
 #pragma once
 
 #include "common.cuh"
@@ -31,6 +34,8 @@ namespace gprat_cu
 
 constexpr int OZ_KB = 128;  // columns per exponent block = digit bytes per TMA box row
 constexpr int OZ_MIN_SLICES = 3;
+constexpr double OZ_BASE = 254.0;  // digit base
+constexpr int OZ_IBASE = 254;
 constexpr int OZ_MAX_SLICES = 7;
 
 struct OzOperand

@@ -7,15 +7,15 @@
 // (oz_gemm, ozaki.cuh) with s digit planes.  Only the 128 x 128 diagonal
 // blocks are factored (and inverted) in native FP64, alpha comes from the
 // FP64 triangular solves, the loss from the FP64 diagonal of L.  The
-// result carries the digits' truncation error, about 2^-(7 s - 1) relative
-// to each block's maximum, instead of the 2^-11 of a TF32 working copy, so
-// mean and variance stay within 1e-8 of the FP64 path (s = 6) with no
-// refinement.
+// result carries the digits' truncation error, about 2^-7 254^-(s-1)
+// relative to each block's maximum, instead of the 2^-11 of a TF32 working
+// copy, so mean and variance stay near the FP64 path with no refinement.
 //
 // Schedule (the same look-ahead as the TF32/BF16 path, reference
 // right_looking_cholesky_tiled, core/src/cpu/tiled_algorithms.cpp:14-57):
-// outer panels of 1024 columns, inside a panel left-looking over 128-column
-// blocks.  Per block column r0:
+// outer panels of 4096 columns (measured best at n = 32768 among 512 to
+// 8192), inside a panel left-looking over 128-column blocks.  Per block
+// column r0:
 //   update   K[r0:n, r0:r0+128] -= L[r0:n, K0:r0] L[r0:r0+128, K0:r0]^T
 //   potrf    L_kk and Linv_k in FP64 (potrf_diag)
 //   split    Linv_k -> block digits; the panel block below -> row digits
@@ -34,7 +34,7 @@ namespace
 {
 
 #ifndef GPRAT_OZ_PANEL_BLOCKS
-#define GPRAT_OZ_PANEL_BLOCKS 8  // outer panels of 8 x 128 columns
+#define GPRAT_OZ_PANEL_BLOCKS 32  // outer panels of 32 x 128 columns
 #endif
 #ifndef GPRAT_OZ_MAIN_PERCENT
 #define GPRAT_OZ_MAIN_PERCENT 80  // SMs the trailing update holds while the side stream works
@@ -126,7 +126,7 @@ void factor_oz(gprat_cu_gp *gp, cudaStream_t s, const std::vector<std::pair<int,
     }
     const int64_t ld = gp->ld;
     const OzOps ops = make_oz_ops(gp);
-    const int nbo = NB * knob("GPRAT_CU_OZ_PANEL_BLOCKS", GPRAT_OZ_PANEL_BLOCKS, 1, 16);
+    const int nbo = NB * knob("GPRAT_CU_OZ_PANEL_BLOCKS", GPRAT_OZ_PANEL_BLOCKS, 1, 64);
     const int nout = ceil_div(n, nbo);
     ensure_lookahead(gp, lookahead_events(n));
     cudaStream_t side = gp->side;
@@ -367,7 +367,8 @@ void variance_oz(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, dou
 //   low-priority variance stream: K* in FP64 from the start (copied aside
 //     for the mean), then the recursive variance solve's left half and its
 //     big update once the factor's left half is final, the next quarter at
-//     three quarters, on GPRAT_CU_OZ_VARIANCE_EARLY_PERCENT % of the SMs,
+//     three quarters, on GPRAT_CU_OZ_VARIANCE_EARLY_PERCENT % of the SMs
+//     (default 80),
 //     the rest after the factorisation;
 //   side stream after the factorisation: alpha (FP64 solves) and the mean.
 void fit_predict_oz(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
@@ -416,7 +417,7 @@ void fit_predict_oz(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
         if (early)
         {
             GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, half, 0));
-            w.max_ctas = std::max(2, sms * sm_percent("GPRAT_CU_OZ_VARIANCE_EARLY_PERCENT", 60) / 100);
+            w.max_ctas = std::max(2, sms * sm_percent("GPRAT_CU_OZ_VARIANCE_EARLY_PERCENT", 80) / 100);
             w.solve(0, h);
             w.update(0, h, h, n);
             GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, three_q, 0));

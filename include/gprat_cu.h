@@ -91,7 +91,7 @@ int gprat_cu_gp_set_precision(gprat_cu_gp *gp, int precision);
 
 /*
  * Digit planes of the int8-emulated FP64 products (GPRAT_CU_PREC_FP64_INT8),
- * 3 <= slices <= 7, default 6.  Each operand keeps 6 + 7 (slices - 1) bits
+ * 3 <= slices <= 7, default 5.  Each operand keeps 6 + 7.99 (slices - 1) bits
  * relative to the largest entry of its 128-column block; a product costs
  * slices * (slices + 1) / 2 int8 tensor-core passes.  No counterpart in the
  * reference (whose GPU path is FP64 cuBLAS/cuSOLVER only).
