@@ -2,9 +2,11 @@
 // and the slice representation are described in ozaki.cuh.
 //
 // oz_split_kernel: one CTA per 128 x 128 block of the FP64 source, 8 warps of
-// 16 rows; a lane holds 4 consecutive values of a row.  Pass 1 finds the
-// row maxima (and the block maximum), pass 2 re-reads the block (L1/L2) and
-// writes s digit planes, 4 bytes per lane and plane (128-byte rows).  Digits
+// 16 rows; a lane holds 4 consecutive values of a row.  A warp loads its 16
+// rows at once into registers (so the block's DRAM latency is paid once, not
+// per row), finds the row maxima and, across the CTA, the block maximum,
+// and writes s digit planes from the registers, 4 bytes per lane and plane
+// (128-byte rows).  Digits
 // are peeled with the 1.5 * 2^52 rounding trick: y = t + 1.5 * 2^52 rounds t
 // to the nearest integer d (ties to even), d is the low word of y, then
 // t <- (t - d) * 254 (t - d is exact; the product rounds only once the
@@ -85,8 +87,9 @@ __device__ __forceinline__ int exp_of(double vmax, bool bad)
     return e < -960 ? OZ_ZERO_EXP : e;
 }
 
-// s digit planes of 4 consecutive values (4 bytes per plane at out + p * plane)
-__device__ __forceinline__ void write_digits(const double v[4], int e, int s, int8_t *out, int64_t plane)
+// S digit planes of 4 consecutive values (4 bytes per plane at out + p * plane)
+template <int S>
+__device__ __forceinline__ void write_digits(const double v[4], int e, int8_t *out, int64_t plane)
 {
     double t[4];
     const bool zero = (e == OZ_ZERO_EXP || e == OZ_BAD_EXP);
@@ -96,7 +99,8 @@ __device__ __forceinline__ void write_digits(const double v[4], int e, int s, in
     {
         t[i] = __dmul_rn(v[i], sc);
     }
-    for (int p = 0; p < s; ++p)
+#pragma unroll
+    for (int p = 0; p < S; ++p)
     {
         uint32_t word = 0;
 #pragma unroll
@@ -114,11 +118,15 @@ __device__ __forceinline__ void write_digits(const double v[4], int e, int s, in
 
 constexpr int SPLIT_THREADS = 256;
 
-__global__ void __launch_bounds__(SPLIT_THREADS) oz_split_kernel(const double *__restrict__ src, int64_t lds, int rows,
+// src is deliberately not __restrict__: loads through a const restrict
+// pointer may be compiled as invariant loads, which the compiler is free to
+// move above griddepcontrol.wait, before the producing kernel has finished.
+template <int S>
+__global__ void __launch_bounds__(SPLIT_THREADS) oz_split_kernel(const double *src, int64_t lds, int rows,
                                                                  int8_t *rdig, int64_t rld, int64_t rplane,
                                                                  int32_t *rexp, int rldE, int8_t *bdig, int64_t bld,
                                                                  int64_t bplane, int32_t *bexp, int bldE, int dst_row0,
-                                                                 int dst_kb0, int s)
+                                                                 int dst_kb0)
 {
     __shared__ double wmax[SPLIT_THREADS / 32];
     __shared__ int wbad[SPLIT_THREADS / 32];
@@ -127,27 +135,41 @@ __global__ void __launch_bounds__(SPLIT_THREADS) oz_split_kernel(const double *_
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t col = static_cast<int64_t>(kb) * OZ_KB + lane * 4;
     const int r_first = rb * 128 + warp * 16;
+    // the warp's 16 rows are loaded at once and kept in registers: the row
+    // maxima, the block maximum and the digits all come from these values
+    double v[16][4];
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+    {
+        const int r = r_first + i;
+        if (r < rows)
+        {
+            const double2 *p2 = reinterpret_cast<const double2 *>(src + static_cast<int64_t>(r) * lds + col);
+            const double2 a = p2[0], b = p2[1];
+            v[i][0] = a.x;
+            v[i][1] = a.y;
+            v[i][2] = b.x;
+            v[i][3] = b.y;
+        }
+        else
+        {
+            v[i][0] = v[i][1] = v[i][2] = v[i][3] = 0.0;
+        }
+    }
     int er[16];
     double bm = 0.0;
     bool bbad = false;
 #pragma unroll
     for (int i = 0; i < 16; ++i)
     {
-        const int r = r_first + i;
         double m = 0.0;
         bool bad = false;
-        if (r < rows)
-        {
-            const double2 *p2 = reinterpret_cast<const double2 *>(src + static_cast<int64_t>(r) * lds + col);
-            const double2 a = p2[0], b = p2[1];
-            const double v[4] = { a.x, a.y, b.x, b.y };
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-            {
-                const double av = fabs(v[j]);
-                bad = bad || !(av <= 1.0e308);
-                m = fmax(m, av);
-            }
+        for (int j = 0; j < 4; ++j)
+        {
+            const double av = fabs(v[i][j]);
+            bad = bad || !(av <= 1.0e308);
+            m = fmax(m, av);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
@@ -156,6 +178,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS) oz_split_kernel(const double *_
         }
         bad = __any_sync(0xffffffffu, bad);
         er[i] = exp_of(m, bad);
+        const int r = r_first + i;
         if (rdig != nullptr && r < rows && lane == 0)
         {
             rexp[static_cast<int64_t>(dst_row0 + r) * rldE + dst_kb0 + kb] = er[i];
@@ -182,25 +205,21 @@ __global__ void __launch_bounds__(SPLIT_THREADS) oz_split_kernel(const double *_
     {
         bexp[static_cast<int64_t>(dst_row0 / 128 + rb) * bldE + dst_kb0 + kb] = eb;
     }
+    const int64_t dcol = static_cast<int64_t>(dst_kb0 + kb) * OZ_KB + lane * 4;
 #pragma unroll
     for (int i = 0; i < 16; ++i)
     {
         const int r = r_first + i;
-        if (r >= rows)
+        if (r < rows)
         {
-            break;
-        }
-        const double2 *p2 = reinterpret_cast<const double2 *>(src + static_cast<int64_t>(r) * lds + col);
-        const double2 a = p2[0], b = p2[1];
-        const double v[4] = { a.x, a.y, b.x, b.y };
-        const int64_t dcol = static_cast<int64_t>(dst_kb0 + kb) * OZ_KB + lane * 4;
-        if (rdig != nullptr)
-        {
-            write_digits(v, er[i], s, rdig + static_cast<int64_t>(dst_row0 + r) * rld + dcol, rplane);
-        }
-        if (bdig != nullptr)
-        {
-            write_digits(v, eb, s, bdig + static_cast<int64_t>(dst_row0 + r) * bld + dcol, bplane);
+            if (rdig != nullptr)
+            {
+                write_digits<S>(v[i], er[i], rdig + static_cast<int64_t>(dst_row0 + r) * rld + dcol, rplane);
+            }
+            if (bdig != nullptr)
+            {
+                write_digits<S>(v[i], eb, bdig + static_cast<int64_t>(dst_row0 + r) * bld + dcol, bplane);
+            }
         }
     }
     pdl_launch_dependents();
@@ -846,13 +865,25 @@ void oz_split(const double *src, int64_t lds, int rows, int cols, const OzOperan
     cudaLaunchAttribute attr[1] = { programmatic_launch_attr() };
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    void (*kern)(const double *, int64_t, int, int8_t *, int64_t, int64_t, int32_t *, int, int8_t *, int64_t,
+                 int64_t, int32_t *, int, int, int) = nullptr;
+    switch (slices)
+    {
+    case 3: kern = oz_split_kernel<3>; break;
+    case 4: kern = oz_split_kernel<4>; break;
+    case 5: kern = oz_split_kernel<5>; break;
+    case 6: kern = oz_split_kernel<6>; break;
+    case 7: kern = oz_split_kernel<7>; break;
+    default: throw Error(1, "oz_split: unsupported digit-plane count");
+    }
+    static_assert(OZ_MAX_SLICES == 7 && OZ_MIN_SLICES == 3, "oz_split instantiates 3..7 digit planes");
     GPRAT_CUDA_CHECK(cudaLaunchKernelEx(
-        &cfg, oz_split_kernel, src, lds, rows, row_op ? row_op->digits : static_cast<int8_t *>(nullptr),
+        &cfg, kern, src, lds, rows, row_op ? row_op->digits : static_cast<int8_t *>(nullptr),
         row_op ? row_op->ld : int64_t(0), row_op ? row_op->plane : int64_t(0),
         row_op ? row_op->exps : static_cast<int32_t *>(nullptr), row_op ? row_op->ldE : 0,
         blk_op ? blk_op->digits : static_cast<int8_t *>(nullptr), blk_op ? blk_op->ld : int64_t(0),
         blk_op ? blk_op->plane : int64_t(0), blk_op ? blk_op->exps : static_cast<int32_t *>(nullptr),
-        blk_op ? blk_op->ldE : 0, dst_row0, dst_col0 / OZ_KB, slices));
+        blk_op ? blk_op->ldE : 0, dst_row0, dst_col0 / OZ_KB));
     GPRAT_LAUNCH_CHECK();
 }
 
