@@ -1109,7 +1109,23 @@ int gprat_cu_fit_predict_device(gprat_cu_gp *gp, const double hyper[3], const do
             require(d_test_in != nullptr && d_mean != nullptr, "device buffers must not be NULL");
             require(n_test_in >= static_cast<int64_t>(m) + gp->d - 1, "test series too short for the sliding window");
             DeviceGuard guard(gp->device);
-            cudaStream_t s = stream != nullptr ? static_cast<cudaStream_t>(stream) : gp->stream;
+            // NULL is the legacy default stream: the work runs on the handle's
+            // own (non-blocking) stream, ordered after the work already on the
+            // default stream and before the work enqueued on it later
+            const bool legacy = stream == nullptr;
+            cudaStream_t s = legacy ? gp->stream : static_cast<cudaStream_t>(stream);
+            if (legacy)
+            {
+                for (cudaEvent_t *e : { &gp->join_in, &gp->join_out })
+                {
+                    if (*e == nullptr)
+                    {
+                        GPRAT_CUDA_CHECK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+                    }
+                }
+                GPRAT_CUDA_CHECK(cudaEventRecord(gp->join_in, cudaStreamLegacy));
+                GPRAT_CUDA_CHECK(cudaStreamWaitEvent(s, gp->join_in, 0));
+            }
             upload_hyper(gp, hyper, s);
             if (d_var != nullptr)
             {
@@ -1120,6 +1136,11 @@ int gprat_cu_fit_predict_device(gprat_cu_gp *gp, const double hyper[3], const do
             {
                 fit(gp, s);
                 predict_device(gp, d_test_in, m, d_mean, nullptr, s);
+            }
+            if (legacy)
+            {
+                GPRAT_CUDA_CHECK(cudaEventRecord(gp->join_out, s));
+                GPRAT_CUDA_CHECK(cudaStreamWaitEvent(cudaStreamLegacy, gp->join_out, 0));
             }
         });
 }

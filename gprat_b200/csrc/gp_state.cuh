@@ -83,6 +83,9 @@ struct gprat_cu_gp
     cudaStream_t side = nullptr;     // high-priority stream of the look-ahead panel factorisation
     cudaStream_t vstream = nullptr;  // low-priority stream of the variance solve beside the factorisation
     std::vector<cudaEvent_t> events;  // look-ahead ordering events (created on first use)
+    // orders a device-resident call given the legacy default stream (NULL)
+    // before and after the caller's work on it (created on first use)
+    cudaEvent_t join_in = nullptr, join_out = nullptr;
     int n = 0, n_tiles = 0, T = 0, d = 0;
     int64_t n_in = 0;
     int64_t ld = 0;    // FP64 leading dimension
@@ -177,6 +180,13 @@ struct gprat_cu_gp
         for (cudaEvent_t e : events)
         {
             cudaEventDestroy(e);
+        }
+        for (cudaEvent_t e : { join_in, join_out })
+        {
+            if (e != nullptr)
+            {
+                cudaEventDestroy(e);
+            }
         }
         if (stream != nullptr)
         {

@@ -186,10 +186,12 @@ int gprat_cu_optimize(gprat_cu_gp *gp,
 /*
  * Device-resident fit + predict: assembly, Cholesky, alpha, mean and
  * variance with the test series, mean and var already in HBM on the same
- * device (d_var may be NULL for mean only).  Enqueued on `stream`
- * (a cudaStream_t; NULL = the handle's own stream); returns without
- * synchronising.  No counterpart in the reference (whose calls always copy
- * from and to the host).
+ * device (d_var may be NULL for mean only).  Enqueued on `stream`, a
+ * cudaStream_t; NULL is the legacy default stream (the work then runs on the
+ * handle's own stream, ordered after the default stream's earlier work and
+ * before its later work, so events recorded on the default stream around the
+ * call time it).  Returns without synchronising.  No counterpart in the
+ * reference (whose calls always copy from and to the host).
  */
 int gprat_cu_fit_predict_device(gprat_cu_gp *gp,
                                 const double hyper[3],
