@@ -481,6 +481,15 @@ def set_mode(gp, name, slices_override=0):
 # roofline above aggregates every GEMM launch of the step, so the per-launch
 # traffic is quoted from the capture instead of being measured in this run.
 TRAFFIC_SAMPLE = {
+    "fp64-int8": {
+        "launch": "oz_gemm_kernel, every launch of one fit+predict step at n_train=32768, 5 digit planes "
+                  "(1027 launches, 1-pass ncu launch list); per-launch mean below; largest launch (variance top "
+                  "update 8192 x 16384 x 16384): 36.55 GB DRAM against 4.1 GB algorithmic",
+        "dram_bytes": 212.94e9 / 1027,
+        "dram_bytes_step": 212.94e9,
+        "workload": "c2",
+        "source": "profiles/launch_list_fit_predict_c2_fp64_int8.md",
+    },
     "mixed-tf32": {
         "launch": "tc_gemm_pair_kernel<TF32>, trailing update after panel 0 at n_train=16384: "
                   "lower 14336 x 14336, K=1024, 51 CTA pairs",
@@ -814,7 +823,9 @@ def run_ours(args, wl):
             "unit": "TOP/s (int8)" if args.precision.startswith("fp64-int8") else "TFLOP/s",
             "frac": (gemm_tflops / peak) if gemm_tflops else None,
             **extra_peaks,
-            "traffic": None,
+            # per-launch DRAM bytes of the dominant kernel where a capture of this workload exists
+            "traffic": ((TRAFFIC_SAMPLE.get(args.precision) or {}).get("dram_bytes")
+                        if (TRAFFIC_SAMPLE.get(args.precision) or {}).get("workload") == args.workload else None),
             "traffic_sample": TRAFFIC_SAMPLE.get(args.precision),
             "gemm_share_of_step": (stats["gemm_ms"] / args.steps) / ms_per_step,
             "gemm_launches_per_step": stats["gemm_launches"] / args.steps,
