@@ -10,8 +10,8 @@ default precision is fp64-int8: every product of the factorisation and of
 the variance solve emulated in FP64 on the int8 tensor cores (5 digit
 planes), FP64 diagonal blocks and triangular solves.  The same run times the
 plain FP64 path on the same inputs ("fp64") and reports the headline mode's
-error against it, times the other modes ("arms": 4 digit planes, TF32,
-BF16) with their errors, and runs the serving stream ("serving": four
+error against it, times the other modes ("arms": 4 and 7 digit planes,
+TF32, BF16) with their errors, and runs the serving stream ("serving": four
 resident models, Poisson requests, p50/p99 latency).  K alone is 8.6 GB
 (> L2), so no L2 flush is needed between steps.
 
@@ -462,9 +462,9 @@ def config_of(wl):
 
 # name: (GPRAT_CU_PREC_*, int8 digit planes or 0 for the library default)
 PRECISIONS = {"fp64": (0, 0), "mixed-tf32": (1, 0), "mixed-bf16": (2, 0), "fp64-int8": (3, 0),
-              "fp64-int8-4": (3, 4), "fp64-int8-6": (3, 6)}
+              "fp64-int8-4": (3, 4), "fp64-int8-6": (3, 6), "fp64-int8-7": (3, 7)}
 # modes timed beside the headline one (besides FP64, which every run times)
-ARM_ORDER = ("fp64-int8", "fp64-int8-4", "mixed-tf32", "mixed-bf16")
+ARM_ORDER = ("fp64-int8", "fp64-int8-4", "fp64-int8-7", "mixed-tf32", "mixed-bf16")
 
 
 DEFAULT_SLICES = 5  # the library's default digit-plane count
