@@ -40,7 +40,7 @@ def _requests(n_models, d, count, seed=5):
     return reqs
 
 
-@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("prec", [0, 1, 3])  # FP64, mixed TF32, int8-emulated FP64
 def test_mixed_batches_bit_identical_to_alone(serving, prec):
     capi, S = serving
     models = _models()
@@ -71,7 +71,7 @@ def test_mixed_batches_bit_identical_to_alone(serving, prec):
         mean, var, _, _ = sv.wait(sv.submit_predict(new_mid, series, 100))
         o = O.OracleGP(fx, fy, 8, 128, 8, (1.1, 1.0, 0.1))
         om, ov = o.predict_with_uncertainty(series, 1, 100)
-        tol_m, tol_v = (1e-10, 1e-10) if prec == 0 else (1e-8, 1.5e-2)
+        tol_m, tol_v = {0: (1e-10, 1e-10), 1: (1e-8, 1.5e-2), 3: (1e-8, 1e-8)}[prec]
         assert np.max(np.abs(mean - om)) / np.max(np.abs(om)) <= tol_m
         assert np.max(np.abs(var - ov) / ov) <= tol_v
         assert st.completed >= 2 * len(reqs)
