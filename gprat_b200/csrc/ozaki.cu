@@ -36,11 +36,12 @@
 //     most 2,112,012,032), converted exactly to FP64 (2^52 + 2^31 bias
 //     trick) and added by one FMA with the pair's scale
 //     2^(eA + eB - 12) / 254^(g + 1) into 64 FP64 registers per thread (a
-//     last unpaired group as 254 P_g at the same scale).  The next block's exponents are loaded while a block
-//     is read.  After the tile's last unit, alpha * acc is staged per warp in
-//     shared memory, 8 columns at a time (16-byte XOR swizzle), and written
-//     to C with coalesced 16-byte accesses (beta = 1 adds to C; those C
-//     values are loaded before the staging).
+//     last unpaired group as 254 P_g at the same scale).  The next block's
+//     exponents are loaded while a block is read.  After the tile's last
+//     unit, alpha * acc is written from the registers, 8 columns at a time,
+//     each lane its own row with 16-byte stores (beta = 1 adds to C; those C
+//     values are loaded first); the shared memory a staging transpose would
+//     take holds a ninth digit-plane slot instead.
 // Every mbarrier wait is bounded (tcgen05_ptx.cuh); a wait that gives up
 // raises the CTA's abort flag, the roles leave their loops, TMA copies in
 // flight get 200 us to land, the MMA issuer drains, TMEM is freed and the
@@ -240,12 +241,11 @@ static_assert(128 * OZ_REGS_PRODUCER + 256 * OZ_REGS_EPILOGUE <= OZ_THREADS * 16
 constexpr int OZ_EPI_WARPS = 8;
 constexpr int OZ_A_BYTES = 128 * 128;  // 128 rows x 128 digit bytes
 constexpr int OZ_B_BYTES = 64 * 128;   // this CTA's half of the 128 B rows
-constexpr int OZ_RING = 8;  // slots of one A and one B digit plane (>= s + 1: the next block's first planes load early)
+constexpr int OZ_RING = 9;  // slots of one A and one B digit plane (>= s + 1: the next block's first planes load early)
 constexpr int OZ_NACC = 4;             // int32 accumulators of 128 TMEM columns
 constexpr int OZ_TMEM_COLS = OZ_NACC * 128;
-constexpr int OZ_EPI_BUF = 32 * 64;   // 32 rows x 8 doubles per epilogue warp
 constexpr int OZ_SMEM_BYTES =
-    1024 + OZ_RING * (OZ_A_BYTES + OZ_B_BYTES) + OZ_EPI_WARPS * OZ_EPI_BUF + 512;
+    1024 + OZ_RING * (OZ_A_BYTES + OZ_B_BYTES) + 512;
 static_assert(OZ_SMEM_BYTES <= 232448, "shared memory of the int8 GEMM exceeds the per-CTA limit");
 static_assert(OZ_RING >= OZ_MAX_SLICES + 1, "the ring must hold one block's planes plus one");
 // D = S32, A and B signed 8-bit, K-major, N = 128, M = 256 (CTA pair)
@@ -362,8 +362,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t *aring = smem;
     uint8_t *bring = aring + OZ_RING * OZ_A_BYTES;
-    uint8_t *epi = bring + OZ_RING * OZ_B_BYTES;
-    uint64_t *full = reinterpret_cast<uint64_t *>(epi + OZ_EPI_WARPS * OZ_EPI_BUF);
+    uint64_t *full = reinterpret_cast<uint64_t *>(bring + OZ_RING * OZ_B_BYTES);
     uint64_t *empty = full + OZ_RING;
     uint64_t *tfull = empty + OZ_RING;
     uint64_t *tempty = tfull + OZ_NACC;
@@ -554,7 +553,6 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const int ew = warp - 4;
         const int q = warp & 3;  // TMEM lane quarter this warp may access
         const int h = ew >> 2;   // column half
-        uint8_t *buf = epi + ew * OZ_EPI_BUF;
         int nu = 0;
         bool ok = true;
         for (int t = pair; ok && t < p.ntiles; t += npairs)
@@ -674,14 +672,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             {
                 break;
             }
-            // ---- write alpha * acc: 8 chunks of 32 rows x 8 columns per warp ----
-            // A lane holds one row; the chunk is transposed through shared memory
-            // (16-byte units swizzled by (row >> 1) & 3, conflict-free both ways)
-            // so that 4 lanes write 64 contiguous bytes of one row.  With beta = 1
-            // the chunk's C values are loaded before the staging, so their
-            // latency overlaps it.
+            // ---- write alpha * acc: each lane its own row, 8 columns at a time ----
+            // 16-byte stores straight from the registers (no shared-memory
+            // staging, which leaves its space to the digit-plane ring); with
+            // beta = 1 the 8 columns' C values are loaded first.
             double sq = 0.0;
-            double2 *buf2 = reinterpret_cast<double2 *>(buf);
+            double *crow = p.C + static_cast<int64_t>(rvalid ? row : 0) * p.ldc;
 #pragma unroll
             for (int c = 0; c < 8; ++c)
             {
@@ -691,55 +687,50 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 {
                     continue;
                 }
-                const int uu = lane & 3;
-                const int gc = col0 + 2 * uu;
-                __syncwarp();
+                double2 cold[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
                 {
+                    const int gc = col0 + 2 * j;
+                    const bool full = rvalid && gc + 1 < p.N && (!p.lower || gc + 1 <= row);
+                    cold[j] = (p.beta && full) ? *reinterpret_cast<const double2 *>(crow + gc) : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    const int gc = col0 + 2 * j;
                     const double x = p.alpha * acc[c * 8 + 2 * j];
                     const double y = p.alpha * acc[c * 8 + 2 * j + 1];
-                    buf2[lane * 4 + (j ^ ((lane >> 1) & 3))] = make_double2(x, y);
                     if (p.rowsq != nullptr && rvalid)
                     {
-                        if (col0 + 2 * j < p.N)
+                        if (gc < p.N)
                         {
                             sq += x * x;
                         }
-                        if (col0 + 2 * j + 1 < p.N)
+                        if (gc + 1 < p.N)
                         {
                             sq += y * y;
                         }
                     }
-                }
-                __syncwarp();
-#pragma unroll
-                for (int it = 0; it < 4; ++it)
-                {
-                    const int r = it * 8 + (lane >> 2);
-                    const int grow = row0w + r;
-                    if (grow >= p.M)
+                    if (!rvalid)
                     {
                         continue;
                     }
-                    const double2 v = buf2[r * 4 + (uu ^ ((r >> 1) & 3))];
-                    double *dst = p.C + static_cast<int64_t>(grow) * p.ldc + gc;
-                    const bool ok0 = gc < p.N && (!p.lower || gc <= grow);
-                    const bool ok1 = gc + 1 < p.N && (!p.lower || gc + 1 <= grow);
+                    const bool ok0 = gc < p.N && (!p.lower || gc <= row);
+                    const bool ok1 = gc + 1 < p.N && (!p.lower || gc + 1 <= row);
                     if (ok0 && ok1)
                     {
-                        double2 o = v;
+                        double2 o = make_double2(x, y);
                         if (p.beta)
                         {
-                            const double2 c0 = *reinterpret_cast<const double2 *>(dst);
-                            o.x += c0.x;
-                            o.y += c0.y;
+                            o.x += cold[j].x;
+                            o.y += cold[j].y;
                         }
-                        *reinterpret_cast<double2 *>(dst) = o;
+                        *reinterpret_cast<double2 *>(crow + gc) = o;
                     }
                     else if (ok0)
                     {
-                        dst[0] = p.beta ? dst[0] + v.x : v.x;
+                        crow[gc] = p.beta ? crow[gc] + x : x;
                     }
                 }
             }
