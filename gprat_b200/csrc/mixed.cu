@@ -459,7 +459,9 @@ void ensure_lookahead(gprat_cu_gp *gp, int nevents)
 
 // Events of one factorisation (two per outer panel of at least one block,
 // one to start) and seven for fit_predict_mixed, at the end.
-int lookahead_events(int n) { return 2 * ceil_div(n, NB) + 8; }
+// the look-ahead's 2 per block column and 1, the pipelines' 7 named ones and
+// up to 8 split points of the int8 path's early variance solve
+int lookahead_events(int n) { return 2 * ceil_div(n, NB) + 16; }
 
 TcGemmArgs limited(TcGemmArgs a, int max_ctas)
 {

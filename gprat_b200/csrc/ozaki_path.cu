@@ -13,9 +13,9 @@
 //
 // Schedule (the same look-ahead as the TF32/BF16 path, reference
 // right_looking_cholesky_tiled, core/src/cpu/tiled_algorithms.cpp:14-57):
-// outer panels of 4096 columns (measured best at n = 32768 among 512 to
-// 8192), inside a panel left-looking over 128-column blocks.  Per block
-// column r0:
+// outer panels of 2048 columns (measured best at n = 32768 among 1024 to
+// 4096, with the whole pipeline timed), inside a panel left-looking over
+// 128-column blocks.  Per block column r0:
 //   update   K[r0:n, r0:r0+128] -= L[r0:n, K0:r0] L[r0:r0+128, K0:r0]^T
 //   potrf    L_kk and Linv_k in FP64 (potrf_diag)
 //   split    Linv_k -> block digits; the panel block below -> row digits
@@ -26,6 +26,7 @@
 #include "gp_state.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <string>
 
 namespace gprat_cu
@@ -34,7 +35,7 @@ namespace
 {
 
 #ifndef GPRAT_OZ_PANEL_BLOCKS
-#define GPRAT_OZ_PANEL_BLOCKS 32  // outer panels of 32 x 128 columns
+#define GPRAT_OZ_PANEL_BLOCKS 16  // outer panels of 16 x 128 columns
 #endif
 #ifndef GPRAT_OZ_MAIN_PERCENT
 #define GPRAT_OZ_MAIN_PERCENT 80  // SMs the trailing update holds while the side stream works
@@ -365,11 +366,11 @@ void variance_oz(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, dou
 // Fit, mean and variance (predict_with_uncertainty) on three streams:
 //   caller's stream + high-priority side stream: the factorisation;
 //   low-priority variance stream: K* in FP64 from the start (copied aside
-//     for the mean), then the recursive variance solve's left half and its
-//     big update once the factor's left half is final, the next quarter at
-//     three quarters, on GPRAT_CU_OZ_VARIANCE_EARLY_PERCENT % of the SMs
-//     (default 80),
-//     the rest after the factorisation;
+//     for the mean), then segment by segment of the factor's columns (split
+//     points below) the recursive variance solve of the segment and its
+//     update of every column right of it, each as soon as the factorisation
+//     has finished the segment's columns, on GPRAT_CU_OZ_VARIANCE_EARLY_PERCENT
+//     % of the SMs (default 100), the last segment after the factorisation;
 //   side stream after the factorisation: alpha (FP64 solves) and the mean.
 void fit_predict_oz(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
 {
@@ -377,13 +378,43 @@ void fit_predict_oz(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     const int ne = lookahead_events(n);
     ensure_lookahead(gp, ne);
     cudaEvent_t kx_ready = gp->events[ne - 7];
-    cudaEvent_t begin = gp->events[ne - 6], half = gp->events[ne - 5], three_q = gp->events[ne - 4];
+    cudaEvent_t begin = gp->events[ne - 6];
     cudaEvent_t factored = gp->events[ne - 3], refined = gp->events[ne - 2], solved = gp->events[ne - 1];
     cudaStream_t side = gp->side, vs = gp->vstream;
     const int sms = device_sm_count();
     const bool early = m >= OZ_RECURSIVE_MIN_ROWS;
-    const int h = (n / NB / 2) * NB;
-    const int h2 = h + ((n - h) / NB / 2) * NB;
+    // The variance solve starts on the factor's columns [0, b_1) as soon as the
+    // factorisation has finished them, then [b_1, b_2) and so on; the last
+    // segment follows the factorisation.  Boundaries as fractions of n
+    // (GPRAT_CU_OZ_VARIANCE_SPLITS, comma-separated, at most 8; default
+    // 0.5,0.75,0.875, within 1 % of the best of the sets measured at
+    // n = 32768), each rounded down to a multiple of 128.
+    std::vector<int> bounds;
+    {
+        const char *env = std::getenv("GPRAT_CU_OZ_VARIANCE_SPLITS");
+        std::string spec = env != nullptr ? env : "0.5,0.75,0.875";
+        size_t pos = 0;
+        while (pos <= spec.size() && bounds.size() < 8)
+        {
+            const size_t comma = spec.find(',', pos);
+            const std::string item = spec.substr(pos, comma == std::string::npos ? std::string::npos : comma - pos);
+            char *end = nullptr;
+            const double f = std::strtod(item.c_str(), &end);
+            if (end != item.c_str() && f > 0.0 && f < 1.0)
+            {
+                const int b = static_cast<int>(f * n / NB) * NB;
+                if (b > (bounds.empty() ? 0 : bounds.back()) && b < n)
+                {
+                    bounds.push_back(b);
+                }
+            }
+            if (comma == std::string::npos)
+            {
+                break;
+            }
+            pos = comma + 1;
+        }
+    }
     // buffers first (an allocation must not fall between launches of different streams)
     const int mm = std::max(m, 1);
     gp->W.ensure(static_cast<int64_t>(mm) * gp->ld);
@@ -397,7 +428,10 @@ void fit_predict_oz(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     std::vector<std::pair<int, cudaEvent_t>> splits;
     if (early)
     {
-        splits = { { h, half }, { h2, three_q } };
+        for (size_t i = 0; i < bounds.size(); ++i)
+        {
+            splits.emplace_back(bounds[i], gp->events[ne - 8 - static_cast<int>(i)]);
+        }
     }
     factor_oz(gp, s, splits);
     GPRAT_CUDA_CHECK(cudaEventRecord(factored, s));
@@ -416,16 +450,18 @@ void fit_predict_oz(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
         OzVariance w = v;
         if (early)
         {
-            GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, half, 0));
-            w.max_ctas = std::max(2, sms * sm_percent("GPRAT_CU_OZ_VARIANCE_EARLY_PERCENT", 80) / 100);
-            w.solve(0, h);
-            w.update(0, h, h, n);
-            GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, three_q, 0));
-            w.solve(h, h2);
-            w.update(h, h2, h2, n);
+            w.max_ctas = std::max(2, sms * sm_percent("GPRAT_CU_OZ_VARIANCE_EARLY_PERCENT", 100) / 100);
+            int c0 = 0;
+            for (const auto &sp : splits)
+            {
+                GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, sp.second, 0));
+                w.solve(c0, sp.first);
+                w.update(c0, sp.first, sp.first, n);
+                c0 = sp.first;
+            }
             GPRAT_CUDA_CHECK(cudaStreamWaitEvent(vs, factored, 0));
             w.max_ctas = 0;
-            w.solve(h2, n);
+            w.solve(c0, n);
         }
         else
         {
