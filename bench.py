@@ -10,8 +10,8 @@ default precision is fp64-int8: every product of the factorisation and of
 the variance solve emulated in FP64 on the int8 tensor cores (5 digit
 planes), FP64 diagonal blocks and triangular solves.  The same run times the
 plain FP64 path on the same inputs ("fp64") and reports the headline mode's
-error against it, times the other modes ("arms": 4 and 7 digit planes,
-TF32, BF16) with their errors, and runs the serving stream ("serving": four
+error against it, times the other modes ("arms": 5 planes with 4 digit
+groups in every product, 4 and 7 planes, TF32, BF16) with their errors, and runs the serving stream ("serving": four
 resident models, Poisson requests, p50/p99 latency).  K alone is 8.6 GB
 (> L2), so no L2 flush is needed between steps.
 
@@ -460,21 +460,24 @@ def config_of(wl):
             "parallelism": "replicas"}
 
 
-# name: (GPRAT_CU_PREC_*, int8 digit planes or 0 for the library default)
-PRECISIONS = {"fp64": (0, 0), "mixed-tf32": (1, 0), "mixed-bf16": (2, 0), "fp64-int8": (3, 0),
-              "fp64-int8-4": (3, 4), "fp64-int8-6": (3, 6), "fp64-int8-7": (3, 7)}
+# name: (GPRAT_CU_PREC_*, int8 digit planes or 0 for the library default,
+#        int8 digit groups kept in every product or 0 for all)
+PRECISIONS = {"fp64": (0, 0, 0), "mixed-tf32": (1, 0, 0), "mixed-bf16": (2, 0, 0), "fp64-int8": (3, 0, 0),
+              "fp64-int8-4": (3, 4, 0), "fp64-int8-6": (3, 6, 0), "fp64-int8-7": (3, 7, 0),
+              "fp64-int8-5g4": (3, 5, 4)}
 # modes timed beside the headline one (besides FP64, which every run times)
-ARM_ORDER = ("fp64-int8", "fp64-int8-4", "fp64-int8-7", "mixed-tf32", "mixed-bf16")
+ARM_ORDER = ("fp64-int8", "fp64-int8-5g4", "fp64-int8-4", "fp64-int8-7", "mixed-tf32", "mixed-bf16")
 
 
 DEFAULT_SLICES = 5  # the library's default digit-plane count
 
 
 def set_mode(gp, name, slices_override=0):
-    prec, slices = PRECISIONS[name]
+    prec, slices, groups = PRECISIONS[name]
     gp.set_precision(prec)
     if prec == 3:
         gp.set_int8_slices(slices_override or slices or DEFAULT_SLICES)
+        gp.set_int8_groups(groups, groups)
 
 # DRAM traffic of one representative launch of the dominant kernel, from an
 # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum); the live

@@ -62,6 +62,7 @@ def _load() -> ctypes.CDLL:
     lib.gprat_cu_gp_destroy.argtypes = [ctypes.c_void_p]
     lib.gprat_cu_gp_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.gprat_cu_gp_set_int8_slices.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.gprat_cu_gp_set_int8_groups.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     lib.gprat_cu_cholesky.argtypes = [ctypes.c_void_p, _dp, _dp]
     lib.gprat_cu_predict.argtypes = [ctypes.c_void_p, _dp, _dp, _i64, ctypes.c_int, ctypes.c_int, _dp]
     for name in ("gprat_cu_predict_with_uncertainty", "gprat_cu_predict_with_full_cov"):
@@ -290,8 +291,13 @@ class CudaGP:
         check(lib.gprat_cu_gp_set_precision(self._h, int(precision)))
 
     def set_int8_slices(self, slices: int) -> None:
-        """Digit planes of the int8-emulated FP64 products (PREC_FP64_INT8), 3..8."""
+        """Digit planes of the int8-emulated FP64 products (PREC_FP64_INT8), 3..7."""
         check(lib.gprat_cu_gp_set_int8_slices(self._h, int(slices)))
+
+    def set_int8_groups(self, factor_groups: int, variance_groups: int) -> None:
+        """Digit groups kept in the factorisation's trailing updates and the
+        variance solve's updates (int8-emulated products; 0 = all of them)."""
+        check(lib.gprat_cu_gp_set_int8_groups(self._h, int(factor_groups), int(variance_groups)))
 
     def cholesky(self, hyper) -> List[Optional[np.ndarray]]:
         nt, t = self.n_tiles, self.n_tile_size

@@ -667,6 +667,8 @@ int64_t gp_copy_fitted(gprat_cu_gp *dst, gprat_cu_gp *src)
         bytes += copy_buf(dst, *pr.first, src, *pr.second, true);
     }
     dst->oz_slices = src->oz_slices;
+    dst->oz_factor_groups = src->oz_factor_groups;
+    dst->oz_variance_groups = src->oz_variance_groups;
     bytes += copy_buf(dst, dst->flags, src, src->flags, true);
     bytes += copy_buf(dst, dst->params, src, src->params, true);
     bytes += copy_buf(dst, dst->status, src, src->status, true);
@@ -829,6 +831,20 @@ int gprat_cu_gp_set_int8_slices(gprat_cu_gp *gp, int slices)
                     "int8 slices must be in [" + std::to_string(OZ_MIN_SLICES) + ", " + std::to_string(OZ_MAX_SLICES) +
                         "] (got " + std::to_string(slices) + ")");
             gp->oz_slices = slices;
+        });
+}
+
+int gprat_cu_gp_set_int8_groups(gprat_cu_gp *gp, int factor_groups, int variance_groups)
+{
+    return guarded(
+        [&]
+        {
+            check_gp(gp);
+            require(factor_groups >= 0 && factor_groups <= OZ_MAX_SLICES && variance_groups >= 0 &&
+                        variance_groups <= OZ_MAX_SLICES,
+                    "int8 digit groups must be in [0, " + std::to_string(OZ_MAX_SLICES) + "] (0 = every group)");
+            gp->oz_factor_groups = factor_groups;
+            gp->oz_variance_groups = variance_groups;
         });
 }
 

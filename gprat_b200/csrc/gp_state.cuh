@@ -117,6 +117,8 @@ struct gprat_cu_gp
     // block (A role, scratch), of the solved rows of W and of one unsolved W
     // block (A role); the cross covariance kept in FP64 for the mean
     int oz_slices = 5;
+    int oz_factor_groups = 0;    // digit groups kept in the factorisation's products (0 = oz_slices)
+    int oz_variance_groups = 0;  // and in the variance solve's
     gprat_cu::DevBuf<int8_t> oz_lr, oz_lb, oz_inv, oz_p, oz_w, oz_wp;
     gprat_cu::DevBuf<int32_t> oz_lr_e, oz_lb_e, oz_inv_e, oz_p_e, oz_w_e, oz_wp_e;
     gprat_cu::DevBuf<double> Kx;

@@ -135,6 +135,10 @@ void factor_oz(gprat_cu_gp *gp, cudaStream_t s, const std::vector<std::pair<int,
     auto evR = [&](int k) { return gp->events[1 + nout + k]; };
     const int sms = device_sm_count();
     const int main_ctas = std::max(2, sms * sm_percent("GPRAT_CU_OZ_MAIN_PERCENT", GPRAT_OZ_MAIN_PERCENT) / 100);
+    // digit groups of the trailing updates (0 = every group); the panel chain
+    // (in-panel updates, panel solves) always keeps every group: the factor's
+    // accuracy near the diagonal sets alpha's
+    const int fg = std::min(gp->oz_slices, gp->oz_factor_groups);
     DeviceStatus *st = gp->status.ptr;
 
     {
@@ -197,10 +201,10 @@ void factor_oz(gprat_cu_gp *gp, cudaStream_t s, const std::vector<std::pair<int,
         GPRAT_CUDA_CHECK(cudaStreamWaitEvent(s, evF(k), 0));
         if (rest > 0)
         {
-            oz_gemm(ops.LR, ops.LB,
-                    oz_args(rest, rest, bo, next_end, K0, next_end, K0, kat(gp, next_end, next_end), ld, -1.0, 1.0,
-                            true, st, ahead ? main_ctas : 0),
-                    s);
+            OzGemmArgs a = oz_args(rest, rest, bo, next_end, K0, next_end, K0, kat(gp, next_end, next_end), ld, -1.0,
+                                   1.0, true, st, ahead ? main_ctas : 0);
+            a.groups = fg;
+            oz_gemm(ops.LR, ops.LB, a, s);
         }
         GPRAT_CUDA_CHECK(cudaEventRecord(evR(k), s));
         if (!ahead)
@@ -212,10 +216,12 @@ void factor_oz(gprat_cu_gp *gp, cudaStream_t s, const std::vector<std::pair<int,
         {
             GPRAT_CUDA_CHECK(cudaStreamWaitEvent(side, evR(k - 1), 0));
         }
-        oz_gemm(ops.LR, ops.LB,
-                oz_args(n - pend, next_end - pend, bo, pend, K0, pend, K0, kat(gp, pend, pend), ld, -1.0, 1.0, false,
-                        st),
-                side);
+        {
+            OzGemmArgs a = oz_args(n - pend, next_end - pend, bo, pend, K0, pend, K0, kat(gp, pend, pend), ld, -1.0,
+                                   1.0, false, st);
+            a.groups = fg;
+            oz_gemm(ops.LR, ops.LB, a, side);
+        }
         factor_panel(pend, next_end);
         maybe_split(next_end);
         GPRAT_CUDA_CHECK(cudaEventRecord(evF(k + 1), side));
@@ -263,9 +269,10 @@ struct OzVariance
         {
             return;
         }
-        oz_gemm(WS, ops.LB,
-                oz_args(m, c1 - c0, k1 - k0, 0, k0, c0, k0, W + c0, ld, -1.0, 1.0, false, gp->status.ptr, max_ctas),
-                s);
+        OzGemmArgs a = oz_args(m, c1 - c0, k1 - k0, 0, k0, c0, k0, W + c0, ld, -1.0, 1.0, false, gp->status.ptr,
+                               max_ctas);
+        a.groups = std::min(gp->oz_slices, gp->oz_variance_groups);
+        oz_gemm(WS, ops.LB, a, s);
     }
 
     void solve_panels(int n) const

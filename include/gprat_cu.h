@@ -99,6 +99,21 @@ int gprat_cu_gp_set_precision(gprat_cu_gp *gp, int precision);
 int gprat_cu_gp_set_int8_slices(gprat_cu_gp *gp, int slices);
 
 /*
+ * Digit groups kept in the bulk of the int8-emulated products
+ * (GPRAT_CU_PREC_FP64_INT8): group g holds the digit pairs (p, q) with
+ * p + q = g, and a product keeps groups 0 .. G-1 (G (G + 1) / 2 int8 passes).
+ * factor_groups applies to the factorisation's trailing updates (the panel
+ * chain, whose accuracy sets alpha's, keeps every group), variance_groups to
+ * the variance solve's updates (its 128-column leaves keep every group); 0
+ * keeps all `slices` groups (default).  With 5 planes and 4 groups at
+ * n = 32768, d = 64, mean and variance stay within 1e-8 of FP64 in about
+ * three quarters of the time; at n = 16384, d = 8 they do not (about 1e-7):
+ * the loss of accuracy depends on the problem.  No counterpart in the
+ * reference.
+ */
+int gprat_cu_gp_set_int8_groups(gprat_cu_gp *gp, int factor_groups, int variance_groups);
+
+/*
  * Tiled Cholesky factor (gprat::GP::cholesky, core/src/gprat_c.cpp:336-361;
  * cpu::cholesky core/src/cpu/gp_functions.cpp:18-78).  Writes n_tiles^2
  * row-major tiles of n_tile_size^2 doubles, tile (i,j) at offset

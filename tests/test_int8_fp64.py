@@ -114,6 +114,31 @@ def test_not_positive_definite(capi):
     gp.close()
 
 
+def test_fewer_groups(capi):
+    """Five planes with four digit groups in the trailing updates and the
+    variance solve's updates: faster, and the loss of accuracy it brings
+    depends on the problem.  At the d=64
+    hyper-parameters mean and variance stay within 1e-8 of the oracle; the
+    full group count on the same handle afterwards is back to its own error."""
+    p = problem("d64_n4096")
+    gp = capi.CudaGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"])
+    gp.set_precision(capi.PREC_FP64_INT8)
+    gp.set_int8_groups(4, 4)
+    mean, var = gp.predict_with_uncertainty(p["h"], p["xt"], 1, p["m"])
+    mean_err = np.max(np.abs(mean - p["om"])) / np.max(np.abs(p["om"]))
+    var_err = np.max(np.abs(var - p["ov"]) / p["ov"])
+    print(f"d64_n4096 s=5 groups=4: mean {mean_err:.2e} var {var_err:.2e}")
+    assert mean_err <= MEAN_TOL and var_err <= VAR_TOL
+    gp.set_int8_groups(0, 0)
+    mean, var = gp.predict_with_uncertainty(p["h"], p["xt"], 1, p["m"])
+    assert np.max(np.abs(mean - p["om"])) / np.max(np.abs(p["om"])) <= 1e-9
+    with pytest.raises(capi.GpratCudaError):
+        gp.set_int8_groups(8, 0)
+    with pytest.raises(capi.GpratCudaError):
+        gp.set_int8_groups(0, -1)
+    gp.close()
+
+
 def test_slices_rejected(capi):
     p = problem("d8_n2048")
     gp = capi.CudaGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"])
