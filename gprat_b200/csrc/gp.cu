@@ -23,6 +23,9 @@
 #include "gprat_cu.h"
 
 #include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -337,6 +340,114 @@ void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, s);
 }
 
+// What a captured int8 pipeline bakes in: buffer addresses (through the
+// allocation count), sizes, the mode and the schedule's knobs.
+std::string pipeline_key(const gprat_cu_gp *gp, const double *d_xt, int m, const double *d_mean, const double *d_var)
+{
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "%d|%d|%d|%d|%d|%d|%d|%p|%p|%p|%llu", gp->device, gp->n, m, gp->precision,
+                  gp->oz_slices, gp->oz_factor_groups, gp->oz_variance_groups, static_cast<const void *>(d_xt),
+                  static_cast<const void *>(d_mean), static_cast<const void *>(d_var),
+                  static_cast<unsigned long long>(alloc_generation()));
+    std::string key(buf);
+    for (const char *name : { "GPRAT_CU_OZ_PANEL_BLOCKS", "GPRAT_CU_OZ_MAIN_PERCENT", "GPRAT_CU_OZ_VARIANCE_SPLITS",
+                              "GPRAT_CU_OZ_VARIANCE_EARLY_PERCENT" })
+    {
+        const char *v = std::getenv(name);
+        key += '|';
+        key += v != nullptr ? v : "";
+    }
+    return key;
+}
+
+// The int8-emulated pipeline enqueues about 2,600 launches on three streams.
+// Enqueued one by one, the host runs ahead of the device by the depth of the
+// launch queue and then waits for room, so the variance stream's launches
+// (enqueued after the factorisation's) reach the device only near the end of
+// the factorisation, although the variance solve may start at its first
+// split point.  As one CUDA graph the pipeline is a single launch, and the
+// device starts every kernel as soon as the kernels it depends on are done
+// (kernel nodes keep the priorities of the streams they were captured on).
+// A run whose key equals the previous eager run's is captured and replayed
+// from then on; so the buffers the graph names exist before the capture, and
+// any later allocation or free changes the key.  Step and GEMM timing, which
+// read their events on the host, a stream the caller is capturing, and
+// GPRAT_CU_GRAPH=0 keep the eager launches.
+void fit_predict_oz_graphed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var,
+                            cudaStream_t s)
+{
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    GPRAT_CUDA_CHECK(cudaStreamIsCapturing(s, &capturing));
+    if (knob("GPRAT_CU_GRAPH", 1, 0, 1) == 0 || steps_enabled() || gemm_timing_enabled() ||
+        capturing != cudaStreamCaptureStatusNone)
+    {
+        // (a caller capturing its stream gets the launches in its own graph)
+        fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);
+        return;
+    }
+    const std::string key = pipeline_key(gp, d_xt, m, d_mean, d_var);
+    if (gp->graph_key == key)
+    {
+        if (gp->graph != nullptr)
+        {
+            GPRAT_CUDA_CHECK(cudaGraphLaunch(gp->graph, s));
+        }
+        else
+        {
+            fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);  // this key did not capture
+        }
+        return;
+    }
+    if (gp->graph_seen != key)
+    {
+        fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);
+        gp->graph_seen = pipeline_key(gp, d_xt, m, d_mean, d_var);
+        return;
+    }
+    if (gp->graph != nullptr)
+    {
+        GPRAT_CUDA_CHECK(cudaGraphExecDestroy(gp->graph));
+        gp->graph = nullptr;
+    }
+    gp->graph_key.clear();
+    cudaGraph_t g = nullptr;
+    GPRAT_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try
+    {
+        fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);
+    }
+    catch (...)
+    {
+        cudaStreamEndCapture(s, &g);
+        if (g != nullptr)
+        {
+            cudaGraphDestroy(g);
+        }
+        cudaGetLastError();
+        gp->graph_seen.clear();
+        throw;
+    }
+    GPRAT_CUDA_CHECK(cudaStreamEndCapture(s, &g));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, g, cudaGraphInstantiateFlagUseNodePriority);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess || pipeline_key(gp, d_xt, m, d_mean, d_var) != key)
+    {
+        // not replayable: this key stays eager
+        if (exec != nullptr)
+        {
+            cudaGraphExecDestroy(exec);
+        }
+        cudaGetLastError();
+        gp->graph_key = key;
+        fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);
+        return;
+    }
+    gp->graph = exec;
+    gp->graph_key = key;
+    GPRAT_CUDA_CHECK(cudaGraphLaunch(exec, s));
+}
+
 void fit_predict_var(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var, cudaStream_t s)
 {
     if (mixed(gp))
@@ -345,7 +456,7 @@ void fit_predict_var(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean,
     }
     else if (int8_fp64(gp))
     {
-        fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);
+        fit_predict_oz_graphed(gp, d_xt, m, d_mean, d_var, s);
     }
     else
     {
@@ -484,8 +595,16 @@ void pool_unhold(int64_t bytes)
     set_release_threshold(dev, total);
 }
 
+namespace
+{
+std::atomic<uint64_t> g_alloc_generation{ 0 };
+}  // namespace
+
+uint64_t alloc_generation() { return g_alloc_generation.load(std::memory_order_acquire); }
+
 void *device_alloc(size_t bytes)
 {
+    g_alloc_generation.fetch_add(1, std::memory_order_acq_rel);
     int dev = 0;
     GPRAT_CUDA_CHECK(cudaGetDevice(&dev));
     cudaStream_t st = alloc_stream(dev);
@@ -508,6 +627,7 @@ void device_free(void *p)
     {
         return;
     }
+    g_alloc_generation.fetch_add(1, std::memory_order_acq_rel);
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess)
     {

@@ -7,7 +7,9 @@
 #include "ozaki.cuh"
 #include "tc_gemm.cuh"
 
+#include <cstdint>
 #include <initializer_list>
+#include <string>
 #include <utility>
 #include <vector>
 
@@ -31,6 +33,10 @@ void device_free(void *p);
 // reservation back with pool_unhold.
 void pool_hold(int64_t bytes);
 void pool_unhold(int64_t bytes);
+// Counts the library's device allocations and frees (any handle, any
+// device): a captured CUDA graph names buffer addresses, so a change of this
+// count since its capture retires it.
+uint64_t alloc_generation();
 
 template <typename T>
 struct DevBuf
@@ -123,6 +129,12 @@ struct gprat_cu_gp
     gprat_cu::DevBuf<int32_t> oz_lr_e, oz_lb_e, oz_inv_e, oz_p_e, oz_w_e, oz_wp_e;
     gprat_cu::DevBuf<double> Kx;
 
+    // the int8-emulated fit + predict pipeline captured as one CUDA graph,
+    // replayed while its key (buffers, sizes, modes, knobs) holds; graph_seen
+    // is the key of the last eager run, captured when it repeats
+    cudaGraphExec_t graph = nullptr;
+    std::string graph_key, graph_seen;
+
     ~gprat_cu_gp()
     {
         int prev = -1;
@@ -158,6 +170,10 @@ struct gprat_cu_gp
         for (gprat_cu::DevBuf<int32_t> *b : { &oz_lr_e, &oz_lb_e, &oz_inv_e, &oz_p_e, &oz_w_e, &oz_wp_e })
         {
             b->release();
+        }
+        if (graph != nullptr)
+        {
+            cudaGraphExecDestroy(graph);
         }
         Kx.release();
         flags.release();

@@ -101,6 +101,56 @@ def test_other_entry_points(capi):
     gp.close()
 
 
+def test_graph_replay(capi, monkeypatch):
+    """The int8 pipeline runs eagerly on a new key, is captured as a CUDA graph
+    when the key repeats and replayed after that.  Every run gives the same
+    bits as the eager launches (GPRAT_CU_GRAPH=0); new hyper-parameters reach a
+    replayed graph (they live in device memory), and new output buffers
+    retire it (their addresses are part of the key)."""
+    import torch
+
+    p = problem("d64_n2048")
+    dev = torch.device("cuda", 0)
+    dxt = torch.tensor(p["xt"], device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def run(gp, hyper, dm, dv):
+        gp.fit_predict_device(hyper, dxt.data_ptr(), dxt.numel(), p["m"], dm.data_ptr(), dv.data_ptr(),
+                              stream.cuda_stream)
+        torch.cuda.synchronize()
+        gp.check_status()
+        return dm.cpu().numpy().copy(), dv.cpu().numpy().copy()
+
+    def buffers():
+        return (torch.full((p["m"],), np.nan, dtype=torch.float64, device=dev),
+                torch.full((p["m"],), np.nan, dtype=torch.float64, device=dev))
+
+    h2 = (3.0, 1.3, 0.02)
+    monkeypatch.setenv("GPRAT_CU_GRAPH", "0")
+    gp = capi.CudaGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"])
+    gp.set_precision(capi.PREC_FP64_INT8)
+    want = run(gp, p["h"], *buffers())
+    want2 = run(gp, h2, *buffers())
+    gp.close()
+    monkeypatch.setenv("GPRAT_CU_GRAPH", "1")
+    gp = capi.CudaGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"])
+    gp.set_precision(capi.PREC_FP64_INT8)
+    dm, dv = buffers()
+    for hyper, ref in [(p["h"], want), (p["h"], want), (p["h"], want), (h2, want2), (p["h"], want)]:
+        dm.fill_(np.nan)
+        dv.fill_(np.nan)
+        got = run(gp, hyper, dm, dv)  # eager, captured, then replayed
+        assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+    dm2, dv2 = buffers()
+    for _ in range(3):
+        got = run(gp, p["h"], dm2, dv2)
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    mean_err = np.max(np.abs(want[0] - p["om"])) / np.max(np.abs(p["om"]))
+    assert mean_err <= MEAN_TOL
+    assert np.max(np.abs(want[1] - p["ov"]) / p["ov"]) <= VAR_TOL
+    gp.close()
+
+
 def test_not_positive_definite(capi):
     """A covariance that is not positive definite (negative noise) raises, and
     the handle then works again."""
