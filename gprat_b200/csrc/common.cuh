@@ -235,10 +235,14 @@ void trsv_fused_forward(const double *L, int64_t ld, const double *Linv, int n, 
                         double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
 void trsv_fused_backward(const double *L, int64_t ld, const double *Linv, int n, double *x, int *flags,
                          double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
+// skip (optional, device): when *skip != 0 at launch the solve returns at once
+// (a preconditioner step of an already converged CG iteration)
 void trsv_fused_forward_f32(const float *L, int64_t ld, const float *Linv, int n, double *x, int *flags,
-                            double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
+                            double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0,
+                            const int *skip = nullptr);
 void trsv_fused_backward_f32(const float *L, int64_t ld, const float *Linv, int n, double *x, int *flags,
-                             double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0);
+                             double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas = 0,
+                             const int *skip = nullptr);
 // Poll budget of the single-launch solves' waits on the current device
 // (polls < 0: the default, about 0.5-1 s).
 void set_trsv_wait_budget(long long polls);

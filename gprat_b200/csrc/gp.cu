@@ -32,6 +32,8 @@
 #include <string>
 #include <vector>
 
+#include <unistd.h>  // environ
+
 using namespace gprat_cu;
 
 namespace
@@ -340,8 +342,9 @@ void predict_device(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, 
     finalize_variance(gp->vacc.ptr, m, gp->params.ptr, d_var, s);
 }
 
-// What a captured int8 pipeline bakes in: buffer addresses (through the
-// allocation count), sizes, the mode and the schedule's knobs.
+// What a captured pipeline bakes in: buffer addresses (through the
+// allocation count), sizes, the mode and the schedule's knobs (every
+// GPRAT_CU_* environment variable).
 std::string pipeline_key(const gprat_cu_gp *gp, const double *d_xt, int m, const double *d_mean, const double *d_var)
 {
     char buf[256];
@@ -350,31 +353,35 @@ std::string pipeline_key(const gprat_cu_gp *gp, const double *d_xt, int m, const
                   static_cast<const void *>(d_mean), static_cast<const void *>(d_var),
                   static_cast<unsigned long long>(alloc_generation()));
     std::string key(buf);
-    for (const char *name : { "GPRAT_CU_OZ_PANEL_BLOCKS", "GPRAT_CU_OZ_MAIN_PERCENT", "GPRAT_CU_OZ_VARIANCE_SPLITS",
-                              "GPRAT_CU_OZ_VARIANCE_EARLY_PERCENT" })
+    for (char **e = environ; e != nullptr && *e != nullptr; ++e)
     {
-        const char *v = std::getenv(name);
-        key += '|';
-        key += v != nullptr ? v : "";
+        if (std::strncmp(*e, "GPRAT_CU_", 9) == 0)
+        {
+            key += '|';
+            key += *e;
+        }
     }
     return key;
 }
 
-// The int8-emulated pipeline enqueues about 2,600 launches on three streams.
-// Enqueued one by one, the host runs ahead of the device by the depth of the
-// launch queue and then waits for room, so the variance stream's launches
-// (enqueued after the factorisation's) reach the device only near the end of
-// the factorisation, although the variance solve may start at its first
-// split point.  As one CUDA graph the pipeline is a single launch, and the
-// device starts every kernel as soon as the kernels it depends on are done
-// (kernel nodes keep the priorities of the streams they were captured on).
+// The tensor-core pipelines enqueue thousands of launches on three streams
+// (about 2,600 for the int8-emulated one at n = 32768).  Enqueued one by one,
+// the host runs ahead of the device by the depth of the launch queue and then
+// waits for room, so the variance stream's launches (enqueued after the
+// factorisation's) reach the device only near the end of the factorisation,
+// although the variance solve may start at its first split point.  As one
+// CUDA graph a pipeline is a single launch, and the device starts every
+// kernel as soon as the kernels it depends on are done (kernel nodes keep the
+// priorities of the streams they were captured on).
 // A run whose key equals the previous eager run's is captured and replayed
 // from then on; so the buffers the graph names exist before the capture, and
 // any later allocation or free changes the key.  Step and GEMM timing, which
 // read their events on the host, a stream the caller is capturing, and
 // GPRAT_CU_GRAPH=0 keep the eager launches.
-void fit_predict_oz_graphed(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var,
-                            cudaStream_t s)
+using PipelineFn = void (*)(gprat_cu_gp *, const double *, int, double *, double *, cudaStream_t);
+
+void fit_predict_graphed(PipelineFn run, gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean, double *d_var,
+                         cudaStream_t s)
 {
     cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
     GPRAT_CUDA_CHECK(cudaStreamIsCapturing(s, &capturing));
@@ -382,7 +389,7 @@ void fit_predict_oz_graphed(gprat_cu_gp *gp, const double *d_xt, int m, double *
         capturing != cudaStreamCaptureStatusNone)
     {
         // (a caller capturing its stream gets the launches in its own graph)
-        fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);
+        run(gp, d_xt, m, d_mean, d_var, s);
         return;
     }
     const std::string key = pipeline_key(gp, d_xt, m, d_mean, d_var);
@@ -394,13 +401,13 @@ void fit_predict_oz_graphed(gprat_cu_gp *gp, const double *d_xt, int m, double *
         }
         else
         {
-            fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);  // this key did not capture
+            run(gp, d_xt, m, d_mean, d_var, s);  // this key did not capture
         }
         return;
     }
     if (gp->graph_seen != key)
     {
-        fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);
+        run(gp, d_xt, m, d_mean, d_var, s);
         gp->graph_seen = pipeline_key(gp, d_xt, m, d_mean, d_var);
         return;
     }
@@ -414,7 +421,7 @@ void fit_predict_oz_graphed(gprat_cu_gp *gp, const double *d_xt, int m, double *
     GPRAT_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try
     {
-        fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);
+        run(gp, d_xt, m, d_mean, d_var, s);
     }
     catch (...)
     {
@@ -440,7 +447,7 @@ void fit_predict_oz_graphed(gprat_cu_gp *gp, const double *d_xt, int m, double *
         }
         cudaGetLastError();
         gp->graph_key = key;
-        fit_predict_oz(gp, d_xt, m, d_mean, d_var, s);
+        run(gp, d_xt, m, d_mean, d_var, s);
         return;
     }
     gp->graph = exec;
@@ -452,11 +459,11 @@ void fit_predict_var(gprat_cu_gp *gp, const double *d_xt, int m, double *d_mean,
 {
     if (mixed(gp))
     {
-        fit_predict_mixed(gp, d_xt, m, d_mean, d_var, s);
+        fit_predict_graphed(fit_predict_mixed, gp, d_xt, m, d_mean, d_var, s);
     }
     else if (int8_fp64(gp))
     {
-        fit_predict_oz_graphed(gp, d_xt, m, d_mean, d_var, s);
+        fit_predict_graphed(fit_predict_oz, gp, d_xt, m, d_mean, d_var, s);
     }
     else
     {
@@ -1288,7 +1295,17 @@ int gprat_cu_gp_pcg_iterations(gprat_cu_gp *gp, int *iterations)
         {
             check_gp(gp);
             require(iterations != nullptr, "iterations must not be NULL");
-            *iterations = mixed(gp) ? gp->pcg_last_iters : 0;
+            *iterations = 0;
+            if (mixed(gp) && gp->pcg_s.ptr != nullptr)
+            {
+                // the solve's counter lives on the device (no host wait inside the solve)
+                DeviceGuard guard(gp->device);
+                PcgScalars h{};
+                GPRAT_CUDA_CHECK(cudaDeviceSynchronize());
+                GPRAT_CUDA_CHECK(cudaMemcpy(&h, gp->pcg_s.ptr, sizeof(PcgScalars), cudaMemcpyDeviceToHost));
+                gp->pcg_last_iters = h.iters;
+                *iterations = h.iters;
+            }
         });
 }
 

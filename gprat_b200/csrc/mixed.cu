@@ -32,7 +32,12 @@ namespace gprat_cu
 namespace
 {
 
-constexpr int PCG_MAX_ITERS = 60;
+// Iterations enqueued per solve.  Nothing waits on the host: once the
+// residual test passes, the iterations after it return at once (their kernels
+// read the converged flag), so the solve is one stream of launches that a
+// CUDA graph can hold.  A solve that has not converged after these keeps its
+// last iterate (4 iterations at n = 32768 with the TF32 preconditioner).
+constexpr int PCG_ITERS = 24;
 // 1e-10: four iterations at n = 32768 with a TF32 factor, the mean then within
 // 1.5e-11 of the FP64 path's (a fifth iteration buys 3e-14)
 constexpr double PCG_TOL = 1e-10;
@@ -114,8 +119,13 @@ TcGemmArgs tc_args(int M, int N, int K, int ar, int ac, int br, int bc, float *C
 constexpr int SV_THREADS = 256;
 
 __global__ void __launch_bounds__(SV_THREADS) symv_tile_kernel(const double *__restrict__ K, int64_t ld, int n,
-                                                               const double *__restrict__ p, double *__restrict__ part)
+                                                               const double *__restrict__ p, double *__restrict__ part,
+                                                               const int *skip)
 {
+    if (*skip != 0)
+    {
+        return;
+    }
     __shared__ double pI[128], pJ[128];
     __shared__ double colsum[8][128];
     __shared__ double rowred[8][16][33];  // [warp][row][lane], padded against bank conflicts
@@ -255,8 +265,13 @@ __global__ void __launch_bounds__(SV_THREADS) symv_tile_kernel(const double *__r
     }
 }
 
-__global__ void symv_reduce_kernel(const double *__restrict__ part, int nblk, int n, double *__restrict__ q)
+__global__ void symv_reduce_kernel(const double *__restrict__ part, int nblk, int n, double *__restrict__ q,
+                                   const int *skip)
 {
+    if (*skip != 0)
+    {
+        return;
+    }
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
     {
@@ -274,8 +289,12 @@ __global__ void symv_reduce_kernel(const double *__restrict__ part, int nblk, in
 
 __global__ void __launch_bounds__(DOT_THREADS) dot_partial_kernel(const double *__restrict__ a,
                                                                   const double *__restrict__ b, int n,
-                                                                  double *__restrict__ part)
+                                                                  double *__restrict__ part, const int *skip)
 {
+    if (skip != nullptr && *skip != 0)
+    {
+        return;
+    }
     __shared__ double red[DOT_THREADS];
     double s = 0.0;
     for (int i = blockIdx.x * DOT_THREADS + threadIdx.x; i < n; i += DOT_BLOCKS * DOT_THREADS)
@@ -315,6 +334,10 @@ __global__ void pcg_scalar_kernel(PcgScalars *s, const double *part, int which, 
     {
         return;
     }
+    if (which >= 2 && s->converged != 0)
+    {
+        return;  // an iteration after convergence: nothing changes
+    }
     const double v = sum_parts(part);
     switch (which)
     {
@@ -345,6 +368,10 @@ __global__ void pcg_update_kernel(const PcgScalars *__restrict__ s, double *__re
                                   double *__restrict__ r, const double *__restrict__ p,
                                   const double *__restrict__ q, int n)
 {
+    if (s->converged != 0)
+    {
+        return;
+    }
     const double a = s->a;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
@@ -357,6 +384,10 @@ __global__ void pcg_update_kernel(const PcgScalars *__restrict__ s, double *__re
 __global__ void pcg_direction_kernel(const PcgScalars *__restrict__ s, double *__restrict__ p,
                                      const double *__restrict__ z, int n)
 {
+    if (s->converged != 0)
+    {
+        return;
+    }
     const double b = s->b;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
@@ -364,9 +395,10 @@ __global__ void pcg_direction_kernel(const PcgScalars *__restrict__ s, double *_
     }
 }
 
-void dot(const double *a, const double *b, int n, double *part, cudaStream_t s)
+// skip (optional, device): the product is not needed when *skip != 0
+void dot(const double *a, const double *b, int n, double *part, cudaStream_t s, const int *skip = nullptr)
 {
-    dot_partial_kernel<<<DOT_BLOCKS, DOT_THREADS, 0, s>>>(a, b, n, part);
+    dot_partial_kernel<<<DOT_BLOCKS, DOT_THREADS, 0, s>>>(a, b, n, part, skip);
     GPRAT_LAUNCH_CHECK();
 }
 
@@ -378,26 +410,26 @@ void scalar(PcgScalars *ps, const double *part, int which, cudaStream_t s)
 
 int blocks_for(int n) { return std::min(ceil_div(n, 256), 148 * 8); }
 
-void symv(gprat_cu_gp *gp, const double *p, double *q, cudaStream_t s)
+void symv(gprat_cu_gp *gp, const double *p, double *q, cudaStream_t s, const int *skip)
 {
     const int tiles = gp->nblk * (gp->nblk + 1) / 2;
-    symv_tile_kernel<<<tiles, SV_THREADS, 0, s>>>(gp->K.ptr, gp->ld, gp->n, p, gp->symv_part.ptr);
+    symv_tile_kernel<<<tiles, SV_THREADS, 0, s>>>(gp->K.ptr, gp->ld, gp->n, p, gp->symv_part.ptr, skip);
     GPRAT_LAUNCH_CHECK();
-    symv_reduce_kernel<<<ceil_div(gp->n, 256), 256, 0, s>>>(gp->symv_part.ptr, gp->nblk, gp->n, q);
+    symv_reduce_kernel<<<ceil_div(gp->n, 256), 256, 0, s>>>(gp->symv_part.ptr, gp->nblk, gp->n, q, skip);
     GPRAT_LAUNCH_CHECK();
 }
 
 // z = (L L^T)^-1 r with the low-precision factor; solve_ctas > 0 bounds the
-// solves' grids.
-void precondition(gprat_cu_gp *gp, const double *r, double *z, cudaStream_t s, int solve_ctas)
+// solves' grids; nothing is solved when *skip != 0.
+void precondition(gprat_cu_gp *gp, const double *r, double *z, cudaStream_t s, int solve_ctas, const int *skip)
 {
     GPRAT_CUDA_CHECK(cudaMemcpyAsync(z, r, gp->n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     gp->flags.ensure(2);
     gp->trsv_b.ensure(gp->n);
     trsv_fused_forward_f32(gp->K32.ptr, gp->ld32, gp->Linv32.ptr, gp->n, z, gp->flags.ptr, gp->trsv_b.ptr,
-                           gp->status.ptr, s, solve_ctas);
+                           gp->status.ptr, s, solve_ctas, skip);
     trsv_fused_backward_f32(gp->K32.ptr, gp->ld32, gp->Linv32.ptr, gp->n, z, gp->flags.ptr, gp->trsv_b.ptr,
-                            gp->status.ptr, s, solve_ctas);
+                            gp->status.ptr, s, solve_ctas, skip);
 }
 
 }  // namespace
@@ -651,38 +683,30 @@ void alpha_mixed(gprat_cu_gp *gp, cudaStream_t s, int solve_ctas)
     double *x = gp->alpha.ptr, *r = gp->pcg_r.ptr, *z = gp->pcg_z.ptr, *p = gp->pcg_p.ptr, *q = gp->pcg_q.ptr;
     const int nb = blocks_for(n);
 
+    const int *done = &ps->converged;  // device flag, set by the residual test
     GPRAT_CUDA_CHECK(cudaMemsetAsync(x, 0, n * sizeof(double), s));
     GPRAT_CUDA_CHECK(cudaMemcpyAsync(r, gp->y.ptr, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     dot(r, r, n, part, s);
     scalar(ps, part, 0, s);
-    precondition(gp, r, z, s, solve_ctas);
-    dot(r, z, n, part, s);
+    precondition(gp, r, z, s, solve_ctas, done);
+    dot(r, z, n, part, s, done);
     scalar(ps, part, 1, s);
     GPRAT_CUDA_CHECK(cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    PcgScalars h{};
-    int it = 0;
-    for (; it < PCG_MAX_ITERS; ++it)
+    for (int it = 0; it < PCG_ITERS; ++it)
     {
-        symv(gp, p, q, s);
-        dot(p, q, n, part, s);
+        symv(gp, p, q, s, done);
+        dot(p, q, n, part, s, done);
         scalar(ps, part, 2, s);
         pcg_update_kernel<<<nb, 256, 0, s>>>(ps, x, r, p, q, n);
         GPRAT_LAUNCH_CHECK();
-        dot(r, r, n, part, s);
+        dot(r, r, n, part, s, done);
         scalar(ps, part, 3, s);
-        GPRAT_CUDA_CHECK(cudaMemcpyAsync(&h, ps, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
-        GPRAT_CUDA_CHECK(cudaStreamSynchronize(s));
-        if (h.converged)
-        {
-            break;
-        }
-        precondition(gp, r, z, s, solve_ctas);
-        dot(r, z, n, part, s);
+        precondition(gp, r, z, s, solve_ctas, done);
+        dot(r, z, n, part, s, done);
         scalar(ps, part, 4, s);
         pcg_direction_kernel<<<nb, 256, 0, s>>>(ps, p, z, n);
         GPRAT_LAUNCH_CHECK();
     }
-    gp->pcg_last_iters = h.iters;
 }
 
 void loss_mixed(gprat_cu_gp *gp, cudaStream_t s)

@@ -460,8 +460,12 @@ __device__ __forceinline__ double reduce_scatter16(double (&v)[16])
 __global__ void __launch_bounds__(FT, 1) trsv_fwd_f32_kernel(const float *__restrict__ L, int64_t ld,
                                                              const float *__restrict__ Linv, int n,
                                                              const double *__restrict__ b, double *x, int *flags,
-                                                             DeviceStatus *st)
+                                                             DeviceStatus *st, const int *skip)
 {
+    if (skip != nullptr && *skip != 0)
+    {
+        return;  // every CTA reads the same word: none waits on another
+    }
     extern __shared__ __align__(16) double sm[];
     // L_{i,i-2} (tile 0) and L_{i,i-1} (tile 1) in thread-major order:
     // tile[k4][t] = the four floats 64h + 4k4 .. of row t >> 1 (h = t & 1), so
@@ -669,8 +673,12 @@ __global__ void __launch_bounds__(FT, 1) trsv_fwd_f32_kernel(const float *__rest
 __global__ void __launch_bounds__(FT, 1) trsv_bwd_f32_kernel(const float *__restrict__ L, int64_t ld,
                                                              const float *__restrict__ Linv, int n, int nblk,
                                                              const double *__restrict__ b, double *x, int *flags,
-                                                             DeviceStatus *st)
+                                                             DeviceStatus *st, const int *skip)
 {
+    if (skip != nullptr && *skip != 0)
+    {
+        return;
+    }
     extern __shared__ __align__(16) double sm[];
     // L_{i+2,i} (tile 0) and L_{i+1,i} (tile 1), row-major with stride TSTR;
     // thread (cc, h) reads column cc, rows 2k + h
@@ -929,7 +937,7 @@ void trsv_fused_backward(const double *L, int64_t ld, const double *Linv, int n,
 }
 
 void trsv_fused_forward_f32(const float *L, int64_t ld, const float *Linv, int n, double *x, int *flags,
-                            double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas)
+                            double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas, const int *skip)
 {
     if ((ld & 3) != 0 || (reinterpret_cast<uintptr_t>(L) & 15) != 0 || (reinterpret_cast<uintptr_t>(Linv) & 15) != 0)
     {
@@ -938,12 +946,13 @@ void trsv_fused_forward_f32(const float *L, int64_t ld, const float *Linv, int n
     const int nblk = ceil_div(n, FB);
     ensure_smem_attr(reinterpret_cast<const void *>(trsv_fwd_f32_kernel), static_cast<int>(SMEM_F32_FWD));
     prepare(x, scratch, n, flags, s);
-    trsv_fwd_f32_kernel<<<grid_for(nblk, max_ctas), FT, SMEM_F32_FWD, s>>>(L, ld, Linv, n, scratch, x, flags, st);
+    trsv_fwd_f32_kernel<<<grid_for(nblk, max_ctas), FT, SMEM_F32_FWD, s>>>(L, ld, Linv, n, scratch, x, flags, st,
+                                                                        skip);
     GPRAT_LAUNCH_CHECK();
 }
 
 void trsv_fused_backward_f32(const float *L, int64_t ld, const float *Linv, int n, double *x, int *flags,
-                             double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas)
+                             double *scratch, DeviceStatus *st, cudaStream_t s, int max_ctas, const int *skip)
 {
     if ((ld & 3) != 0 || (reinterpret_cast<uintptr_t>(L) & 15) != 0 || (reinterpret_cast<uintptr_t>(Linv) & 15) != 0)
     {
@@ -953,7 +962,7 @@ void trsv_fused_backward_f32(const float *L, int64_t ld, const float *Linv, int 
     ensure_smem_attr(reinterpret_cast<const void *>(trsv_bwd_f32_kernel), static_cast<int>(SMEM_F32_BWD));
     prepare(x, scratch, n, flags, s);
     trsv_bwd_f32_kernel<<<grid_for(nblk, max_ctas), FT, SMEM_F32_BWD, s>>>(L, ld, Linv, n, nblk, scratch, x, flags,
-                                                                        st);
+                                                                        st, skip);
     GPRAT_LAUNCH_CHECK();
 }
 

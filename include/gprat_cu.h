@@ -222,8 +222,8 @@ int gprat_cu_fit_predict_device(gprat_cu_gp *gp,
 int gprat_cu_check_status(gprat_cu_gp *gp);
 
 /* Number of preconditioned-CG iterations the last mixed-precision alpha
- * solve of this handle took (0 in FP64 mode).  No counterpart in the
- * reference. */
+ * solve of this handle took (0 in FP64 mode); waits for the device (the
+ * count is kept there).  No counterpart in the reference. */
 int gprat_cu_gp_pcg_iterations(gprat_cu_gp *gp, int *iterations);
 
 /*

@@ -101,13 +101,18 @@ def test_other_entry_points(capi):
     gp.close()
 
 
-def test_graph_replay(capi, monkeypatch):
-    """The int8 pipeline runs eagerly on a new key, is captured as a CUDA graph
-    when the key repeats and replayed after that.  Every run gives the same
-    bits as the eager launches (GPRAT_CU_GRAPH=0); new hyper-parameters reach a
-    replayed graph (they live in device memory), and new output buffers
-    retire it (their addresses are part of the key)."""
+@pytest.mark.parametrize("mode", ["int8", "tf32"])
+def test_graph_replay(capi, monkeypatch, mode):
+    """The tensor-core pipelines (int8-emulated FP64; TF32 with its PCG solve
+    for alpha, which waits on nothing on the host) run eagerly on a new key,
+    are captured as a CUDA graph when the key repeats and replayed after that.
+    Every run gives the same bits as the eager launches (GPRAT_CU_GRAPH=0); new
+    hyper-parameters reach a replayed graph (they live in device memory), and
+    new output buffers retire it (their addresses are part of the key)."""
     import torch
+
+    prec = capi.PREC_FP64_INT8 if mode == "int8" else capi.PREC_MIXED_TF32
+    mean_tol, var_tol = (MEAN_TOL, VAR_TOL) if mode == "int8" else (1e-8, 1.5e-2)
 
     p = problem("d64_n2048")
     dev = torch.device("cuda", 0)
@@ -128,13 +133,13 @@ def test_graph_replay(capi, monkeypatch):
     h2 = (3.0, 1.3, 0.02)
     monkeypatch.setenv("GPRAT_CU_GRAPH", "0")
     gp = capi.CudaGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"])
-    gp.set_precision(capi.PREC_FP64_INT8)
+    gp.set_precision(prec)
     want = run(gp, p["h"], *buffers())
     want2 = run(gp, h2, *buffers())
     gp.close()
     monkeypatch.setenv("GPRAT_CU_GRAPH", "1")
     gp = capi.CudaGP(p["x"], p["y"], p["n"] // p["T"], p["T"], p["d"])
-    gp.set_precision(capi.PREC_FP64_INT8)
+    gp.set_precision(prec)
     dm, dv = buffers()
     for hyper, ref in [(p["h"], want), (p["h"], want), (p["h"], want), (h2, want2), (p["h"], want)]:
         dm.fill_(np.nan)
@@ -146,8 +151,10 @@ def test_graph_replay(capi, monkeypatch):
         got = run(gp, p["h"], dm2, dv2)
         assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
     mean_err = np.max(np.abs(want[0] - p["om"])) / np.max(np.abs(p["om"]))
-    assert mean_err <= MEAN_TOL
-    assert np.max(np.abs(want[1] - p["ov"]) / p["ov"]) <= VAR_TOL
+    assert mean_err <= mean_tol
+    assert np.max(np.abs(want[1] - p["ov"]) / p["ov"]) <= var_tol
+    if mode == "tf32":
+        assert 1 <= gp.pcg_iterations() <= 24
     gp.close()
 
 
