@@ -486,10 +486,10 @@ def set_mode(gp, name, slices_override=0):
 TRAFFIC_SAMPLE = {
     "fp64-int8": {
         "launch": "oz_gemm_kernel, every launch of one fit+predict step at n_train=32768, 5 digit planes "
-                  "(1027 launches, 1-pass ncu launch list); per-launch mean below; largest launch (variance top "
-                  "update 8192 x 16384 x 16384): 36.55 GB DRAM against 4.1 GB algorithmic",
-        "dram_bytes": 212.94e9 / 1027,
-        "dram_bytes_step": 212.94e9,
+                  "(1035 launches, 1-pass ncu launch list); per-launch mean below; largest launch (variance top "
+                  "update 8192 x 16384 x 16384): 35.86 GB DRAM against 4.1 GB algorithmic",
+        "dram_bytes": 208.86e9 / 1035,
+        "dram_bytes_step": 208.86e9,
         "workload": "c2",
         "source": "profiles/launch_list_fit_predict_c2_fp64_int8.md",
     },
