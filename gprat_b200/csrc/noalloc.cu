@@ -21,7 +21,8 @@
 //     the GPU (different streams or threads, same device) race on it.
 //   * The first call on a device resolves the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current).
-//     Make that first call before any stream capture.  With CUDA's lazy
+//     Every call reads the status word back and synchronises its stream, so
+//     no call can be captured into a CUDA graph.  With CUDA's lazy
 //     module loading (the default) that first call may also load the
 //     library's device code and so reserve the array: a caller that must
 //     never allocate makes one warm-up call outside its critical region.

@@ -240,9 +240,10 @@ int gprat_cu_gp_pcg_iterations(gprat_cu_gp *gp, int *iterations);
  * process exits), so n_tiles * n_tile_size is limited to 1024; larger
  * problems return GPRAT_CU_ERR_INVALID_ARG.  The array is shared by every
  * call and keeps the last call's contents: calls that overlap on the GPU
- * race.  The first call on a device resolves the array's device address
- * (cudaGetSymbolAddress, once per device); make it before any stream capture.
- * With CUDA's lazy module loading that first call may also load the
+ * race.  Every call reads the status word back and synchronises its stream,
+ * so the call cannot be captured into a CUDA graph.  The first call on a
+ * device resolves the array's device address (cudaGetSymbolAddress, once per
+ * device).  With CUDA's lazy module loading that first call may also load the
  * library's device code and reserve the array, so a caller that must never
  * allocate makes one warm-up call outside its critical region; the address
  * is kept for the life of the process (cudaDeviceReset of that device
