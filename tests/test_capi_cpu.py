@@ -87,3 +87,22 @@ def test_trsv_entry_rejects_bad_arguments():
     with pytest.raises(capi.GpratCudaError) as e:
         capi.test_trsv(2, L, np.ones(4))  # no such kind
     assert e.value.code == capi.ERR_INVALID_ARG
+
+
+def test_mode_setters_reject_a_null_handle():
+    """The precision-mode setters, the CG counter and the device-resident call
+    validate the handle before anything reaches the device."""
+    lib = capi.lib
+    calls = [
+        lambda: lib.gprat_cu_gp_set_precision(None, capi.PREC_FP64_INT8),
+        lambda: lib.gprat_cu_gp_set_int8_slices(None, 5),
+        lambda: lib.gprat_cu_gp_set_int8_groups(None, 4, 4),
+        lambda: lib.gprat_cu_gp_pcg_iterations(None, ctypes.byref(ctypes.c_int())),
+    ]
+    for call in calls:
+        assert call() == capi.ERR_INVALID_ARG
+        assert b"NULL" in lib.gprat_cu_last_error()
+    h = np.array([1.0, 1.0, 0.1])
+    rc = lib.gprat_cu_fit_predict_device(None, h.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), None, 0, 0,
+                                         None, None, None)
+    assert rc == capi.ERR_INVALID_ARG
